@@ -1,0 +1,131 @@
+/*
+ * piks3d_gpu.h — C ABI of the B200 solver for PIKS3D's discrete-velocity source
+ * iteration (linearised BGK on binary voxel images).
+ *
+ * PIKS3D (Fortran 90 + MPI + OpenMP) has no library API: main.F90 drives zero-argument
+ * module routines over module globals. Each entry point below replaces one of those
+ * routines for a single-process, single-GPU run (the reference's mpi 1x1x1 layout) and
+ * keeps its argument meaning, file formats and error behaviour. Every function takes
+ * plain pointers and sizes, is callable from C, C++, Fortran ISO_C_BINDING or ctypes,
+ * and returns a piks_status (0 = success). piks_last_error() gives the message.
+ *
+ * Threading: one host thread per context at a time; each context owns one CUDA stream
+ * (or uses the one given with piks_set_stream). Host arrays are borrowed for the call.
+ */
+#ifndef PIKS3D_GPU_H
+#define PIKS3D_GPU_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum piks_status {
+  PIKS_OK = 0,
+  PIKS_ERR_ARG = 1,          /* bad argument or parameter value                           */
+  PIKS_ERR_NC = 2,           /* Nc_fundamental not in {2,4,6,8,12,16} (velocityGrid.F90:122-126, :149-153) */
+  PIKS_ERR_IMAGE = 3,        /* voxel byte other than 0/1 or short stream (physicalGrid.F90:268-275) */
+  PIKS_ERR_CUDA = 4,         /* CUDA runtime error                                        */
+  PIKS_ERR_OOM = 5,          /* device memory exhausted                                   */
+  PIKS_ERR_STATE = 6,        /* call out of order (e.g. iterate before the image is set)  */
+  PIKS_ERR_IO = 7,           /* cannot open / read / write a file (parameters.F90:101-105, output.F90:241-245) */
+  PIKS_ERR_NOT_FOUND = 8     /* no GPU, or the extension was built without a device        */
+} piks_status;
+
+/* Namelist variables of para.in, as read (before initParams adds 2*fluidlayer to Nx and
+ * multiplies by block_rep): parameters.F90:78-82. imageFileName is returned separately. */
+typedef struct piks_params {
+  int32_t Nx, Ny, Nz;            /* physicalNml */
+  int32_t wallExtOrder;          /* 1, 2 (default) or 3                                  */
+  int32_t fluidlayer;            /* fluid layers added at inlet and outlet (default 0)   */
+  double Ref_L;                  /* 1 (default) or 2                                     */
+  int32_t Nc_fundamental;        /* velocityNml: half the points per velocity axis       */
+  int32_t halfRange;             /* 1 = half-range Gauss-Hermite                          */
+  int32_t mpi_xdim, mpi_ydim, mpi_zdim;   /* mpiNml: read and ignored (one process)      */
+  int32_t block_repx, block_repy, block_repz;
+  int32_t maxStep, chkConvergeStep, saveStep;   /* solverNml */
+  double eps;
+  int32_t saveLast, saveFormat;  /* saveFormat 1 = VTI, 2 = Tecplot, 3 = VTK               */
+  double Kn, pressDrop, accom;   /* flowNml */
+} piks_params;
+
+typedef struct piks_ctx piks_ctx;
+
+/* Fills the defaults of initParams (parameters.F90:91-98); other fields zero. */
+piks_status piks_params_default(piks_params *p);
+
+/* Reads the namelists physicalNml, velocityNml, mpiNml, solverNml, flowNml from a para.in
+ * file (initParams, parameters.F90:100-118). image_file receives imageFileName. */
+piks_status piks_read_params(const char *path, piks_params *p, char *image_file, int32_t image_file_len);
+
+/* Creates a context on CUDA device `device`: applies initParams' adjustments and sets up
+ * the velocity grid (setupVelocityGrid, velocityGrid.F90:90-192). device = -1 gives a
+ * host-only context that preprocesses images and answers the getters but cannot iterate. */
+piks_status piks_create(const piks_params *p, int32_t device, piks_ctx **out);
+
+/* setupPhysicalGrid + setupFlow + allocateBuf (physicalGrid.F90:217-1625, flow.F90:76-163):
+ * takes the raw image stream exactly as the reference reads it from imageFileName
+ * (uint8, 0 = fluid, 1 = solid, x fastest, Nx*Ny*Nz bytes for the para.in extents),
+ * drills / thins / labels it on the host, uploads the compact state and zeroes f. */
+piks_status piks_setup_physical_grid(piks_ctx *ctx, const uint8_t *raw, int64_t nbytes);
+
+/* `nsteps` calls of iterate (solver.F90:111-1940) on the device, asynchronously on the
+ * context's stream. iStep advances by nsteps. */
+piks_status piks_iterate(piks_ctx *ctx, int32_t nsteps);
+
+/* chkConverge (output.F90:60-164) at the current iStep: mass flux through x = 2,
+ * error = |1 - mass_new/mass_old| / chkConvergeStep, permeability = mass*Kn*sqrt(4/pi).
+ * Blocks until the device result is on the host. Outputs may be NULL. */
+piks_status piks_chk_converge(piks_ctx *ctx, double *mass, double *permeability, double *error);
+
+/* main.F90:95-128: iterate / chkConverge until error <= eps or maxStep; appends each
+ * check to results_path (Results.dat format, may be NULL) and prints the reference's
+ * stdout lines when verbose. Saves fields every saveStep and at the end (saveLast) into
+ * out_dir when out_dir is not NULL. */
+piks_status piks_run(piks_ctx *ctx, const char *results_path, const char *out_dir, int32_t verbose,
+                     int32_t *steps, double *permeability, double *seconds);
+
+/* Rho, Ux, Uy, Uz over the Nx*Ny*Nz box (x fastest, 0 at non-fluid voxels); any may be NULL. */
+piks_status piks_get_macro(piks_ctx *ctx, double *rho, double *ux, double *uy, double *uz);
+
+/* Field writers saveFlowFieldVTI / saveFlowField / saveFlowFieldVTK (output.F90:166-360)
+ * into directory dir; format as saveFormat. */
+piks_status piks_save_fields(piks_ctx *ctx, const char *dir, int32_t format);
+
+/* Interior voxel labels after preprocessing (image(1:Nx,1:Ny,1:Nz), x fastest): 0 fluid,
+ * 1 solid, 20..73 wall labels of physicalGrid.F90:127-134. */
+piks_status piks_get_labels(piks_ctx *ctx, int32_t *labels);
+
+/* Sizes: [Nx, Ny, Nz, Nc8, Nfluid, nWall, nCorner, nNodes, iStep, nWallLevels]. */
+piks_status piks_get_info(piks_ctx *ctx, int64_t *info, int32_t n);
+
+/* Distribution function in the reference's layout f(Ntotal, Nc8, 8) over the ghosted box
+ * (Nx+4)(Ny+4)(Nz+4), column-major; only voxels the solver reads (fluid voxels and solid
+ * voxels within two cells of fluid along an axis) are filled, the rest are 0. And fw. */
+piks_status piks_get_f(piks_ctx *ctx, double *f_ref, double *fw);
+
+/* Host-side arrays of the preprocessed geometry by name ("label", "nodemap", "roles",
+ * "commit", "wall_nb", ...), for inspection and tests; *count receives the element count,
+ * out (capacity bytes) the data when not NULL. */
+piks_status piks_geometry_array(piks_ctx *ctx, const char *name, void *out, int64_t capacity, int64_t *count);
+
+/* Makes the context enqueue on `stream` (a cudaStream_t); NULL restores its own stream. */
+piks_status piks_set_stream(piks_ctx *ctx, void *stream);
+
+/* Per-kernel device time accumulated since the last reset (CUDA events on the context's
+ * stream): out[2*k] = milliseconds, out[2*k+1] = launches, k over piks_kernel_names(). */
+piks_status piks_kernel_times(piks_ctx *ctx, double *out, int32_t n, int32_t reset);
+const char *piks_kernel_names(void);  /* comma-separated */
+piks_status piks_enable_timing(piks_ctx *ctx, int32_t on);
+
+/* Number of kernel launches one iterate issues on this context (for launch accounting). */
+piks_status piks_launches_per_iteration(piks_ctx *ctx, int64_t *n);
+
+piks_status piks_synchronize(piks_ctx *ctx);
+piks_status piks_destroy(piks_ctx *ctx);
+const char *piks_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

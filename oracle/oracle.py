@@ -1,0 +1,182 @@
+"""TEST INFRASTRUCTURE — ctypes binding of the CPU oracle (oracle/liboracle.so).
+
+Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline / reference leg use this
+module, as the checker or as the timed CPU baseline; the product never imports it.
+See piks_oracle.h for what it restates and for its parity status (unpinned).
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+
+
+class OracleParams(ctypes.Structure):
+    _fields_ = [
+        ("Nx", ctypes.c_int32), ("Ny", ctypes.c_int32), ("Nz", ctypes.c_int32),
+        ("wallExtOrder", ctypes.c_int32), ("fluidlayer", ctypes.c_int32), ("Ref_L", ctypes.c_double),
+        ("Nc_fundamental", ctypes.c_int32), ("halfRange", ctypes.c_int32),
+        ("block_repx", ctypes.c_int32), ("block_repy", ctypes.c_int32), ("block_repz", ctypes.c_int32),
+        ("maxStep", ctypes.c_int32), ("chkConvergeStep", ctypes.c_int32), ("saveStep", ctypes.c_int32),
+        ("eps", ctypes.c_double), ("saveLast", ctypes.c_int32), ("saveFormat", ctypes.c_int32),
+        ("Kn", ctypes.c_double), ("pressDrop", ctypes.c_double), ("accom", ctypes.c_double),
+    ]
+
+
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def load():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        lib = ctypes.CDLL(LIB_PATH)
+        P = ctypes.POINTER
+        d, i32, i64 = ctypes.c_double, ctypes.c_int32, ctypes.c_int64
+        lib.oracle_create.restype = ctypes.c_void_p
+        lib.oracle_create.argtypes = [P(OracleParams), ctypes.c_char_p, i64, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]
+        lib.oracle_destroy.argtypes = [ctypes.c_void_p]
+        lib.oracle_iterate.argtypes = [ctypes.c_void_p, i32]
+        lib.oracle_chk_converge.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, P(d), P(d), P(d)]
+        lib.oracle_run.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, P(i32), P(d), P(d)]
+        lib.oracle_dims.argtypes = [ctypes.c_void_p, P(i64)]
+        lib.oracle_scalars.argtypes = [ctypes.c_void_p, P(d)]
+        lib.oracle_velocity.argtypes = [ctypes.c_void_p, P(d), P(d), P(d), P(d)]
+        for name in ("oracle_get_image", "oracle_get_which_corner", "oracle_get_vecwall", "oracle_get_mapf"):
+            getattr(lib, name).argtypes = [ctypes.c_void_p, P(i32)]
+        for name in ("oracle_get_extcoef", "oracle_get_f", "oracle_get_fw"):
+            getattr(lib, name).argtypes = [ctypes.c_void_p, P(d)]
+        lib.oracle_set_f.argtypes = [ctypes.c_void_p, P(d)]
+        lib.oracle_get_macro.argtypes = [ctypes.c_void_p, P(d), P(d), P(d), P(d)]
+        lib.oracle_get_dir.argtypes = [ctypes.c_void_p, ctypes.c_int, P(i32)]
+        lib.oracle_get_coef.argtypes = [ctypes.c_void_p, ctypes.c_int, P(d)]
+        lib.oracle_save.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int]
+        lib.oracle_save.restype = ctypes.c_int
+        _lib = lib
+    return _lib
+
+
+def _d(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _i(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+
+
+DIM_KEYS = ("Nx", "Ny", "Nz", "Nxtotal", "Nytotal", "Nztotal", "Ntotal", "Nc8", "nWall", "nCorner",
+            "Nfluid", "iStep") + tuple("Nstencil%d" % o for o in range(1, 9))
+
+
+class Oracle:
+    """Single-rank CPU restatement of PIKS3D (reference layout f(Ntotal, Nc8, 8))."""
+
+    def __init__(self, params, raw, nthreads=0):
+        lib = load()
+        op = OracleParams()
+        for name, _ in OracleParams._fields_:
+            setattr(op, name, getattr(params, name) if not isinstance(params, dict) else params[name])
+        data = bytes(np.ascontiguousarray(raw, dtype=np.uint8).reshape(-1)) if not isinstance(raw, (bytes, bytearray)) else bytes(raw)
+        err = ctypes.create_string_buffer(256)
+        self.h = lib.oracle_create(ctypes.byref(op), data, len(data), int(nthreads), err, 256)
+        if not self.h:
+            raise ValueError(err.value.decode())
+        self.lib = lib
+
+    def close(self):
+        if self.h:
+            self.lib.oracle_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def dims(self):
+        a = np.zeros(20, dtype=np.int64)
+        self.lib.oracle_dims(self.h, a.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)))
+        return dict(zip(DIM_KEYS, a.tolist()))
+
+    def scalars(self):
+        a = np.zeros(6)
+        self.lib.oracle_scalars(self.h, _d(a))
+        return dict(zip(("ds", "mu", "DiffFlux", "mass", "error", "permeability"), a.tolist()))
+
+    def velocity(self):
+        n = self.dims()["Nc8"]
+        out = [np.zeros(n) for _ in range(4)]
+        self.lib.oracle_velocity(self.h, *[_d(a) for a in out])
+        return out
+
+    def iterate(self, n=1):
+        self.lib.oracle_iterate(self.h, int(n))
+
+    def chk_converge(self, results_path=None, verbose=False):
+        m, k, e = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        self.lib.oracle_chk_converge(self.h, os.fsencode(results_path) if results_path else None, int(verbose),
+                                     ctypes.byref(m), ctypes.byref(k), ctypes.byref(e))
+        return m.value, k.value, e.value
+
+    def run(self, results_path=None, verbose=False):
+        s, k, t = ctypes.c_int32(), ctypes.c_double(), ctypes.c_double()
+        self.lib.oracle_run(self.h, os.fsencode(results_path) if results_path else None, int(verbose),
+                            ctypes.byref(s), ctypes.byref(k), ctypes.byref(t))
+        return s.value, k.value, t.value
+
+    def image(self):
+        d = self.dims()
+        a = np.zeros(d["Ntotal"], dtype=np.int32)
+        self.lib.oracle_get_image(self.h, _i(a))
+        return a.reshape(d["Nztotal"], d["Nytotal"], d["Nxtotal"])
+
+    def labels(self):
+        """Interior labels as (Nz, Ny, Nx)."""
+        return self.image()[2:-2, 2:-2, 2:-2]
+
+    def f(self):
+        d = self.dims()
+        a = np.zeros(d["Ntotal"] * d["Nc8"] * 8)
+        self.lib.oracle_get_f(self.h, _d(a))
+        return a
+
+    def set_f(self, a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        self.lib.oracle_set_f(self.h, _d(a))
+
+    def fw(self):
+        d = self.dims()
+        a = np.zeros(max(1, d["nCorner"]) * d["Nc8"] * 8)
+        self.lib.oracle_get_fw(self.h, _d(a))
+        return a[: d["nCorner"] * d["Nc8"] * 8]
+
+    def macro(self):
+        """Rho, Ux, Uy, Uz over the ghosted box, shaped (Nztotal, Nytotal, Nxtotal)."""
+        d = self.dims()
+        out = [np.zeros(d["Ntotal"]) for _ in range(4)]
+        self.lib.oracle_get_macro(self.h, *[_d(a) for a in out])
+        return [a.reshape(d["Nztotal"], d["Nytotal"], d["Nxtotal"]) for a in out]
+
+    def extcoef(self):
+        n = self.dims()["nWall"]
+        a = np.zeros(max(1, 2 * n))
+        self.lib.oracle_get_extcoef(self.h, _d(a))
+        return a[: 2 * n].reshape(2, n)
+
+    def vecwall(self):
+        n = self.dims()["nWall"]
+        a = np.zeros(max(1, n), dtype=np.int32)
+        self.lib.oracle_get_vecwall(self.h, _i(a))
+        return a[:n]
+
+    def save(self, out_dir, fmt):
+        return self.lib.oracle_save(self.h, os.fsencode(out_dir), int(fmt))

@@ -1,0 +1,527 @@
+// C ABI of libpiks3d_b200 (include/piks3d_gpu.h): context life cycle, device memory,
+// the per-iteration launch schedule and the host-facing getters / writers.
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "kernels.h"
+#include "piks3d_gpu.h"
+#include "piks_internal.h"
+
+namespace piks {
+void write_fields(const Setup &s, const Geometry &g, const double *rho, const double *ux,
+                  const double *uy, const double *uz, const char *dir, int format, std::string &err, bool &ok);
+}
+
+using namespace piks;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+piks_status fail(piks_status st, const std::string &msg) {
+  g_last_error = msg;
+  return st;
+}
+
+const char kKernelNames[] = "sweep,commit,capture,walls,inlet_outlet,symmetry,moments,flux";
+enum { KT_SWEEP, KT_COMMIT, KT_CAPTURE, KT_WALLS, KT_INLET, KT_SYM, KT_MOM, KT_FLUX, KT_N };
+
+}  // namespace
+
+struct piks_ctx {
+  Setup setup;
+  Velocity vel;
+  Geometry geo;
+  int device = 0;
+  cudaStream_t own_stream = nullptr, stream = nullptr;
+  bool have_geometry = false;       // device state ready
+  bool have_host_geometry = false;  // preprocessing done
+  DevState ds{};
+  std::vector<void *> allocations;
+  int iStep = 0;
+  double mass = 1.0, error = 1.0, permeability = 0.0;
+  bool timing = false;
+  double kt_ms[KT_N] = {0};
+  int64_t kt_n[KT_N] = {0};
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
+  size_t ev_next = 0;
+};
+
+namespace {
+
+piks_status cuda_check(cudaError_t e, const char *what) {
+  if (e == cudaSuccess) return PIKS_OK;
+  if (e == cudaErrorMemoryAllocation) return fail(PIKS_ERR_OOM, std::string(what) + ": " + cudaGetErrorString(e));
+  return fail(PIKS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <typename T>
+piks_status upload(piks_ctx *c, const std::vector<T> &v, T **out, size_t min_count = 1) {
+  size_t n = v.size() < min_count ? min_count : v.size();
+  void *p = nullptr;
+  piks_status st = cuda_check(cudaMalloc(&p, n * sizeof(T)), "cudaMalloc");
+  if (st) return st;
+  c->allocations.push_back(p);
+  if (!v.empty()) {
+    st = cuda_check(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, c->stream), "upload");
+    if (st) return st;
+  }
+  *out = static_cast<T *>(p);
+  return PIKS_OK;
+}
+
+template <typename T>
+piks_status zeros(piks_ctx *c, size_t n, T **out) {
+  void *p = nullptr;
+  piks_status st = cuda_check(cudaMalloc(&p, (n ? n : 1) * sizeof(T)), "cudaMalloc");
+  if (st) return st;
+  c->allocations.push_back(p);
+  st = cuda_check(cudaMemsetAsync(p, 0, (n ? n : 1) * sizeof(T), c->stream), "memset");
+  if (st) return st;
+  *out = static_cast<T *>(p);
+  return PIKS_OK;
+}
+
+void free_device(piks_ctx *c) {
+  for (void *p : c->allocations) cudaFree(p);
+  c->allocations.clear();
+  c->have_geometry = false;
+}
+
+// Event-timed launch of one kernel group when timing is on.
+struct Timed {
+  piks_ctx *c;
+  int k;
+  cudaEvent_t a = nullptr, b = nullptr;
+  Timed(piks_ctx *cc, int kk) : c(cc), k(kk) {
+    if (!c->timing) return;
+    if (c->ev_next + 2 > c->ev_pool.size()) {
+      for (int i = 0; i < 64; ++i) { cudaEvent_t e; cudaEventCreate(&e); c->ev_pool.push_back(e); }
+    }
+    a = c->ev_pool[c->ev_next++];
+    b = c->ev_pool[c->ev_next++];
+    cudaEventRecord(a, c->stream);
+  }
+  ~Timed() {
+    if (!c->timing) return;
+    cudaEventRecord(b, c->stream);
+    c->pending.push_back({k, {a, b}});
+  }
+};
+
+void drain_timing(piks_ctx *c) {
+  if (c->pending.empty()) return;
+  cudaStreamSynchronize(c->stream);
+  for (auto &p : c->pending) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, p.second.first, p.second.second);
+    c->kt_ms[p.first] += ms;
+    c->kt_n[p.first] += 1;
+  }
+  c->pending.clear();
+  c->ev_next = 0;
+}
+
+// One source iteration (solver.F90:111-1940) as a launch sequence on the context stream.
+void enqueue_iteration(piks_ctx *c) {
+  DevState &s = c->ds;
+  cudaStream_t st = c->stream;
+  const int n = c->iStep + 1;          // the iteration being run (1-based)
+  const int cap = n & 1, prev = (n - 1) & 1;
+  const int nd = sweep_num_diagonals(s);
+  {
+    Timed t(c, KT_SWEEP);
+    for (int d = 0; d < nd; ++d) launch_sweep_diagonal(s, d, st);
+  }
+  { Timed t(c, KT_COMMIT); launch_commit(s, st); }
+  { Timed t(c, KT_CAPTURE); launch_capture(s, cap, st); }
+  {
+    Timed t(c, KT_WALLS);
+    const auto &ls = c->geo.level_start;
+    for (size_t L = 0; L + 1 < ls.size(); ++L) launch_walls(s, ls[L], ls[L + 1], prev, st);
+  }
+  { Timed t(c, KT_INLET); launch_inlet_outlet(s, prev, st); }
+  { Timed t(c, KT_SYM); launch_symmetry(s, st); }
+  { Timed t(c, KT_MOM); launch_moments(s, st); }
+  c->iStep = n;
+  if (c->timing && c->pending.size() > 4096) drain_timing(c);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *piks_last_error(void) { return g_last_error.c_str(); }
+const char *piks_kernel_names(void) { return kKernelNames; }
+
+piks_status piks_params_default(piks_params *p) {
+  if (!p) return fail(PIKS_ERR_ARG, "null params");
+  std::memset(p, 0, sizeof *p);
+  // parameters.F90:91-98
+  p->block_repx = p->block_repy = p->block_repz = 1;
+  p->wallExtOrder = 2;
+  p->fluidlayer = 0;
+  p->Ref_L = 1.0;
+  p->saveLast = 1;
+  p->saveFormat = 1;
+  p->halfRange = 1;
+  p->mpi_xdim = p->mpi_ydim = p->mpi_zdim = 1;
+  p->accom = 1.0;
+  p->chkConvergeStep = 10;
+  p->saveStep = 1 << 30;
+  p->maxStep = 1000;
+  p->eps = 1e-8;
+  return PIKS_OK;
+}
+
+piks_status piks_read_params(const char *path, piks_params *p, char *image_file, int32_t len) {
+  if (!path || !p) return fail(PIKS_ERR_ARG, "null argument");
+  std::string img, err;
+  piks_status st = read_namelist(path, *p, img, err);
+  if (st) return fail(st, err);
+  if (image_file && len > 0) {
+    std::strncpy(image_file, img.c_str(), (size_t)len - 1);
+    image_file[len - 1] = 0;
+  }
+  return PIKS_OK;
+}
+
+piks_status piks_create(const piks_params *p, int32_t device, piks_ctx **out) {
+  if (!p || !out) return fail(PIKS_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (device < -1) return fail(PIKS_ERR_ARG, "device index out of range");
+  if (device >= 0) {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(PIKS_ERR_NOT_FOUND, "no CUDA device");
+    if (device >= ndev) return fail(PIKS_ERR_ARG, "device index out of range");
+  }
+  auto *c = new piks_ctx();
+  std::string err;
+  piks_status st = make_setup(*p, c->setup, err);
+  if (!st) st = make_velocity(*p, c->vel, err);
+  if (st) { delete c; return fail(st, err); }
+  c->device = device;
+  if (device < 0) { *out = c; return PIKS_OK; }  // host-only context: preprocessing and getters
+  st = cuda_check(cudaSetDevice(device), "cudaSetDevice");
+  if (!st) st = cuda_check(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+  if (st) { delete c; return st; }
+  c->stream = c->own_stream;
+  upload_tables();
+  st = cuda_check(cudaGetLastError(), "upload_tables");
+  if (st) { cudaStreamDestroy(c->own_stream); delete c; return st; }
+  *out = c;
+  return PIKS_OK;
+}
+
+piks_status piks_setup_physical_grid(piks_ctx *c, const uint8_t *raw, int64_t nbytes) {
+  if (!c) return fail(PIKS_ERR_ARG, "null context");
+  if (c->device >= 0) { cudaSetDevice(c->device); free_device(c); }
+  c->have_host_geometry = false;
+  std::string err;
+  piks_status st = preprocess(c->setup, raw, nbytes, c->geo, err);
+  if (st) return fail(st, err);
+  c->have_host_geometry = true;
+  if (c->device < 0) return PIKS_OK;
+  const Geometry &g = c->geo;
+  const Velocity &v = c->vel;
+  DevState &s = c->ds;
+  s = DevState{};
+  s.Nx = g.Nx; s.Ny = g.Ny; s.Nz = g.Nz; s.GX = g.GX; s.GXY = g.GX * g.GY;
+  s.NF = g.NF; s.NB = g.NB; s.Nc8 = v.Nc8; s.nchunk = (v.Nc8 + 31) / 32;
+  const double ds = c->setup.ds;
+  s.mu = c->setup.mu;
+  s.c15 = 1.5 / ds; s.c20 = 2.0 / ds; s.c05 = -0.5 / ds; s.c10 = 1.0 / ds;
+  s.accom = c->setup.p.accom; s.pressDrop = c->setup.p.pressDrop; s.DiffFlux = v.DiffFlux;
+  const size_t nnodes = (size_t)g.NF + g.NB;
+  int32_t *pi = nullptr; uint8_t *pu8 = nullptr; uint16_t *pu16 = nullptr; double *pd = nullptr;
+#define UP(vec, field, ptr) do { st = upload(c, vec, &ptr); if (st) return st; s.field = ptr; } while (0)
+  UP(g.nodemap, nodemap, pi);
+  UP(g.label, label, pu8);
+  UP(g.bcorner, bcorner, pi);
+  UP(g.roles, roles, pu16);
+  UP(v.cx, cx, pd); UP(v.cy, cy, pd); UP(v.cz, cz, pd); UP(v.w, w, pd);
+  UP(g.wall_node, wall_node, pi); UP(g.wall_label, wall_label, pi); UP(g.wall_corner, wall_corner, pi);
+  UP(g.wall_nb, wall_nb, pi); UP(g.wall_order, wall_order, pi); UP(g.wall_e, wall_e, pd);
+  UP(g.commit, commit, pi);
+  UP(g.plane_x1, plane_x1, pi); UP(g.plane_xN, plane_xN, pi);
+  UP(g.sym_node, sym_node, pi); UP(g.sym_flag, sym_flag, pu8);
+  UP(g.flux_list, flux_list, pi);
+#undef UP
+  s.nWall = g.nWall;
+  s.ncommit = (int)(g.commit.size() / 3);
+  s.nsym = (int)g.sym_node.size();
+  for (int i = 0; i < 10; ++i) s.flux_groups[i] = g.flux_groups[i];
+  const size_t hsize = nnodes * 8 * (size_t)v.Nc8;
+  if ((st = zeros(c, hsize, &s.h))) return st;                                   // flow.F90:92 f = 0
+  if ((st = zeros(c, (size_t)g.nCorner * 8 * v.Nc8, &s.fw))) return st;         // physicalGrid.F90:1624
+  if ((st = zeros(c, (size_t)g.NF, &s.rho))) return st;
+  if ((st = zeros(c, (size_t)g.NF, &s.ux))) return st;
+  if ((st = zeros(c, (size_t)g.NF, &s.uy))) return st;
+  if ((st = zeros(c, (size_t)g.NF, &s.uz))) return st;
+  const size_t plane = (size_t)g.Ny * g.Nz * 4 * v.Nc8;
+  for (int b = 0; b < 2; ++b) {                                                  // flow.F90:151-162
+    if ((st = zeros(c, plane, &s.ghostW[b]))) return st;
+    if ((st = zeros(c, plane, &s.ghostE[b]))) return st;
+  }
+  if ((st = zeros(c, (size_t)1, &s.flux_out))) return st;
+  st = cuda_check(cudaStreamSynchronize(c->stream), "setup");
+  if (st) return st;
+  c->have_geometry = true;
+  c->iStep = 0;
+  c->mass = 1.0;  // flow.F90:97
+  c->error = 1.0;
+  c->permeability = 0.0;
+  return PIKS_OK;
+}
+
+piks_status piks_iterate(piks_ctx *c, int32_t nsteps) {
+  if (!c) return fail(PIKS_ERR_ARG, "null context");
+  if (c->device < 0) return fail(PIKS_ERR_NOT_FOUND, "host-only context (device -1) cannot iterate");
+  if (!c->have_geometry) return fail(PIKS_ERR_STATE, "piks_setup_physical_grid has not been called");
+  if (nsteps < 0) return fail(PIKS_ERR_ARG, "nsteps < 0");
+  cudaSetDevice(c->device);
+  for (int n = 0; n < nsteps; ++n) enqueue_iteration(c);
+  return cuda_check(cudaGetLastError(), "iterate launch");
+}
+
+piks_status piks_chk_converge(piks_ctx *c, double *mass, double *perm, double *err) {
+  if (!c) return fail(PIKS_ERR_ARG, "null context");
+  if (!c->have_geometry) return fail(PIKS_ERR_STATE, "piks_setup_physical_grid has not been called");
+  cudaSetDevice(c->device);
+  const double inv = 1.0 / c->setup.p.Ref_L;
+  {
+    Timed t(c, KT_FLUX);
+    launch_flux(c->ds, c->setup.ds, std::sqrt(1.0 / 2.0), inv * inv, c->stream);
+  }
+  double m2 = 0.0;
+  piks_status st = cuda_check(cudaMemcpyAsync(&m2, c->ds.flux_out, sizeof(double), cudaMemcpyDeviceToHost, c->stream), "flux D2H");
+  if (!st) st = cuda_check(cudaStreamSynchronize(c->stream), "flux sync");
+  if (st) return st;
+  // output.F90:151-155
+  const double kPi = std::atan(1.0) * 4.0;
+  c->error = std::fabs(1.0 - m2 / c->mass) / (double)c->setup.p.chkConvergeStep;
+  c->mass = m2;
+  c->permeability = c->mass * c->setup.p.Kn * std::sqrt(4.0 / kPi);
+  if (mass) *mass = c->mass;
+  if (perm) *perm = c->permeability;
+  if (err) *err = c->error;
+  return PIKS_OK;
+}
+
+piks_status piks_get_macro(piks_ctx *c, double *rho, double *ux, double *uy, double *uz) {
+  if (!c || !c->have_geometry) return fail(PIKS_ERR_STATE, "no geometry");
+  cudaSetDevice(c->device);
+  const Geometry &g = c->geo;
+  std::vector<double> tmp(g.NF);
+  double *dst[4] = {rho, ux, uy, uz};
+  double *src[4] = {c->ds.rho, c->ds.ux, c->ds.uy, c->ds.uz};
+  const size_t box = (size_t)g.Nx * g.Ny * g.Nz;
+  for (int q = 0; q < 4; ++q) {
+    if (!dst[q]) continue;
+    piks_status st = cuda_check(cudaMemcpyAsync(tmp.data(), src[q], g.NF * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "macro D2H");
+    if (!st) st = cuda_check(cudaStreamSynchronize(c->stream), "macro sync");
+    if (st) return st;
+    std::memset(dst[q], 0, box * sizeof(double));
+    for (int32_t n = 0; n < g.NF; ++n) {
+      int64_t gi = g.node_g[n];
+      int i = (int)(gi % g.GX) - 1, j = (int)((gi / g.GX) % g.GY) - 1, k = (int)(gi / ((int64_t)g.GX * g.GY)) - 1;
+      dst[q][(size_t)(i - 1) + (size_t)(j - 1) * g.Nx + (size_t)(k - 1) * g.Nx * g.Ny] = tmp[n];
+    }
+  }
+  return PIKS_OK;
+}
+
+piks_status piks_get_labels(piks_ctx *c, int32_t *labels) {
+  if (!c || !c->have_host_geometry || !labels) return fail(PIKS_ERR_STATE, "no geometry");
+  const Geometry &g = c->geo;
+  for (int k = 1; k <= g.Nz; ++k)
+    for (int j = 1; j <= g.Ny; ++j)
+      for (int i = 1; i <= g.Nx; ++i)
+        labels[(size_t)(i - 1) + (size_t)(j - 1) * g.Nx + (size_t)(k - 1) * g.Nx * g.Ny] = g.label[g.ghost_index(i, j, k)];
+  return PIKS_OK;
+}
+
+piks_status piks_get_info(piks_ctx *c, int64_t *info, int32_t n) {
+  if (!c || !info) return fail(PIKS_ERR_ARG, "null argument");
+  const Geometry &g = c->geo;
+  int64_t v[10] = {c->setup.Nx, c->setup.Ny, c->setup.Nz, c->vel.Nc8, g.NF, g.nWall, g.nCorner,
+                   (int64_t)g.NF + g.NB, c->iStep, (int64_t)(g.level_start.empty() ? 0 : g.level_start.size() - 1)};
+  for (int i = 0; i < n && i < 10; ++i) info[i] = v[i];
+  return PIKS_OK;
+}
+
+piks_status piks_get_f(piks_ctx *c, double *f_ref, double *fw) {
+  if (!c || !c->have_geometry) return fail(PIKS_ERR_STATE, "no geometry");
+  cudaSetDevice(c->device);
+  const Geometry &g = c->geo;
+  const int Nc8 = c->vel.Nc8;
+  const size_t nnodes = (size_t)g.NF + g.NB;
+  piks_status st;
+  if (f_ref) {
+    std::vector<double> h(nnodes * 8 * Nc8);
+    st = cuda_check(cudaMemcpyAsync(h.data(), c->ds.h, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "f D2H");
+    if (!st) st = cuda_check(cudaStreamSynchronize(c->stream), "f sync");
+    if (st) return st;
+    const size_t Ntot = (size_t)g.GX * g.GY * g.GZ;
+    std::memset(f_ref, 0, Ntot * Nc8 * 8 * sizeof(double));
+    for (size_t n = 0; n < nnodes; ++n)
+      for (int o = 0; o < 8; ++o)
+        for (int l = 0; l < Nc8; ++l)
+          f_ref[(size_t)g.node_g[n] + (size_t)l * Ntot + (size_t)o * Ntot * Nc8] = h[(n * 8 + o) * Nc8 + l];
+  }
+  if (fw && g.nCorner > 0) {
+    std::vector<double> t((size_t)g.nCorner * 8 * Nc8);
+    st = cuda_check(cudaMemcpyAsync(t.data(), c->ds.fw, t.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "fw D2H");
+    if (!st) st = cuda_check(cudaStreamSynchronize(c->stream), "fw sync");
+    if (st) return st;
+    for (int cc = 0; cc < g.nCorner; ++cc)
+      for (int o = 0; o < 8; ++o)
+        for (int l = 0; l < Nc8; ++l)
+          fw[(size_t)cc + (size_t)l * g.nCorner + (size_t)o * g.nCorner * Nc8] = t[((size_t)cc * 8 + o) * Nc8 + l];
+  }
+  return PIKS_OK;
+}
+
+piks_status piks_save_fields(piks_ctx *c, const char *dir, int32_t format) {
+  if (!c || !c->have_geometry) return fail(PIKS_ERR_STATE, "no geometry");
+  const Geometry &g = c->geo;
+  const size_t box = (size_t)g.Nx * g.Ny * g.Nz;
+  std::vector<double> r(box), u(box), v(box), w(box);
+  piks_status st = piks_get_macro(c, r.data(), u.data(), v.data(), w.data());
+  if (st) return st;
+  std::string err;
+  bool ok = true;
+  write_fields(c->setup, g, r.data(), u.data(), v.data(), w.data(), dir ? dir : ".", format, err, ok);
+  if (!ok) return fail(PIKS_ERR_IO, err);
+  return PIKS_OK;
+}
+
+piks_status piks_run(piks_ctx *c, const char *results_path, const char *out_dir, int32_t verbose,
+                     int32_t *steps, double *perm, double *seconds) {
+  if (!c || !c->have_geometry) return fail(PIKS_ERR_STATE, "no geometry");
+  const piks_params &p = c->setup.p;
+  c->error = 1.0;  // main.F90:95
+  auto t0 = std::chrono::steady_clock::now();
+  int step;
+  piks_status st;
+  for (step = 1; step <= p.maxStep; ++step) {
+    if ((st = piks_iterate(c, 1))) return st;
+    if (step % p.chkConvergeStep == 0) {
+      if ((st = piks_chk_converge(c, nullptr, nullptr, nullptr))) return st;
+      if (verbose)
+        std::printf("%10d%s%s%s\n", step, fortran_es15_6(c->mass).c_str(), fortran_es15_6(c->permeability).c_str(),
+                    fortran_es15_6(c->error).c_str());
+      if (results_path && results_path[0]) {
+        FILE *fh = std::fopen(results_path, "a");
+        if (!fh) return fail(PIKS_ERR_IO, std::string("cannot open ") + results_path);
+        std::fprintf(fh, "%s%s%s%s%15d\n", fortran_es15_6(p.Kn).c_str(), fortran_es15_6(c->mass).c_str(),
+                     fortran_es15_6(c->permeability).c_str(), fortran_es15_6(c->error).c_str(), step);
+        std::fclose(fh);
+      }
+    }
+    if (out_dir && p.saveStep > 0 && step % p.saveStep == 0)
+      if ((st = piks_save_fields(c, out_dir, p.saveFormat))) return st;
+    if (c->error <= p.eps) {
+      if (step < p.chkConvergeStep) {
+        if ((st = piks_chk_converge(c, nullptr, nullptr, nullptr))) return st;
+      }
+      break;
+    }
+  }
+  cudaStreamSynchronize(c->stream);
+  double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  if (verbose) {
+    char wt[32];
+    std::snprintf(wt, sizeof wt, "%11.3E", secs);
+    std::printf("Walltime= %s, Steps= %6d, K= %s\n", wt, step, fortran_es15_6(c->permeability).c_str());
+  }
+  if (out_dir && p.saveLast)
+    if ((st = piks_save_fields(c, out_dir, p.saveFormat))) return st;
+  if (steps) *steps = step;
+  if (perm) *perm = c->permeability;
+  if (seconds) *seconds = secs;
+  return PIKS_OK;
+}
+
+piks_status piks_geometry_array(piks_ctx *c, const char *name, void *out, int64_t capacity, int64_t *count) {
+  if (!c || !name || !c->have_host_geometry) return fail(PIKS_ERR_STATE, "no geometry");
+  const Geometry &g = c->geo;
+  const void *src = nullptr;
+  size_t n = 0, esz = 0;
+  std::string nm(name);
+#define ARR(key, vec) if (nm == key) { src = vec.data(); n = vec.size(); esz = sizeof(vec[0]); }
+  ARR("nodemap", g.nodemap) ARR("label", g.label) ARR("node_g", g.node_g) ARR("wall_node", g.wall_node)
+  ARR("wall_label", g.wall_label) ARR("wall_e", g.wall_e) ARR("wall_corner", g.wall_corner)
+  ARR("wall_nb", g.wall_nb) ARR("wall_order", g.wall_order) ARR("level_start", g.level_start)
+  ARR("bcorner", g.bcorner) ARR("roles", g.roles) ARR("commit", g.commit) ARR("plane_x1", g.plane_x1)
+  ARR("plane_xN", g.plane_xN) ARR("sym_node", g.sym_node) ARR("sym_flag", g.sym_flag)
+  ARR("flux_list", g.flux_list) ARR("cx", c->vel.cx) ARR("cy", c->vel.cy) ARR("cz", c->vel.cz) ARR("w", c->vel.w)
+#undef ARR
+  if (nm == "flux_groups") { src = g.flux_groups; n = 10; esz = sizeof(int32_t); }
+  if (!esz) return fail(PIKS_ERR_ARG, "unknown geometry array " + nm);
+  if (count) *count = (int64_t)n;
+  if (out) {
+    if (capacity < (int64_t)(n * esz)) return fail(PIKS_ERR_ARG, "buffer too small for " + nm);
+    std::memcpy(out, src, n * esz);
+  }
+  return PIKS_OK;
+}
+
+piks_status piks_set_stream(piks_ctx *c, void *stream) {
+  if (!c) return fail(PIKS_ERR_ARG, "null context");
+  c->stream = stream ? static_cast<cudaStream_t>(stream) : c->own_stream;
+  return PIKS_OK;
+}
+
+piks_status piks_enable_timing(piks_ctx *c, int32_t on) {
+  if (!c) return fail(PIKS_ERR_ARG, "null context");
+  drain_timing(c);
+  c->timing = on != 0;
+  return PIKS_OK;
+}
+
+piks_status piks_kernel_times(piks_ctx *c, double *out, int32_t n, int32_t reset) {
+  if (!c) return fail(PIKS_ERR_ARG, "null context");
+  drain_timing(c);
+  for (int k = 0; k < KT_N && 2 * k + 1 < n; ++k) { out[2 * k] = c->kt_ms[k]; out[2 * k + 1] = (double)c->kt_n[k]; }
+  if (reset) for (int k = 0; k < KT_N; ++k) { c->kt_ms[k] = 0; c->kt_n[k] = 0; }
+  return PIKS_OK;
+}
+
+piks_status piks_launches_per_iteration(piks_ctx *c, int64_t *n) {
+  if (!c || !n || !c->have_geometry) return fail(PIKS_ERR_STATE, "no geometry");
+  const DevState &s = c->ds;
+  int64_t k = sweep_num_diagonals(s);
+  k += (s.ncommit > 0) + 1 /*capture*/ + (int64_t)(c->geo.level_start.size() - 1) + 1 /*inlet*/ +
+       (s.nsym > 0) + (s.NF > 0);
+  *n = k;
+  return PIKS_OK;
+}
+
+piks_status piks_synchronize(piks_ctx *c) {
+  if (!c) return fail(PIKS_ERR_ARG, "null context");
+  cudaSetDevice(c->device);
+  return cuda_check(cudaStreamSynchronize(c->stream), "synchronize");
+}
+
+piks_status piks_destroy(piks_ctx *c) {
+  if (!c) return PIKS_OK;
+  if (c->device < 0) { delete c; return PIKS_OK; }
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
+  free_device(c);
+  if (c->own_stream) cudaStreamDestroy(c->own_stream);
+  delete c;
+  return PIKS_OK;
+}
+
+}  // extern "C"

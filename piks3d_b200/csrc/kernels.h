@@ -1,0 +1,56 @@
+// Device-side data of one solve and the launch wrappers of the iteration kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace piks {
+
+// Everything the kernels read, as device pointers (one struct passed by value).
+struct DevState {
+  int Nx, Ny, Nz, GX, GXY;      // interior extents; ghosted row / plane strides
+  int NF, NB, Nc8, nchunk;      // fluid nodes, solid nodes read by the solver, velocities per octant
+  const int32_t *nodemap;       // ghosted: >=0 node, -1 unread solid, -2 ghost
+  const uint8_t *label;         // ghosted labels
+  double *h;                    // [node][octant][Nc8] distribution function
+  double *fw;                   // [corner][octant][Nc8] 3-fold corner storage
+  const int32_t *bcorner;       // [NB] corner of a solid node or -1
+  const uint16_t *roles;        // [NB][8] sources seen by y1/y2/z1/z2 readers
+  double *rho, *ux, *uy, *uz;   // [NF] moments
+  const double *cx, *cy, *cz, *w;  // [Nc8]
+  double mu;                    // sqrt(pi/2)/Kn
+  double c15, c20, c05, c10;    // 1.5/ds, 2/ds, -0.5/ds, 1/ds (physicalGrid.F90:1259-1297)
+  double accom, pressDrop, DiffFlux;
+  // walls
+  int nWall;
+  const int32_t *wall_node, *wall_label, *wall_corner, *wall_nb, *wall_order;
+  const double *wall_e;
+  // post-sweep switch commits
+  int ncommit;
+  const int32_t *commit;
+  // x = 1 / x = Nx planes and the two lagged ghost planes
+  const int32_t *plane_x1, *plane_xN;
+  double *ghostW[2], *ghostE[2];  // [Ny*Nz][4][Nc8]
+  // symmetry planes
+  int nsym;
+  const int32_t *sym_node;
+  const uint8_t *sym_flag;
+  // chkConverge
+  const int32_t *flux_list;
+  int flux_groups[10];
+  double *flux_out;             // [1]
+};
+
+// Tile of the sweep: TV x TW pencils (warps) per CTA.
+constexpr int kTV = 4, kTW = 4;
+int sweep_num_diagonals(const DevState &s);
+void launch_sweep_diagonal(const DevState &s, int diag, cudaStream_t st);
+void launch_commit(const DevState &s, cudaStream_t st);
+void launch_capture(const DevState &s, int buf, cudaStream_t st);
+void launch_walls(const DevState &s, int begin, int end, int gbuf, cudaStream_t st);
+void launch_inlet_outlet(const DevState &s, int buf, cudaStream_t st);
+void launch_symmetry(const DevState &s, cudaStream_t st);
+void launch_moments(const DevState &s, cudaStream_t st);
+void launch_flux(const DevState &s, double ds, double sqrt_half, double inv_refl2, cudaStream_t st);
+void upload_tables();
+
+}  // namespace piks

@@ -1,0 +1,93 @@
+// Internal host-side structures of libpiks3d_b200 (not part of the C ABI).
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "piks3d_gpu.h"
+
+namespace piks {
+
+// Voxel labels of PIKS3D (physicalGrid.F90:127-134).
+enum : int {
+  L_FLUID = 0, L_SOLID = 1, L_GHOST = 4,
+  L_E = 20, L_W = 21, L_N = 22, L_S = 23, L_F = 24, L_B = 25,
+  L_EN = 30, L_WN = 31, L_ES = 32, L_WS = 33,
+  L_NF = 40, L_NB = 41, L_SF = 42, L_SB = 43,
+  L_EF = 50, L_EB = 51, L_WF = 52, L_WB = 53,
+  L_ENF = 60, L_WNF = 61, L_WSF = 62, L_ESF = 63,
+  L_ENB = 70, L_WNB = 71, L_WSB = 72, L_ESB = 73
+};
+
+// Fluid-side bits of a wall label: which face neighbours are fluid.
+enum : uint8_t { FACE_E = 1, FACE_W = 2, FACE_N = 4, FACE_S = 8, FACE_F = 16, FACE_B = 32 };
+uint8_t face_mask(int label);  // 0 for non-wall labels
+bool is_wall_label(int label);
+bool is_corner3_label(int label);
+
+// Octant o (0-based, the reference's group o+1) velocity signs.
+inline int oct_sx(int o) { return (o == 0 || o == 3 || o == 4 || o == 7) ? 1 : -1; }
+inline int oct_sy(int o) { return (o == 0 || o == 1 || o == 4 || o == 5) ? 1 : -1; }
+inline int oct_sz(int o) { return o < 4 ? 1 : -1; }
+
+// Source code of a resolved read: 0..7 = slot (octant) of the same node, 8 = fw(corner, o).
+constexpr int SRC_FW = 8;
+
+// Wall re-emission program (solver.F90:772-1823), shared with the device kernels.
+enum { DIR_PX, DIR_MX, DIR_PY, DIR_MY, DIR_PZ, DIR_MZ };
+enum { ST_F, ST_Z, ST_W };
+struct WFace { int dir, store; };
+struct WWrite { int dst_store, dst_o, face, src_store, src_o; };
+struct WProg { int label, nface; WFace face[3]; int nwr; WWrite wr[12]; };
+const WProg *wall_program(int label);
+extern const int kIncoming[6][4];  // 1-based octants arriving from each fluid side
+
+struct Velocity {
+  int Nc_fundamental = 0, Nc = 0, Nc8 = 0;
+  std::vector<double> cx, cy, cz, w;
+  double DiffFlux = 0.0;
+};
+
+// initParams-adjusted sizes and constants.
+struct Setup {
+  piks_params p{};
+  int Nx = 0, Ny = 0, Nz = 0;              // box after fluidlayer and block_rep
+  int Nx_base = 0, Ny_base = 0, Nz_base = 0;
+  double ds = 0.0, mu = 0.0;
+};
+
+// Compact device-side geometry produced by preprocess().
+struct Geometry {
+  int Nx = 0, Ny = 0, Nz = 0, GX = 0, GY = 0, GZ = 0;  // ghosted extents = N + 4
+  std::vector<uint8_t> label;      // ghosted labels
+  std::vector<int32_t> nodemap;    // ghosted: >= 0 node index, -1 never read, -2 ghost
+  int32_t NF = 0, NB = 0;          // nodes [0,NF) fluid (raster order), [NF,NF+NB) solid read by the solver
+  std::vector<int32_t> node_g;     // ghosted linear index of each node
+  int32_t nWall = 0, nCorner = 0;
+  std::vector<int32_t> wall_node;  // vecWall order
+  std::vector<int32_t> wall_label;
+  std::vector<double> wall_e;      // [nWall][2] extrapolation coefficients
+  std::vector<int32_t> wall_corner;
+  std::vector<int32_t> wall_nb;    // [nWall][3][2]: node at +d and code at +2d (see kernels)
+  std::vector<int32_t> wall_order; // wall indices grouped by dependency level
+  std::vector<int32_t> level_start;  // nlevels + 1 offsets into wall_order
+  std::vector<int32_t> bcorner;    // [NB] corner index or -1
+  std::vector<uint16_t> roles;     // [NB][8] 4-bit sources for reads as y1,y2,z1,z2
+  std::vector<int32_t> commit;     // triples (node, octant, src): post-sweep slot content
+  std::vector<int32_t> plane_x1, plane_xN;  // [Nz*Ny] node at x=1 / x=Nx or -1
+  std::vector<int32_t> sym_node;   // nodes on the y/z boundary planes
+  std::vector<uint8_t> sym_flag;   // bit0 y=1, bit1 y=Ny, bit2 z=1, bit3 z=Nz
+  std::vector<int32_t> flux_list;  // x=2 plane entries in chkConverge's summation order
+  int32_t flux_groups[10] = {0};   // offsets of the 9 partial sums
+  int64_t ghost_index(int i, int j, int k) const {
+    return (int64_t)(i + 1) + (int64_t)(j + 1) * GX + (int64_t)(k + 1) * GX * GY;
+  }
+};
+
+piks_status make_setup(const piks_params &p, Setup &s, std::string &err);
+piks_status make_velocity(const piks_params &p, Velocity &v, std::string &err);
+piks_status preprocess(const Setup &s, const uint8_t *raw, int64_t nbytes, Geometry &g, std::string &err);
+piks_status read_namelist(const char *path, piks_params &p, std::string &image_file, std::string &err);
+std::string fortran_es15_6(double v);
+
+}  // namespace piks
