@@ -452,7 +452,10 @@ piks_status piks_run(piks_ctx *c, const char *results_path, const char *out_dir,
 }
 
 piks_status piks_geometry_array(piks_ctx *c, const char *name, void *out, int64_t capacity, int64_t *count) {
-  if (!c || !name || !c->have_host_geometry) return fail(PIKS_ERR_STATE, "no geometry");
+  if (!c || !name) return fail(PIKS_ERR_ARG, "null argument");
+  const bool velocity = !std::strcmp(name, "cx") || !std::strcmp(name, "cy") || !std::strcmp(name, "cz") ||
+                        !std::strcmp(name, "w");
+  if (!velocity && !c->have_host_geometry) return fail(PIKS_ERR_STATE, "no geometry");
   const Geometry &g = c->geo;
   const void *src = nullptr;
   size_t n = 0, esz = 0;

@@ -21,26 +21,39 @@ def centred_sphere(n=32, radius=12.0):
     return np.ascontiguousarray(solid.astype(np.uint8))
 
 
-def sphere_pack(n, porosity, rmin=4.0, rmax=8.0, seed=12345, batch=64):
-    """Boolean overlapping spheres in an n^3 box until porosity <= `porosity`."""
+def quarter_sphere(n=100, porosity=0.75):
+    """The tutorial geometry of PIKS3D's conf/createSphere.F90: a solid sphere of radius
+    floor((n-1)*((1-porosity)*3/(4*pi))^(1/3)) centred at ((n+1)/2, 1, 1), so that the
+    box holds a quarter sphere; voxel (i,j,k) 1-based is solid if its squared distance
+    to the centre is below radius^2."""
+    import math
+    r = math.floor((n - 1) * ((1.0 - porosity) * 3.0 / 4.0 / (math.atan(1.0) * 4.0)) ** (1.0 / 3.0))
+    idx = np.arange(1, n + 1, dtype=np.float64)
+    z, y, x = np.meshgrid(idx, idx, idx, indexing="ij")
+    d2 = (z - 1.0) ** 2 + (y - 1.0) ** 2 + (x - (n + 1) / 2.0) ** 2
+    return np.ascontiguousarray((d2 < r * r).astype(np.uint8))
+
+
+def sphere_pack(n, porosity, rmin=4.0, rmax=8.0, seed=12345):
+    """Boolean overlapping spheres in an n^3 box, added until porosity <= `porosity`.
+    Centres uniform in the box, radii uniform in [rmin, rmax] (numpy PCG64, `seed`)."""
     rng = np.random.default_rng(seed)
     solid = np.zeros((n, n, n), dtype=bool)
     coords = np.arange(n, dtype=np.float64) + 0.5
     target_solid = (1.0 - porosity) * n ** 3
-    count = 0
-    while solid.sum() < target_solid:
-        for _ in range(batch):
-            c = rng.uniform(0.0, n, size=3)
-            r = rng.uniform(rmin, rmax)
-            lo = np.maximum(np.floor(c - r).astype(int), 0)
-            hi = np.minimum(np.ceil(c + r).astype(int) + 1, n)
-            zz = coords[lo[2]:hi[2], None, None] - c[2]
-            yy = coords[None, lo[1]:hi[1], None] - c[1]
-            xx = coords[None, None, lo[0]:hi[0]] - c[0]
-            solid[lo[2]:hi[2], lo[1]:hi[1], lo[0]:hi[0]] |= (xx * xx + yy * yy + zz * zz) < r * r
-            count += 1
-            if solid.sum() >= target_solid:
-                break
+    nsolid = 0
+    while nsolid < target_solid:
+        c = rng.uniform(0.0, n, size=3)
+        r = rng.uniform(rmin, rmax)
+        lo = np.maximum(np.floor(c - r).astype(int), 0)
+        hi = np.minimum(np.ceil(c + r).astype(int) + 1, n)
+        zz = coords[lo[2]:hi[2], None, None] - c[2]
+        yy = coords[None, lo[1]:hi[1], None] - c[1]
+        xx = coords[None, None, lo[0]:hi[0]] - c[0]
+        ball = (xx * xx + yy * yy + zz * zz) < r * r
+        block = solid[lo[2]:hi[2], lo[1]:hi[1], lo[0]:hi[0]]
+        nsolid += int(np.count_nonzero(ball & ~block))
+        block |= ball
     return np.ascontiguousarray(solid.astype(np.uint8))
 
 

@@ -1,0 +1,145 @@
+"""CPU tests of the product's host side: C ABI exports, parameter reading, error codes,
+image preprocessing (labels identical to the oracle) and the device data flow (numpy
+model over the library's exported geometry, bit-identical to the oracle)."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import piks3d_b200 as pk
+from piks3d_b200 import images
+from conftest import ROOT, base_params
+from device_model import DeviceModel
+from oracle import Oracle
+
+
+def test_library_exports_every_declared_symbol():
+    hdr = open(os.path.join(ROOT, "include", "piks3d_gpu.h")).read()
+    names = set(re.findall(r"^\s*(?:piks_status|const char \*)\s*(piks_\w+)\s*\(", hdr, re.M))
+    assert len(names) >= 20
+    lib = ctypes.CDLL(pk.LIB_PATH)
+    missing = [n for n in sorted(names) if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_read_params_reference_format(tmp_path):
+    txt = """&physicalNml
+imageFileName = 'singleSphere100^3.raw'
+Nx = 100
+Ny = 100
+Nz = 100
+wallExtOrder = 1
+fluidLayer = 0
+Ref_L = 1.d0
+/
+
+&velocityNml
+Nc_fundamental = 4
+halfRange = T
+/
+
+&mpiNml
+mpi_xdim = 2
+mpi_ydim = 2
+mpi_zdim = 1
+/
+
+&solverNml
+maxStep = 100
+chkConvergeStep = 10
+saveStep = 50
+eps = 1.0d-7
+saveLast = T
+saveFormat = 1
+/
+
+&flowNml
+Kn = 1.0d-1
+pressDrop = 1.0d-1
+accom = 1.d0
+/
+"""
+    f = tmp_path / "para.in"
+    f.write_text(txt)
+    p, image = pk.read_params(str(f))
+    assert image == "singleSphere100^3.raw"
+    assert (p.Nx, p.Ny, p.Nz, p.wallExtOrder, p.fluidlayer) == (100, 100, 100, 1, 0)
+    assert p.Nc_fundamental == 4 and p.halfRange == 1 and p.mpi_xdim == 2
+    assert (p.maxStep, p.chkConvergeStep, p.saveStep, p.saveLast, p.saveFormat) == (100, 10, 50, 1, 1)
+    assert p.eps == 1.0e-7 and p.Kn == 0.1 and p.pressDrop == 0.1 and p.accom == 1.0
+    assert p.block_repx == 1 and p.Ref_L == 1.0
+
+
+def test_error_codes(tmp_path):
+    with pytest.raises(pk.PiksError) as e:
+        pk.read_params(str(tmp_path / "missing.in"))
+    assert e.value.status == 7
+    with pytest.raises(pk.PiksError) as e:
+        pk.Solver(base_params(8, Nc_fundamental=3), device=-1)
+    assert e.value.status == 2
+    s = pk.Solver(base_params(8), device=-1)
+    bad = np.zeros((8, 8, 8), np.uint8)
+    bad[3, 3, 3] = 7
+    with pytest.raises(pk.PiksError) as e:
+        s.setup_physical_grid(bad)
+    assert e.value.status == 3
+    with pytest.raises(pk.PiksError) as e:
+        s.setup_physical_grid(np.zeros(100, np.uint8))
+    assert e.value.status == 3
+    s.setup_physical_grid(np.zeros((8, 8, 8), np.uint8))
+    with pytest.raises(pk.PiksError) as e:
+        s.iterate(1)
+    assert e.value.status == 8
+
+
+@pytest.mark.parametrize("n,por,seed,kw", [
+    (24, 0.5, 1, {}), (20, 0.35, 2, dict(fluidlayer=2)), (18, 0.6, 3, dict(block_repx=2, block_repz=2)),
+    (16, 0.45, 4, dict(wallExtOrder=3)),
+])
+def test_preprocessing_matches_oracle(n, por, seed, kw):
+    img = images.sphere_pack(n, por, 1.2, 4.0, seed=seed)
+    p = base_params(n, **kw)
+    o = Oracle(p, img.tobytes(), nthreads=2)
+    s = pk.Solver(p, device=-1)
+    s.setup_physical_grid(img)
+    assert np.array_equal(o.labels(), s.get_labels())
+    d, inf = o.dims(), s.info()
+    assert (d["Nfluid"], d["nWall"], d["nCorner"]) == (inf["Nfluid"], inf["nWall"], inf["nCorner"])
+    # vecWall order and extrapolation coefficients
+    wn = s.geometry_array("wall_node")
+    ng = s.geometry_array("node_g")
+    assert np.array_equal(o.vecwall() - 1, ng[wn])
+    assert np.array_equal(o.extcoef().T.reshape(-1), s.geometry_array("wall_e"))
+
+
+def test_velocity_grid_matches_oracle():
+    for nc in (2, 4, 6, 8, 12, 16):
+        for half in (1, 0):
+            p = base_params(6, Nc_fundamental=nc, halfRange=half)
+            s = pk.Solver(p, device=-1)
+            o = Oracle(p, np.zeros(216, np.uint8).tobytes(), nthreads=1)
+            for a, name in zip(o.velocity(), ("cx", "cy", "cz", "w")):
+                assert np.array_equal(a, s.geometry_array(name)), (nc, half, name)
+
+
+@pytest.mark.parametrize("n,por,seed,kw", [
+    (12, 0.5, 11, dict(Kn=0.7)), (12, 0.4, 12, dict(wallExtOrder=1, accom=0.8)),
+    (11, 0.45, 13, dict(wallExtOrder=3, fluidlayer=1)), (9, 0.6, 14, dict(Nc_fundamental=4, Kn=0.3, pressDrop=0.1)),
+])
+def test_device_model_bit_exact(n, por, seed, kw):
+    img = images.sphere_pack(n, por, 1.2, 3.0, seed=seed)
+    p = base_params(n, **kw)
+    o = Oracle(p, img.tobytes(), nthreads=1)
+    s = pk.Solver(p, device=-1)
+    s.setup_physical_grid(img)
+    m = DeviceModel(s, p)
+    nodes = m.node_g
+    for _ in range(3):
+        o.iterate(1)
+        m.iterate(1)
+        fo = o.f().reshape(8, m.Nc8, -1)[:, :, nodes]
+        fm = m.f_reference_layout().reshape(8, m.Nc8, -1)[:, :, nodes]
+        assert np.array_equal(fo, fm)
+        assert o.chk_converge()[0] == m.mass_flux()
