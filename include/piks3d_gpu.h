@@ -121,6 +121,11 @@ piks_status piks_enable_timing(piks_ctx *ctx, int32_t on);
 /* Number of kernel launches one iterate issues on this context (for launch accounting). */
 piks_status piks_launches_per_iteration(piks_ctx *ctx, int64_t *n);
 
+/* Device self-test of the sweep's division (a correctly rounded reciprocal followed by one
+ * fused correction step) against IEEE division: counts differing quotients over `samples`
+ * random operand pairs. Expected 0. */
+piks_status piks_selftest_division(int32_t device, int64_t samples, uint64_t seed, int64_t *mismatches);
+
 piks_status piks_synchronize(piks_ctx *ctx);
 piks_status piks_destroy(piks_ctx *ctx);
 const char *piks_last_error(void);

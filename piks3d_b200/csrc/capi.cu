@@ -235,7 +235,9 @@ piks_status piks_setup_physical_grid(piks_ctx *c, const uint8_t *raw, int64_t nb
   DevState &s = c->ds;
   s = DevState{};
   s.Nx = g.Nx; s.Ny = g.Ny; s.Nz = g.Nz; s.GX = g.GX; s.GXY = g.GX * g.GY;
-  s.NF = g.NF; s.NB = g.NB; s.Nc8 = v.Nc8; s.nchunk = (v.Nc8 + 31) / 32;
+  s.NF = g.NF; s.NB = g.NB; s.Nc8 = v.Nc8;
+  s.vpl = v.Nc8 >= 64 ? 2 : 1;
+  s.nchunk = (v.Nc8 + 32 * s.vpl - 1) / (32 * s.vpl);
   const double ds = c->setup.ds;
   s.mu = c->setup.mu;
   s.c15 = 1.5 / ds; s.c20 = 2.0 / ds; s.c05 = -0.5 / ds; s.c10 = 1.0 / ds;
@@ -254,6 +256,23 @@ piks_status piks_setup_physical_grid(piks_ctx *c, const uint8_t *raw, int64_t nb
   UP(g.plane_x1, plane_x1, pi); UP(g.plane_xN, plane_xN, pi);
   UP(g.sym_node, sym_node, pi); UP(g.sym_flag, sym_flag, pu8);
   UP(g.flux_list, flux_list, pi);
+  {
+    // sweep denominators 0.5*mu + cx*C0x + cy*C0y + cz*C0z (solver.F90:214) by first-order
+    // class, with C0 = 1.5/ds (second order) or 1/ds (first order), and their reciprocals
+    std::vector<double> dt((size_t)8 * v.Nc8), rt((size_t)8 * v.Nc8);
+    const double c15 = 1.5 / ds, c10 = 1.0 / ds;
+    for (int cls = 0; cls < 8; ++cls)
+      for (int l = 0; l < v.Nc8; ++l) {
+        double den = 0.5 * s.mu;
+        den = den + v.cx[l] * ((cls & 1) ? c10 : c15);
+        den = den + v.cy[l] * ((cls & 2) ? c10 : c15);
+        den = den + v.cz[l] * ((cls & 4) ? c10 : c15);
+        dt[(size_t)cls * v.Nc8 + l] = den;
+        rt[(size_t)cls * v.Nc8 + l] = 1.0 / den;
+      }
+    UP(dt, dtab, pd);
+    UP(rt, rtab, pd);
+  }
 #undef UP
   s.nWall = g.nWall;
   s.ncommit = (int)(g.commit.size() / 3);
@@ -476,6 +495,21 @@ piks_status piks_geometry_array(piks_ctx *c, const char *name, void *out, int64_
     std::memcpy(out, src, n * esz);
   }
   return PIKS_OK;
+}
+
+piks_status piks_selftest_division(int32_t device, int64_t samples, uint64_t seed, int64_t *mismatches) {
+  if (!mismatches || samples <= 0) return fail(PIKS_ERR_ARG, "bad argument");
+  piks_status st = cuda_check(cudaSetDevice(device), "cudaSetDevice");
+  if (st) return st;
+  unsigned long long *d = nullptr;
+  if ((st = cuda_check(cudaMalloc(&d, sizeof(unsigned long long)), "cudaMalloc"))) return st;
+  cudaMemset(d, 0, sizeof(unsigned long long));
+  launch_division_selftest(samples, seed, d);
+  unsigned long long h = 0;
+  st = cuda_check(cudaMemcpy(&h, d, sizeof h, cudaMemcpyDeviceToHost), "selftest");
+  cudaFree(d);
+  *mismatches = (int64_t)h;
+  return st;
 }
 
 piks_status piks_set_stream(piks_ctx *c, void *stream) {

@@ -29,37 +29,45 @@ __device__ __forceinline__ int dsz(int o) { return o < 4 ? 1 : -1; }
 // octant -> slot within a ghost plane (cx>0 octants 0,3,4,7 ; cx<0 octants 1,2,5,6)
 __device__ __forceinline__ int plane_slot(int o) { return o >> 1; }
 
-// Upwind value for a y/z neighbour of a fluid node in octant o's sweep.
-//  fluid, inside this CTA's tile  -> the value computed this sweep (shared-memory ring)
-//  fluid, outside the tile        -> global h (earlier tile of this sweep, or an inflow
-//                                    boundary node whose value the BCs set)
-//  solid node read by the solver  -> the slot its reader position sees (static switch
-//                                    resolution of solver.F90:184-204 etc.)
-//  anything else                  -> 0 (ghost layers; only ever multiplied by 0)
-__device__ __forceinline__ double upwind_value(const DevState &a, int m, int o, int role, int l,
-                                               bool in_tile, const double *ring_entry) {
-  if (m >= 0 && m < a.NF) return in_tile ? *ring_entry : a.h[hidx(m, o, a.Nc8, l)];
-  if (m >= a.NF) {
-    const int b = m - a.NF;
-    const int src = (a.roles[(size_t)b * 8 + o] >> (4 * role)) & 15;
-    if (src < 8) return a.h[hidx(m, src, a.Nc8, l)];
-    return a.fw[hidx(a.bcorner[b], o, a.Nc8, l)];
-  }
-  return 0.0;
+// ---------------------------------------------------------------------------------------
+// Octant sweeps (solver.F90:176-526).
+//
+// One CTA = one tile of TV x TW pencils of one octant and one chunk of 32*VPL velocities
+// (VPL per lane). Warp (pv, pw) owns pencil (v, w) of the octant's local frame (u, v, w
+// increase along the sweep) and walks u = 1 .. Nx-1 keeping the two x-upwind values in
+// registers. Pencils advance on a diagonal schedule, pencil (pv, pw) handling u at step
+// t = u - 1 + pv + pw, so a node's y/z-upwind values inside the tile were produced one or
+// two steps earlier and sit in a 3-deep shared-memory ring. Tiles of one launch lie on one
+// anti-diagonal of the tile grid; their y/z-upwind tiles finished in earlier launches.
+//
+// Everything a step reads from global memory (node map rows, the old value, the moments,
+// upwind values that are not produced inside the tile) is fetched one step ahead, node-map
+// rows 32 positions at a time, so a step waits only for the ring and its own arithmetic.
+//
+// Arithmetic (solver.F90:206-214) in the reference's order. Written in the octant's local
+// frame every term is added with a non-negative-octant coefficient: for a negative
+// velocity axis the reference subtracts (c * -C) * f, which is bit-identical to adding
+// (c * C) * f. The coefficient products c*C and the denominators depend only on the
+// velocity and on the first/second-order flags of the three axes, so they are tabulated
+// (same operations, same rounding); the division num/den is evaluated from the correctly
+// rounded reciprocal y = RN(1/den) by Markstein's correction q = RN(q0 + RN-exact(num -
+// den*q0) * y) with q0 = RN(num*y), which returns RN(num/den) (Markstein, IBM J. Res. Dev.
+// 34 (1990); see piks_selftest_division for the check against __ddiv_rn).
+__device__ __forceinline__ double markstein_div(double num, double den, double y) {
+  const double q0 = __dmul_rn(num, y);
+  const double r = __fma_rn(-q0, den, num);
+  return __fma_rn(r, y, q0);
 }
 
-// ---------------------------------------------------------------------------------------
-// Octant sweeps (solver.F90:176-526). One CTA = one tile of TV x TW pencils of one octant
-// and one 32-velocity chunk; warp (pv, pw) owns pencil (v, w) of the octant's local frame
-// (u, v, w increase along the sweep) and walks u = 1 .. Nx-1 keeping the two x-upwind
-// values in registers. Pencils advance on a diagonal schedule, pencil (pv, pw) handling u
-// at step t = u - 1 + pv + pw, so the y/z-upwind values of a node were produced one or two
-// steps earlier and are read from a 3-deep shared-memory ring. Tiles of one launch lie on
-// one anti-diagonal of the tile grid; their y/z-upwind tiles finished in earlier launches.
-template <int TV, int TW>
-__global__ void __launch_bounds__(TV * TW * 32)
+template <int TV, int TW, int VPL>
+__global__ void __launch_bounds__(TV * TW * 32, 1)
 k_sweep(const DevState a, int diag, int ntw) {
-  __shared__ double ring[3][TV * TW][32];
+  constexpr int NP = TV * TW;
+  constexpr int NV = 32 * VPL;
+  __shared__ double ring[3][NP][VPL][32];
+  __shared__ double sP[9][NV];      // c*(2/ds), c*(1/ds), c*(-0.5/ds) for c = cx, cy, cz
+  __shared__ double sD[8][NV];      // denominators by first-order class (fx | fy<<1 | fz<<2)
+  __shared__ double sR[8][NV];      // their correctly rounded reciprocals
   const int per_tile = 8 * a.nchunk;
   const int tile = blockIdx.x / per_tile;
   const int rem = blockIdx.x - tile * per_tile;
@@ -73,15 +81,28 @@ k_sweep(const DevState a, int diag, int ntw) {
   const int v = 1 + b * TV + pv, w = 1 + c * TW + pw;
   const bool active = v <= a.Ny - 1 && w <= a.Nz - 1;
   const int Nc8 = a.Nc8;
-  const int l = chunk * 32 + lane;
-  const bool lv = l < Nc8;
-  double cxl = 0.0, cyl = 0.0, czl = 0.0, wl = 0.0;
-  if (lv) { cxl = a.cx[l]; cyl = a.cy[l]; czl = a.cz[l]; wl = a.w[l]; }
-  // signed upwind coefficients (physicalGrid.F90:1254-1622): second / first order
-  const double X0 = sx > 0 ? a.c15 : -a.c15, X1 = sx > 0 ? a.c20 : -a.c20, X2 = sx > 0 ? a.c05 : -a.c05;
-  const double Y0 = sy > 0 ? a.c15 : -a.c15, Y1 = sy > 0 ? a.c20 : -a.c20, Y2 = sy > 0 ? a.c05 : -a.c05;
-  const double Z0 = sz > 0 ? a.c15 : -a.c15, Z1 = sz > 0 ? a.c20 : -a.c20, Z2 = sz > 0 ? a.c05 : -a.c05;
-  const double XF = sx > 0 ? a.c10 : -a.c10, YF = sy > 0 ? a.c10 : -a.c10, ZF = sz > 0 ? a.c10 : -a.c10;
+  const int lbase = chunk * NV;
+  for (int e = threadIdx.x; e < NV; e += blockDim.x) {
+    const int l = lbase + e;
+    const bool ok = l < Nc8;
+    const double cx = ok ? a.cx[l] : 0.0, cy = ok ? a.cy[l] : 0.0, cz = ok ? a.cz[l] : 0.0;
+    sP[0][e] = dmul(cx, a.c20); sP[1][e] = dmul(cx, a.c10); sP[2][e] = dmul(cx, a.c05);
+    sP[3][e] = dmul(cy, a.c20); sP[4][e] = dmul(cy, a.c10); sP[5][e] = dmul(cy, a.c05);
+    sP[6][e] = dmul(cz, a.c20); sP[7][e] = dmul(cz, a.c10); sP[8][e] = dmul(cz, a.c05);
+    for (int cls = 0; cls < 8; ++cls) {
+      sD[cls][e] = ok ? a.dtab[(size_t)cls * Nc8 + l] : 1.0;
+      sR[cls][e] = ok ? a.rtab[(size_t)cls * Nc8 + l] : 1.0;
+    }
+  }
+  double cxv[VPL], cyv[VPL], czv[VPL], wv[VPL];
+  bool lv[VPL];
+#pragma unroll
+  for (int q = 0; q < VPL; ++q) {
+    const int l = lbase + q * 32 + lane;
+    lv[q] = l < Nc8;
+    cxv[q] = lv[q] ? a.cx[l] : 0.0; cyv[q] = lv[q] ? a.cy[l] : 0.0;
+    czv[q] = lv[q] ? a.cz[l] : 0.0; wv[q] = lv[q] ? a.w[l] : 0.0;
+  }
   const uint8_t xbit = sx > 0 ? FACE_E : FACE_W;
   const uint8_t ybit = sy > 0 ? FACE_N : FACE_S;
   const uint8_t zbit = sz > 0 ? FACE_F : FACE_B;
@@ -90,67 +111,152 @@ k_sweep(const DevState a, int diag, int ntw) {
   const int i0 = sx > 0 ? 1 : a.Nx;
   const long gbase = (long)(i0 + 1) + (long)(j + 1) * a.GX + (long)(k + 1) * a.GXY;
   const long SY = (long)sy * a.GX, SZ = (long)sz * a.GXY;
-  const double half_mu = dmul(0.5, a.mu);
+  const double mu = a.mu;
+  const int Nx = a.Nx;
 
-  double xm1 = 0.0, xm2 = 0.0;  // x-upwind values at u-1, u-2 (u-2 = ghost at u = 1)
+  // node-map rows of this pencil and of its y1, y2, z1, z2 neighbour pencils, 32 positions
+  // per load: lane i of the current block holds u = ub + i
+  int nm[5], lb[3], nmn[5], lbn[3];
+  auto load_block = [&](int ub, int *dn, int *dl) {
+    const int u = ub + lane;
+    if (active && u <= Nx - 1) {
+      const long g = gbase + (long)sx * u;
+      dn[0] = __ldg(a.nodemap + g);
+      dn[1] = __ldg(a.nodemap + g - SY);
+      dn[2] = __ldg(a.nodemap + g - 2 * SY);
+      dn[3] = __ldg(a.nodemap + g - SZ);
+      dn[4] = __ldg(a.nodemap + g - 2 * SZ);
+      dl[0] = __ldg(a.label + g);
+      dl[1] = __ldg(a.label + g - SY);
+      dl[2] = __ldg(a.label + g - SZ);
+    } else {
+      dn[0] = dn[1] = dn[2] = dn[3] = dn[4] = -2;
+      dl[0] = dl[1] = dl[2] = L_GHOST;
+    }
+  };
+  int ub = 0;
+  load_block(0, nm, lb);
+  load_block(32, nmn, lbn);
+
+  // state of the node at the next step (prefetched)
+  struct Next {
+    int m, lab, ring_mask;       // node, label, which of y1 y2 z1 z2 come from the ring
+    bool fy, fz;
+    double fold[VPL], st[4][VPL];  // old value (or a solid node's slot o), static upwinds
+    double rho, ux, uy, uz;
+  };
+  Next nx;
+  auto prefetch = [&](int u) {  // called by whole warps; u in [0, Nx-1]
+    if (u - ub >= 32) {  // advance the node-map block
+      ub += 32;
+#pragma unroll
+      for (int e = 0; e < 5; ++e) nm[e] = nmn[e];
+#pragma unroll
+      for (int e = 0; e < 3; ++e) lb[e] = lbn[e];
+      load_block(ub + 32, nmn, lbn);
+    }
+    const int s = u - ub;
+    const int m = __shfl_sync(0xffffffffu, nm[0], s);
+    const int my1 = __shfl_sync(0xffffffffu, nm[1], s), my2 = __shfl_sync(0xffffffffu, nm[2], s);
+    const int mz1 = __shfl_sync(0xffffffffu, nm[3], s), mz2 = __shfl_sync(0xffffffffu, nm[4], s);
+    nx.m = m;
+    nx.lab = __shfl_sync(0xffffffffu, lb[0], s);
+    nx.fy = (v == 1) || (c_face[__shfl_sync(0xffffffffu, lb[1], s)] & ybit);
+    nx.fz = (w == 1) || (c_face[__shfl_sync(0xffffffffu, lb[2], s)] & zbit);
+    const int mq[4] = {my1, my2, mz1, mz2};
+    const bool intile[4] = {pv >= 1, pv >= 2, pw >= 1, pw >= 2};
+    nx.ring_mask = 0;
+    const bool fluid = m >= 0 && m < a.NF && u >= 1;
+#pragma unroll
+    for (int q = 0; q < VPL; ++q) {
+      const int l = lbase + q * 32 + lane;
+      nx.fold[q] = (m >= 0 && lv[q]) ? __ldcg(a.h + hidx(m, o, Nc8, l)) : 0.0;
+    }
+    if (fluid) {
+      nx.rho = __ldg(a.rho + m); nx.ux = __ldg(a.ux + m); nx.uy = __ldg(a.uy + m); nx.uz = __ldg(a.uz + m);
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int mr = mq[r];
+        const bool ring_fluid = mr >= 0 && mr < a.NF && intile[r];
+        if (ring_fluid) nx.ring_mask |= 1 << r;
+#pragma unroll
+        for (int q = 0; q < VPL; ++q) {
+          const int l = lbase + q * 32 + lane;
+          double val = 0.0;
+          if (!ring_fluid && lv[q]) {
+            if (mr >= 0 && mr < a.NF) {
+              val = __ldcg(a.h + hidx(mr, o, Nc8, l));
+            } else if (mr >= a.NF) {
+              const int bb = mr - a.NF;
+              const int src = (__ldg(a.roles + (size_t)bb * 8 + o) >> (4 * r)) & 15;
+              val = src < 8 ? __ldcg(a.h + hidx(mr, src, Nc8, l)) : __ldcg(a.fw + hidx(__ldg(a.bcorner + bb), o, Nc8, l));
+            }
+          }
+          nx.st[r][q] = val;
+        }
+      }
+    }
+  };
+
+  double xm1[VPL], xm2[VPL];
   int labprev = L_GHOST;
   if (active) {
-    const int m0 = a.nodemap[gbase];
-    labprev = a.label[gbase];
-    if (m0 >= 0 && lv) xm1 = a.h[hidx(m0, o, Nc8, l)];
+    prefetch(0);
+#pragma unroll
+    for (int q = 0; q < VPL; ++q) { xm1[q] = nx.fold[q]; xm2[q] = 0.0; }
+    labprev = nx.lab;
+    prefetch(1);
+  } else {
+#pragma unroll
+    for (int q = 0; q < VPL; ++q) { xm1[q] = 0.0; xm2[q] = 0.0; }
   }
-  const int nsteps = (a.Nx - 1) + (TV - 1) + (TW - 1);
+  __syncthreads();  // tables in shared memory
+
+  const int nsteps = (Nx - 1) + (TV - 1) + (TW - 1);
   for (int t = 0; t < nsteps; ++t) {
     const int u = t - pv - pw + 1;
-    if (active && u >= 1 && u <= a.Nx - 1) {
-      const long g = gbase + (long)sx * u;
-      const int m = a.nodemap[g];
-      const int lab = a.label[g];
-      double out = 0.0;
+    if (active && u >= 1 && u <= Nx - 1) {
+      const Next cur = nx;
+      if (u + 1 <= Nx - 1) prefetch(u + 1);
+      const int m = cur.m;
+      double out[VPL];
       if (m >= 0 && m < a.NF) {
         const bool fx = (u == 1) || (c_face[labprev] & xbit);
-        const long gy1 = g - SY, gz1 = g - SZ;
-        const int my1 = a.nodemap[gy1], my2 = a.nodemap[gy1 - SY];
-        const int mz1 = a.nodemap[gz1], mz2 = a.nodemap[gz1 - SZ];
-        const bool fy = (v == 1) || (c_face[a.label[gy1]] & ybit);
-        const bool fz = (w == 1) || (c_face[a.label[gz1]] & zbit);
-        if (lv) {
-          const int p = wid;
-          const double y1 = upwind_value(a, my1, o, 0, l, pv >= 1, &ring[(t + 2) % 3][p - (pv >= 1 ? 1 : 0)][lane]);
-          const double y2 = upwind_value(a, my2, o, 1, l, pv >= 2, &ring[(t + 1) % 3][p - (pv >= 2 ? 2 : 0)][lane]);
-          const double z1 = upwind_value(a, mz1, o, 2, l, pw >= 1, &ring[(t + 2) % 3][p - (pw >= 1 ? TV : 0)][lane]);
-          const double z2 = upwind_value(a, mz2, o, 3, l, pw >= 2, &ring[(t + 1) % 3][p - (pw >= 2 ? 2 * TV : 0)][lane]);
-          const double fold = a.h[hidx(m, o, Nc8, l)];
-          // fEq = w*(Rho + (+-cx*Ux +- cy*Uy +- cz*Uz))   (solver.F90:206)
-          double ex = dmul(cxl, a.ux[m]); if (sx < 0) ex = -ex;
-          double ey = dmul(cyl, a.uy[m]); if (sy < 0) ey = -ey;
-          double ez = dmul(czl, a.uz[m]); if (sz < 0) ez = -ez;
-          const double feq = dmul(wl, dadd(a.rho[m], dadd(dadd(ex, ey), ez)));
-          // (solver.F90:207-214) a term of a negative-velocity axis is subtracted with its
-          // negative coefficient, exactly as the reference writes it
-          double num = dmul(a.mu, dsub(feq, dmul(0.5, fold)));
-          double tt;
-          tt = dmul(dmul(cxl, fx ? XF : X1), xm1);   num = sx > 0 ? dadd(num, tt) : dsub(num, tt);
-          tt = dmul(dmul(cxl, fx ? 0.0 : X2), xm2);  num = sx > 0 ? dadd(num, tt) : dsub(num, tt);
-          tt = dmul(dmul(cyl, fy ? YF : Y1), y1);    num = sy > 0 ? dadd(num, tt) : dsub(num, tt);
-          tt = dmul(dmul(cyl, fy ? 0.0 : Y2), y2);   num = sy > 0 ? dadd(num, tt) : dsub(num, tt);
-          tt = dmul(dmul(czl, fz ? ZF : Z1), z1);    num = sz > 0 ? dadd(num, tt) : dsub(num, tt);
-          tt = dmul(dmul(czl, fz ? 0.0 : Z2), z2);   num = sz > 0 ? dadd(num, tt) : dsub(num, tt);
-          double den = half_mu;
-          tt = dmul(cxl, fx ? XF : X0); den = sx > 0 ? dadd(den, tt) : dsub(den, tt);
-          tt = dmul(cyl, fy ? YF : Y0); den = sy > 0 ? dadd(den, tt) : dsub(den, tt);
-          tt = dmul(czl, fz ? ZF : Z0); den = sz > 0 ? dadd(den, tt) : dsub(den, tt);
-          out = __ddiv_rn(num, den);
-          a.h[hidx(m, o, Nc8, l)] = out;
-          ring[t % 3][p][lane] = out;
+        const int cls = (fx ? 1 : 0) | (cur.fy ? 2 : 0) | (cur.fz ? 4 : 0);
+#pragma unroll
+        for (int q = 0; q < VPL; ++q) {
+          const int e = q * 32 + lane;
+          double ex = dmul(cxv[q], cur.ux); if (sx < 0) ex = -ex;
+          double ey = dmul(cyv[q], cur.uy); if (sy < 0) ey = -ey;
+          double ez = dmul(czv[q], cur.uz); if (sz < 0) ez = -ez;
+          const double feq = dmul(wv[q], dadd(cur.rho, dadd(dadd(ex, ey), ez)));
+          double num = dmul(mu, dsub(feq, dmul(0.5, cur.fold[q])));
+          num = dadd(num, dmul(sP[fx ? 1 : 0][e], xm1[q]));
+          if (!fx) num = dadd(num, dmul(sP[2][e], xm2[q]));
+          const double y1 = (cur.ring_mask & 1) ? ring[(t + 2) % 3][wid - 1][q][lane] : cur.st[0][q];
+          num = dadd(num, dmul(sP[cur.fy ? 4 : 3][e], y1));
+          if (!cur.fy) {
+            const double y2 = (cur.ring_mask & 2) ? ring[(t + 1) % 3][wid - 2][q][lane] : cur.st[1][q];
+            num = dadd(num, dmul(sP[5][e], y2));
+          }
+          const double z1 = (cur.ring_mask & 4) ? ring[(t + 2) % 3][wid - TV][q][lane] : cur.st[2][q];
+          num = dadd(num, dmul(sP[cur.fz ? 7 : 6][e], z1));
+          if (!cur.fz) {
+            const double z2 = (cur.ring_mask & 8) ? ring[(t + 1) % 3][wid - 2 * TV][q][lane] : cur.st[3][q];
+            num = dadd(num, dmul(sP[8][e], z2));
+          }
+          out[q] = markstein_div(num, sD[cls][e], sR[cls][e]);
+          ring[t % 3][wid][q][lane] = out[q];
+          if (lv[q]) a.h[hidx(m, o, Nc8, lbase + e)] = out[q];
         }
-      } else if (m >= 0) {
-        // solid node read by the solver: x readers always see its slot o unswitched
-        if (lv) out = a.h[hidx(m, o, Nc8, l)];
+      } else {
+        // solid node read by the solver: x readers see its slot o unswitched; others 0
+#pragma unroll
+        for (int q = 0; q < VPL; ++q) out[q] = cur.fold[q];
       }
-      xm2 = xm1;
-      xm1 = out;
-      labprev = lab;
+#pragma unroll
+      for (int q = 0; q < VPL; ++q) { xm2[q] = xm1[q]; xm1[q] = out[q]; }
+      labprev = cur.lab;
     }
     __syncthreads();
   }
@@ -303,46 +409,49 @@ __global__ void k_symmetry(const DevState a) {
   if (f & 8) { hp[4 * S] = hp[0 * S]; hp[5 * S] = hp[1 * S]; hp[6 * S] = hp[2 * S]; hp[7 * S] = hp[3 * S]; }
 }
 
-// Moments Rho, Ux, Uy, Uz (solver.F90:1923-1938): one warp per fluid node stages 32
-// velocities x 8 octants in shared memory; lanes 0..3 run the four sums serially over
-// (l, octant) in the reference's order.
-constexpr int kMomWarps = 8;
+// Moments Rho, Ux, Uy, Uz (solver.F90:1923-1938). One lane per fluid node runs the four
+// sums serially over (l, octant) in the reference's order; a warp stages its 32 nodes'
+// values 8 velocities at a time in shared memory with coalesced 64-byte row loads.
+constexpr int kMomWarps = 2;
+constexpr int kMomL = 8;
+constexpr int kMomStride = 8 * kMomL + 1;  // odd stride in doubles: conflict-free lane reads
 __global__ void __launch_bounds__(kMomWarps * 32) k_moments(const DevState a) {
-  __shared__ double sm[kMomWarps][8][33];
+  __shared__ double sm[kMomWarps][32 * kMomStride];
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int node = blockIdx.x * kMomWarps + wid;
-  if (node >= a.NF) return;  // whole warp
+  const int node0 = (blockIdx.x * kMomWarps + wid) * 32;
+  if (node0 >= a.NF) return;  // whole warp
   const int Nc8 = a.Nc8;
-  double acc = 0.0;
-  for (int l0 = 0; l0 < Nc8; l0 += 32) {
-    const int l = l0 + lane;
-    for (int o = 0; o < 8; ++o) sm[wid][o][lane] = l < Nc8 ? a.h[hidx(node, o, Nc8, l)] : 0.0;
+  const int my = node0 + lane;
+  const bool valid = my < a.NF;
+  double r = 0.0, ux = 0.0, uy = 0.0, uz = 0.0;
+  double *buf = sm[wid];
+  for (int l0 = 0; l0 < Nc8; l0 += kMomL) {
+    // 32 nodes x 8 octants rows of kMomL values; lane group g (4 groups of 8 lanes) loads a row
+    const int sub = lane & 7, grp = lane >> 3;
+    for (int row = grp; row < 32 * 8; row += 4) {
+      const int nn = row >> 3, o = row & 7;
+      const int node = node0 + nn;
+      double val = 0.0;
+      if (node < a.NF && l0 + sub < Nc8) val = __ldcs(a.h + hidx(node, o, Nc8, l0 + sub));
+      buf[nn * kMomStride + o * kMomL + sub] = val;
+    }
     __syncwarp();
-    if (lane < 4) {
-      const int nl = min(32, Nc8 - l0);
-      for (int s = 0; s < nl; ++s) {
-        const double f1 = sm[wid][0][s], f2 = sm[wid][1][s], f3 = sm[wid][2][s], f4 = sm[wid][3][s];
-        const double f5 = sm[wid][4][s], f6 = sm[wid][5][s], f7 = sm[wid][6][s], f8 = sm[wid][7][s];
-        if (lane == 0) {
-          acc = dadd(dadd(dadd(dadd(dadd(dadd(dadd(dadd(acc, f1), f2), f3), f4), f5), f6), f7), f8);
-        } else if (lane == 1) {
-          const double d = dadd(dsub(dsub(dadd(dadd(dsub(dsub(f1, f2), f3), f4), f5), f6), f7), f8);
-          acc = dadd(acc, dmul(a.cx[l0 + s], d));
-        } else if (lane == 2) {
-          const double d = dsub(dsub(dadd(dadd(dsub(dsub(dadd(f1, f2), f3), f4), f5), f6), f7), f8);
-          acc = dadd(acc, dmul(a.cy[l0 + s], d));
-        } else {
-          const double d = dsub(dsub(dsub(dsub(dadd(dadd(dadd(f1, f2), f3), f4), f5), f6), f7), f8);
-          acc = dadd(acc, dmul(a.cz[l0 + s], d));
-        }
-      }
+    const int nl = min(kMomL, Nc8 - l0);
+    const double *mine = buf + lane * kMomStride;
+    for (int s = 0; s < nl; ++s) {
+      const double f1 = mine[0 * kMomL + s], f2 = mine[1 * kMomL + s], f3 = mine[2 * kMomL + s], f4 = mine[3 * kMomL + s];
+      const double f5 = mine[4 * kMomL + s], f6 = mine[5 * kMomL + s], f7 = mine[6 * kMomL + s], f8 = mine[7 * kMomL + s];
+      r = dadd(dadd(dadd(dadd(dadd(dadd(dadd(dadd(r, f1), f2), f3), f4), f5), f6), f7), f8);
+      const double dx = dadd(dsub(dsub(dadd(dadd(dsub(dsub(f1, f2), f3), f4), f5), f6), f7), f8);
+      const double dy = dsub(dsub(dadd(dadd(dsub(dsub(dadd(f1, f2), f3), f4), f5), f6), f7), f8);
+      const double dz = dsub(dsub(dsub(dsub(dadd(dadd(dadd(f1, f2), f3), f4), f5), f6), f7), f8);
+      ux = dadd(ux, dmul(__ldg(a.cx + l0 + s), dx));
+      uy = dadd(uy, dmul(__ldg(a.cy + l0 + s), dy));
+      uz = dadd(uz, dmul(__ldg(a.cz + l0 + s), dz));
     }
     __syncwarp();
   }
-  if (lane == 0) a.rho[node] = acc;
-  else if (lane == 1) a.ux[node] = acc;
-  else if (lane == 2) a.uy[node] = acc;
-  else if (lane == 3) a.uz[node] = acc;
+  if (valid) { a.rho[my] = r; a.ux[my] = ux; a.uy[my] = uy; a.uz[my] = uz; }
 }
 
 // Mass flux through x = 2 (output.F90:90-142) in the reference's summation order; one
@@ -370,7 +479,42 @@ __global__ void k_flux(const DevState a, double ds, double sqrt_half, double inv
 
 inline unsigned blocks_for(size_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
 
+// Self-test of markstein_div against __ddiv_rn: numerators and denominators spread over
+// 2^-40 .. 2^40 with random mantissas (splitmix64), plus denominators in the range the
+// sweep uses.
+__device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+__device__ __forceinline__ double random_double(uint64_t r, int emin, int erange) {
+  const uint64_t mant = r & ((1ull << 52) - 1);
+  const int e = emin + (int)((r >> 52) % (uint64_t)erange);
+  const uint64_t bits = ((uint64_t)(e + 1023) << 52) | mant;
+  double d = __longlong_as_double((long long)bits);
+  return (r >> 63) ? -d : d;
+}
+__global__ void k_division_selftest(int64_t samples, uint64_t seed, unsigned long long *mismatches) {
+  unsigned long long bad = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < samples; i += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t r1 = splitmix64(seed ^ (uint64_t)(2 * i)), r2 = splitmix64(seed ^ (uint64_t)(2 * i + 1));
+    const double num = random_double(r1, -40, 80);
+    double den = random_double(r2, -40, 80);
+    if (i & 1) den = fabs(random_double(r2, -2, 9));  // 0.25 .. 128: the sweep's range
+    const double y = __ddiv_rn(1.0, den);
+    const double q = markstein_div(num, den, y);
+    const double ref = __ddiv_rn(num, den);
+    if (__double_as_longlong(q) != __double_as_longlong(ref)) ++bad;
+  }
+  if (bad) atomicAdd(mismatches, bad);
+}
+
 }  // namespace
+
+void launch_division_selftest(int64_t samples, uint64_t seed, unsigned long long *mismatches) {
+  k_division_selftest<<<148 * 8, 256>>>(samples, seed, mismatches);
+}
 
 void upload_tables() {
   uint8_t face[128];
@@ -400,7 +544,10 @@ void launch_sweep_diagonal(const DevState &s, int diag, cudaStream_t st) {
   const int bhi = diag < ntv - 1 ? diag : ntv - 1;
   const int ntiles = bhi - blo + 1;
   if (ntiles <= 0) return;
-  k_sweep<kTV, kTW><<<ntiles * 8 * s.nchunk, kTV * kTW * 32, 0, st>>>(s, diag, ntw);
+  if (s.vpl == 2)
+    k_sweep<kTV, kTW, 2><<<ntiles * 8 * s.nchunk, kTV * kTW * 32, 0, st>>>(s, diag, ntw);
+  else
+    k_sweep<kTV, kTW, 1><<<ntiles * 8 * s.nchunk, kTV * kTW * 32, 0, st>>>(s, diag, ntw);
 }
 
 void launch_commit(const DevState &s, cudaStream_t st) {
@@ -427,7 +574,7 @@ void launch_symmetry(const DevState &s, cudaStream_t st) {
 
 void launch_moments(const DevState &s, cudaStream_t st) {
   if (s.NF == 0) return;
-  k_moments<<<blocks_for((size_t)s.NF, kMomWarps), kMomWarps * 32, 0, st>>>(s);
+  k_moments<<<blocks_for((size_t)s.NF, kMomWarps * 32), kMomWarps * 32, 0, st>>>(s);
 }
 
 void launch_walls(const DevState &s, int begin, int end, int gbuf, cudaStream_t st) {

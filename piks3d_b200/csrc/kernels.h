@@ -8,7 +8,7 @@ namespace piks {
 // Everything the kernels read, as device pointers (one struct passed by value).
 struct DevState {
   int Nx, Ny, Nz, GX, GXY;      // interior extents; ghosted row / plane strides
-  int NF, NB, Nc8, nchunk;      // fluid nodes, solid nodes read by the solver, velocities per octant
+  int NF, NB, Nc8, nchunk, vpl; // fluid nodes, read solid nodes, velocities per octant, sweep chunks, velocities per lane
   const int32_t *nodemap;       // ghosted: >=0 node, -1 unread solid, -2 ghost
   const uint8_t *label;         // ghosted labels
   double *h;                    // [node][octant][Nc8] distribution function
@@ -20,6 +20,7 @@ struct DevState {
   double mu;                    // sqrt(pi/2)/Kn
   double c15, c20, c05, c10;    // 1.5/ds, 2/ds, -0.5/ds, 1/ds (physicalGrid.F90:1259-1297)
   double accom, pressDrop, DiffFlux;
+  const double *dtab, *rtab;    // [8][Nc8] sweep denominators by first-order class, reciprocals
   // walls
   int nWall;
   const int32_t *wall_node, *wall_label, *wall_corner, *wall_nb, *wall_order;
@@ -52,5 +53,6 @@ void launch_symmetry(const DevState &s, cudaStream_t st);
 void launch_moments(const DevState &s, cudaStream_t st);
 void launch_flux(const DevState &s, double ds, double sqrt_half, double inv_refl2, cudaStream_t st);
 void upload_tables();
+void launch_division_selftest(int64_t samples, uint64_t seed, unsigned long long *mismatches);
 
 }  // namespace piks

@@ -98,3 +98,32 @@ def test_run_writes_reference_files(tmp_path):
         for nm in names:
             assert (odir / nm).read_text() == (sdir / nm).read_text(), nm
     s.close()
+
+
+def test_sweep_division_matches_ieee():
+    """The sweep divides with a correctly rounded reciprocal and one fused correction
+    (Markstein); it must return exactly the IEEE quotient."""
+    import ctypes
+    lib = pk.load_library()
+    lib.piks_selftest_division.argtypes = [ctypes.c_int32, ctypes.c_int64, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int64)]
+    bad = ctypes.c_int64(-1)
+    assert lib.piks_selftest_division(0, 1 << 28, 12345, ctypes.byref(bad)) == 0
+    assert bad.value == 0
+
+
+def test_tutorial_case_trace_matches_golden():
+    """The reference's shipped tutorial (tutorials/cubicSpherePacking: 100^3 quarter
+    sphere, 512 velocities, Kn = 0.1, first-order wall extrapolation, 100 steps) run
+    through the C ABI reproduces the oracle's committed chkConverge trace exactly."""
+    import json
+    import os
+    from conftest import ROOT
+    tr = json.load(open(os.path.join(ROOT, "tests", "golden", "oracle_traces.json")))["tutorial_cubicSpherePacking"]
+    p = pk.default_params(**{k: v for k, v in tr["params"].items()})
+    s = pk.Solver(p, device=0)
+    s.setup_physical_grid(images.quarter_sphere(100, 0.75))
+    for step, mass, perm, err in tr["checks"]:
+        s.iterate(p.chkConvergeStep)
+        m, k, e = s.chk_converge()
+        assert (repr(m), repr(k), repr(e)) == (mass, perm, err), step
+    s.close()
