@@ -236,7 +236,7 @@ piks_status piks_setup_physical_grid(piks_ctx *c, const uint8_t *raw, int64_t nb
   s = DevState{};
   s.Nx = g.Nx; s.Ny = g.Ny; s.Nz = g.Nz; s.GX = g.GX; s.GXY = g.GX * g.GY;
   s.NF = g.NF; s.NB = g.NB; s.Nc8 = v.Nc8;
-  s.vpl = v.Nc8 >= 64 ? 2 : 1;
+  s.vpl = (v.Nc8 % 64 == 0) ? 2 : 1;
   s.nchunk = (v.Nc8 + 32 * s.vpl - 1) / (32 * s.vpl);
   const double ds = c->setup.ds;
   s.mu = c->setup.mu;

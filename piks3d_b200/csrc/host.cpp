@@ -415,7 +415,8 @@ piks_status preprocess(const Setup &s, const uint8_t *raw, int64_t nbytes, Geome
   g.NF = 0;
   for (int32_t gi : g.node_g) if (g.label[gi] == L_FLUID) g.NF++;
   g.NB = (int32_t)g.node_g.size() - g.NF;
-  if ((int64_t)g.node_g.size() >= (int64_t)1 << 31) { err = "image too large"; return PIKS_ERR_ARG; }
+  // node*8 + slot codes of the sweep must stay below 2^30
+  if ((int64_t)g.node_g.size() * 8 >= (int64_t)1 << 30) { err = "image too large (more than 2^27 nodes read by the solver)"; return PIKS_ERR_ARG; }
 
   // walls in raster (vecWall) order, 3-fold corners numbered in the same order
   g.wall_node.clear(); g.wall_label.clear(); g.wall_corner.clear(); g.wall_e.clear(); g.wall_nb.clear();

@@ -59,15 +59,47 @@ __device__ __forceinline__ double markstein_div(double num, double den, double y
   return __fma_rn(r, y, q0);
 }
 
-template <int TV, int TW, int VPL>
+// Asynchronous global->shared copies (cp.async): 16-byte L2-only and 8-byte variants.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Where a fluid node's y1/y2/z1/z2 upwind value comes from, resolved when the node-map
+// block is loaded: kSrcRing (fluid node of this tile: shared ring), kSrcZero (ghost layer,
+// only ever multiplied by 0), or a static slot: node*8 + slot of h, or with kSrcFw set,
+// corner*8 + octant of fw (a wall slot as switched in the reference, solver.F90:184-204).
+constexpr int kSrcRing = -1, kSrcZero = -2, kSrcFw = 1 << 30;
+
+template <int TV, int TW, int VPL, int D>
+struct SweepSmem {
+  static constexpr int NP = TV * TW, NV = 32 * VPL;
+  double ring[3][NP][NV];
+  double P[9][NV];            // c*(2/ds), c*(1/ds), c*(-0.5/ds) for c = cx, cy, cz
+  double Dn[8][NV];           // denominators by first-order class (fx | fy<<1 | fz<<2)
+  double Rc[8][NV];           // their correctly rounded reciprocals
+  struct Stage {
+    double fold[NV];          // old value of the node (or slot o of a solid node)
+    double st[4][NV];         // static upwind values (y1, y2, z1, z2)
+    double mom[4];            // Rho, Ux, Uy, Uz
+  } pipe[NP][D];
+  int meta[NP][D][2];         // node, flags (fy, fz, label<<8, source kinds <<16)
+};
+
+template <int TV, int TW, int VPL, int D>
 __global__ void __launch_bounds__(TV * TW * 32, 1)
 k_sweep(const DevState a, int diag, int ntw) {
-  constexpr int NP = TV * TW;
-  constexpr int NV = 32 * VPL;
-  __shared__ double ring[3][NP][VPL][32];
-  __shared__ double sP[9][NV];      // c*(2/ds), c*(1/ds), c*(-0.5/ds) for c = cx, cy, cz
-  __shared__ double sD[8][NV];      // denominators by first-order class (fx | fy<<1 | fz<<2)
-  __shared__ double sR[8][NV];      // their correctly rounded reciprocals
+  using SM = SweepSmem<TV, TW, VPL, D>;
+  constexpr int NV = SM::NV;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  SM &S = *reinterpret_cast<SM *>(smem_raw);
   const int per_tile = 8 * a.nchunk;
   const int tile = blockIdx.x / per_tile;
   const int rem = blockIdx.x - tile * per_tile;
@@ -86,23 +118,25 @@ k_sweep(const DevState a, int diag, int ntw) {
     const int l = lbase + e;
     const bool ok = l < Nc8;
     const double cx = ok ? a.cx[l] : 0.0, cy = ok ? a.cy[l] : 0.0, cz = ok ? a.cz[l] : 0.0;
-    sP[0][e] = dmul(cx, a.c20); sP[1][e] = dmul(cx, a.c10); sP[2][e] = dmul(cx, a.c05);
-    sP[3][e] = dmul(cy, a.c20); sP[4][e] = dmul(cy, a.c10); sP[5][e] = dmul(cy, a.c05);
-    sP[6][e] = dmul(cz, a.c20); sP[7][e] = dmul(cz, a.c10); sP[8][e] = dmul(cz, a.c05);
+    S.P[0][e] = dmul(cx, a.c20); S.P[1][e] = dmul(cx, a.c10); S.P[2][e] = dmul(cx, a.c05);
+    S.P[3][e] = dmul(cy, a.c20); S.P[4][e] = dmul(cy, a.c10); S.P[5][e] = dmul(cy, a.c05);
+    S.P[6][e] = dmul(cz, a.c20); S.P[7][e] = dmul(cz, a.c10); S.P[8][e] = dmul(cz, a.c05);
     for (int cls = 0; cls < 8; ++cls) {
-      sD[cls][e] = ok ? a.dtab[(size_t)cls * Nc8 + l] : 1.0;
-      sR[cls][e] = ok ? a.rtab[(size_t)cls * Nc8 + l] : 1.0;
+      S.Dn[cls][e] = ok ? a.dtab[(size_t)cls * Nc8 + l] : 1.0;
+      S.Rc[cls][e] = ok ? a.rtab[(size_t)cls * Nc8 + l] : 1.0;
     }
   }
+  // this lane's velocities: e = lane*VPL + q (contiguous pairs for 16-byte copies)
   double cxv[VPL], cyv[VPL], czv[VPL], wv[VPL];
   bool lv[VPL];
 #pragma unroll
   for (int q = 0; q < VPL; ++q) {
-    const int l = lbase + q * 32 + lane;
+    const int l = lbase + lane * VPL + q;
     lv[q] = l < Nc8;
     cxv[q] = lv[q] ? a.cx[l] : 0.0; cyv[q] = lv[q] ? a.cy[l] : 0.0;
     czv[q] = lv[q] ? a.cz[l] : 0.0; wv[q] = lv[q] ? a.w[l] : 0.0;
   }
+  const bool lane_ok = lv[0];  // VPL = 2 is used only when Nc8 is a multiple of 64
   const uint8_t xbit = sx > 0 ? FACE_E : FACE_W;
   const uint8_t ybit = sy > 0 ? FACE_N : FACE_S;
   const uint8_t zbit = sz > 0 ? FACE_F : FACE_B;
@@ -113,102 +147,99 @@ k_sweep(const DevState a, int diag, int ntw) {
   const long SY = (long)sy * a.GX, SZ = (long)sz * a.GXY;
   const double mu = a.mu;
   const int Nx = a.Nx;
+  const bool intile[4] = {pv >= 1, pv >= 2, pw >= 1, pw >= 2};
 
-  // node-map rows of this pencil and of its y1, y2, z1, z2 neighbour pencils, 32 positions
-  // per load: lane i of the current block holds u = ub + i
-  int nm[5], lb[3], nmn[5], lbn[3];
-  auto load_block = [&](int ub, int *dn, int *dl) {
-    const int u = ub + lane;
-    if (active && u <= Nx - 1) {
-      const long g = gbase + (long)sx * u;
-      dn[0] = __ldg(a.nodemap + g);
-      dn[1] = __ldg(a.nodemap + g - SY);
-      dn[2] = __ldg(a.nodemap + g - 2 * SY);
-      dn[3] = __ldg(a.nodemap + g - SZ);
-      dn[4] = __ldg(a.nodemap + g - 2 * SZ);
-      dl[0] = __ldg(a.label + g);
-      dl[1] = __ldg(a.label + g - SY);
-      dl[2] = __ldg(a.label + g - SZ);
-    } else {
-      dn[0] = dn[1] = dn[2] = dn[3] = dn[4] = -2;
-      dl[0] = dl[1] = dl[2] = L_GHOST;
+  // Node-map block: lane i describes position u = ub + i of this pencil: node, label,
+  // whether y1/z1 face the node (first-order flags), and the four upwind sources.
+  struct Block { int m, flags, src[4]; };
+  auto load_block = [&](int ubase, Block &B) {
+    const int u = ubase + lane;
+    B.m = -2; B.flags = 0;
+    B.src[0] = B.src[1] = B.src[2] = B.src[3] = kSrcZero;
+    if (!active || u > Nx - 1) return;
+    const long g = gbase + (long)sx * u;
+    B.m = __ldg(a.nodemap + g);
+    const int lab = __ldg(a.label + g);
+    const bool fy = (v == 1) || (c_face[__ldg(a.label + g - SY)] & ybit);
+    const bool fz = (w == 1) || (c_face[__ldg(a.label + g - SZ)] & zbit);
+    B.flags = (fy ? 1 : 0) | (fz ? 2 : 0) | (lab << 8);
+    if (!(B.m >= 0 && B.m < a.NF) || u < 1) return;
+    const long gq[4] = {g - SY, g - 2 * SY, g - SZ, g - 2 * SZ};
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int mr = __ldg(a.nodemap + gq[r]);
+      int code = kSrcZero;
+      if (mr >= 0 && mr < a.NF) {
+        code = intile[r] ? kSrcRing : mr * 8 + o;
+      } else if (mr >= a.NF) {
+        const int bb = mr - a.NF;
+        const int src = (__ldg(a.roles + (size_t)bb * 8 + o) >> (4 * r)) & 15;
+        code = src < 8 ? mr * 8 + src : (kSrcFw | (__ldg(a.bcorner + bb) * 8 + o));
+      }
+      B.src[r] = code;
     }
   };
+  Block cur, nxt;
   int ub = 0;
-  load_block(0, nm, lb);
-  load_block(32, nmn, lbn);
+  load_block(0, cur);
+  load_block(32, nxt);
 
-  // state of the node at the next step (prefetched)
-  struct Next {
-    int m, lab, ring_mask;       // node, label, which of y1 y2 z1 z2 come from the ring
-    bool fy, fz;
-    double fold[VPL], st[4][VPL];  // old value (or a solid node's slot o), static upwinds
-    double rho, ux, uy, uz;
-  };
-  Next nx;
-  auto prefetch = [&](int u) {  // called by whole warps; u in [0, Nx-1]
-    if (u - ub >= 32) {  // advance the node-map block
-      ub += 32;
+  // Issue the copies of position ui into pipeline stage ui % D (one commit group).
+  auto issue = [&](int ui) {
+    if (ui <= Nx - 1) {
+      if (ui - ub >= 32) {
+        ub += 32;
+        cur = nxt;
+        load_block(ub + 32, nxt);
+      }
+      const int s = ui - ub;
+      const int m = __shfl_sync(0xffffffffu, cur.m, s);
+      const int fl = __shfl_sync(0xffffffffu, cur.flags, s);
+      int src[4];
 #pragma unroll
-      for (int e = 0; e < 5; ++e) nm[e] = nmn[e];
+      for (int r = 0; r < 4; ++r) src[r] = __shfl_sync(0xffffffffu, cur.src[r], s);
+      const int slot = ui % D;
+      typename SM::Stage &st = S.pipe[wid][slot];
+      int kinds = 0;
 #pragma unroll
-      for (int e = 0; e < 3; ++e) lb[e] = lbn[e];
-      load_block(ub + 32, nmn, lbn);
-    }
-    const int s = u - ub;
-    const int m = __shfl_sync(0xffffffffu, nm[0], s);
-    const int my1 = __shfl_sync(0xffffffffu, nm[1], s), my2 = __shfl_sync(0xffffffffu, nm[2], s);
-    const int mz1 = __shfl_sync(0xffffffffu, nm[3], s), mz2 = __shfl_sync(0xffffffffu, nm[4], s);
-    nx.m = m;
-    nx.lab = __shfl_sync(0xffffffffu, lb[0], s);
-    nx.fy = (v == 1) || (c_face[__shfl_sync(0xffffffffu, lb[1], s)] & ybit);
-    nx.fz = (w == 1) || (c_face[__shfl_sync(0xffffffffu, lb[2], s)] & zbit);
-    const int mq[4] = {my1, my2, mz1, mz2};
-    const bool intile[4] = {pv >= 1, pv >= 2, pw >= 1, pw >= 2};
-    nx.ring_mask = 0;
-    const bool fluid = m >= 0 && m < a.NF && u >= 1;
+      for (int r = 0; r < 4; ++r) kinds |= (src[r] == kSrcRing ? 1 : src[r] == kSrcZero ? 2 : 0) << (2 * r);
+      if (lane == 0) { S.meta[wid][slot][0] = m; S.meta[wid][slot][1] = fl | (kinds << 16); }
+      if (m >= 0 && lane_ok) {
+        const double *gp = a.h + hidx(m, o, Nc8, lbase + lane * VPL);
+        if (VPL == 2) cp_async16(&st.fold[lane * 2], gp); else cp_async8(&st.fold[lane], gp);
+      }
+      if (m >= 0 && m < a.NF && ui >= 1) {
+        if (lane < 4) {
+          const double *mp = lane == 0 ? a.rho : lane == 1 ? a.ux : lane == 2 ? a.uy : a.uz;
+          cp_async8(&st.mom[lane], mp + m);
+        }
 #pragma unroll
-    for (int q = 0; q < VPL; ++q) {
-      const int l = lbase + q * 32 + lane;
-      nx.fold[q] = (m >= 0 && lv[q]) ? __ldcg(a.h + hidx(m, o, Nc8, l)) : 0.0;
-    }
-    if (fluid) {
-      nx.rho = __ldg(a.rho + m); nx.ux = __ldg(a.ux + m); nx.uy = __ldg(a.uy + m); nx.uz = __ldg(a.uz + m);
-#pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        const int mr = mq[r];
-        const bool ring_fluid = mr >= 0 && mr < a.NF && intile[r];
-        if (ring_fluid) nx.ring_mask |= 1 << r;
-#pragma unroll
-        for (int q = 0; q < VPL; ++q) {
-          const int l = lbase + q * 32 + lane;
-          double val = 0.0;
-          if (!ring_fluid && lv[q]) {
-            if (mr >= 0 && mr < a.NF) {
-              val = __ldcg(a.h + hidx(mr, o, Nc8, l));
-            } else if (mr >= a.NF) {
-              const int bb = mr - a.NF;
-              const int src = (__ldg(a.roles + (size_t)bb * 8 + o) >> (4 * r)) & 15;
-              val = src < 8 ? __ldcg(a.h + hidx(mr, src, Nc8, l)) : __ldcg(a.fw + hidx(__ldg(a.bcorner + bb), o, Nc8, l));
-            }
-          }
-          nx.st[r][q] = val;
+        for (int r = 0; r < 4; ++r) {
+          if (src[r] < 0 || !lane_ok) continue;
+          const double *gp = (src[r] & kSrcFw) ? a.fw + (size_t)(src[r] & ~kSrcFw) * Nc8
+                                               : a.h + (size_t)src[r] * Nc8;
+          gp += lbase + lane * VPL;
+          if (VPL == 2) cp_async16(&st.st[r][lane * 2], gp); else cp_async8(&st.st[r][lane], gp);
         }
       }
     }
+    cp_async_commit();
   };
 
   double xm1[VPL], xm2[VPL];
+#pragma unroll
+  for (int q = 0; q < VPL; ++q) { xm1[q] = 0.0; xm2[q] = 0.0; }
   int labprev = L_GHOST;
   if (active) {
-    prefetch(0);
+    issue(0);
+    cp_async_wait<0>();
+    __syncwarp();
+    const int m0 = S.meta[wid][0][0];
 #pragma unroll
-    for (int q = 0; q < VPL; ++q) { xm1[q] = nx.fold[q]; xm2[q] = 0.0; }
-    labprev = nx.lab;
-    prefetch(1);
-  } else {
-#pragma unroll
-    for (int q = 0; q < VPL; ++q) { xm1[q] = 0.0; xm2[q] = 0.0; }
+    for (int q = 0; q < VPL; ++q) xm1[q] = (m0 >= 0) ? S.pipe[wid][0].fold[lane * VPL + q] : 0.0;
+    labprev = S.meta[wid][0][1] >> 8 & 0xff;
+    __syncwarp();
+    for (int ui = 1; ui < D; ++ui) issue(ui);
   }
   __syncthreads();  // tables in shared memory
 
@@ -216,51 +247,67 @@ k_sweep(const DevState a, int diag, int ntw) {
   for (int t = 0; t < nsteps; ++t) {
     const int u = t - pv - pw + 1;
     if (active && u >= 1 && u <= Nx - 1) {
-      const Next cur = nx;
-      if (u + 1 <= Nx - 1) prefetch(u + 1);
-      const int m = cur.m;
+      issue(u + D - 1);
+      cp_async_wait<D - 1>();
+      __syncwarp();
+      const int slot = u % D;
+      const typename SM::Stage &st = S.pipe[wid][slot];
+      const int m = S.meta[wid][slot][0];
+      const int fl = S.meta[wid][slot][1];
       double out[VPL];
       if (m >= 0 && m < a.NF) {
         const bool fx = (u == 1) || (c_face[labprev] & xbit);
-        const int cls = (fx ? 1 : 0) | (cur.fy ? 2 : 0) | (cur.fz ? 4 : 0);
+        const bool fy = fl & 1, fz = fl & 2;
+        const int kinds = fl >> 16;
+        const int cls = (fx ? 1 : 0) | (fy ? 2 : 0) | (fz ? 4 : 0);
+        const double rho = st.mom[0], ux = st.mom[1], uy = st.mom[2], uz = st.mom[3];
 #pragma unroll
         for (int q = 0; q < VPL; ++q) {
-          const int e = q * 32 + lane;
-          double ex = dmul(cxv[q], cur.ux); if (sx < 0) ex = -ex;
-          double ey = dmul(cyv[q], cur.uy); if (sy < 0) ey = -ey;
-          double ez = dmul(czv[q], cur.uz); if (sz < 0) ez = -ez;
-          const double feq = dmul(wv[q], dadd(cur.rho, dadd(dadd(ex, ey), ez)));
-          double num = dmul(mu, dsub(feq, dmul(0.5, cur.fold[q])));
-          num = dadd(num, dmul(sP[fx ? 1 : 0][e], xm1[q]));
-          if (!fx) num = dadd(num, dmul(sP[2][e], xm2[q]));
-          const double y1 = (cur.ring_mask & 1) ? ring[(t + 2) % 3][wid - 1][q][lane] : cur.st[0][q];
-          num = dadd(num, dmul(sP[cur.fy ? 4 : 3][e], y1));
-          if (!cur.fy) {
-            const double y2 = (cur.ring_mask & 2) ? ring[(t + 1) % 3][wid - 2][q][lane] : cur.st[1][q];
-            num = dadd(num, dmul(sP[5][e], y2));
+          const int e = lane * VPL + q;
+          double ex = dmul(cxv[q], ux); if (sx < 0) ex = -ex;
+          double ey = dmul(cyv[q], uy); if (sy < 0) ey = -ey;
+          double ez = dmul(czv[q], uz); if (sz < 0) ez = -ez;
+          const double feq = dmul(wv[q], dadd(rho, dadd(dadd(ex, ey), ez)));
+          double num = dmul(mu, dsub(feq, dmul(0.5, st.fold[e])));
+          num = dadd(num, dmul(S.P[fx ? 1 : 0][e], xm1[q]));
+          if (!fx) num = dadd(num, dmul(S.P[2][e], xm2[q]));
+          double up[4];
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            const int kd = (kinds >> (2 * r)) & 3;
+            const int pn = wid - (r == 0 ? 1 : r == 1 ? 2 : r == 2 ? TV : 2 * TV);
+            const int rs = (r == 0 || r == 2) ? (t + 2) % 3 : (t + 1) % 3;
+            up[r] = kd == 1 ? S.ring[rs][pn][e] : kd == 2 ? 0.0 : st.st[r][e];
           }
-          const double z1 = (cur.ring_mask & 4) ? ring[(t + 2) % 3][wid - TV][q][lane] : cur.st[2][q];
-          num = dadd(num, dmul(sP[cur.fz ? 7 : 6][e], z1));
-          if (!cur.fz) {
-            const double z2 = (cur.ring_mask & 8) ? ring[(t + 1) % 3][wid - 2 * TV][q][lane] : cur.st[3][q];
-            num = dadd(num, dmul(sP[8][e], z2));
-          }
-          out[q] = markstein_div(num, sD[cls][e], sR[cls][e]);
-          ring[t % 3][wid][q][lane] = out[q];
-          if (lv[q]) a.h[hidx(m, o, Nc8, lbase + e)] = out[q];
+          num = dadd(num, dmul(S.P[fy ? 4 : 3][e], up[0]));
+          if (!fy) num = dadd(num, dmul(S.P[5][e], up[1]));
+          num = dadd(num, dmul(S.P[fz ? 7 : 6][e], up[2]));
+          if (!fz) num = dadd(num, dmul(S.P[8][e], up[3]));
+          out[q] = markstein_div(num, S.Dn[cls][e], S.Rc[cls][e]);
+          S.ring[t % 3][wid][e] = out[q];
+        }
+        if (lane_ok) {
+          double *hp = a.h + hidx(m, o, Nc8, lbase + lane * VPL);
+          if (VPL == 2) *reinterpret_cast<double2 *>(hp) = make_double2(out[0], out[VPL - 1]);
+          else hp[0] = out[0];
         }
       } else {
         // solid node read by the solver: x readers see its slot o unswitched; others 0
 #pragma unroll
-        for (int q = 0; q < VPL; ++q) out[q] = cur.fold[q];
+        for (int q = 0; q < VPL; ++q) out[q] = (m >= 0) ? st.fold[lane * VPL + q] : 0.0;
       }
 #pragma unroll
       for (int q = 0; q < VPL; ++q) { xm2[q] = xm1[q]; xm1[q] = out[q]; }
-      labprev = cur.lab;
+      labprev = fl >> 8 & 0xff;
+      __syncwarp();
     }
     __syncthreads();
   }
+  cp_async_wait<0>();
 }
+
+template <int TV, int TW, int VPL, int D>
+size_t sweep_smem_bytes() { return sizeof(SweepSmem<TV, TW, VPL, D>); }
 
 // Post-sweep content of switched wall slots: slot o of a wall ends the reference's sweep
 // holding the last value switched into it (z-upwind reader, else y-upwind reader).
@@ -538,16 +585,28 @@ int sweep_num_diagonals(const DevState &s) {
   return ntv + ntw - 1;
 }
 
+constexpr int kStages = 4;
+
 void launch_sweep_diagonal(const DevState &s, int diag, cudaStream_t st) {
   const int ntv = (s.Ny - 1 + kTV - 1) / kTV, ntw = (s.Nz - 1 + kTW - 1) / kTW;
   const int blo = diag - (ntw - 1) > 0 ? diag - (ntw - 1) : 0;
   const int bhi = diag < ntv - 1 ? diag : ntv - 1;
   const int ntiles = bhi - blo + 1;
   if (ntiles <= 0) return;
+  static unsigned long long configured = 0;  // one bit per device
+  const size_t sm2 = sweep_smem_bytes<kTV, kTW, 2, kStages>();
+  const size_t sm1 = sweep_smem_bytes<kTV, kTW, 1, kStages>();
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!(configured >> (dev & 63) & 1ull)) {
+    cudaFuncSetAttribute(k_sweep<kTV, kTW, 2, kStages>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2);
+    cudaFuncSetAttribute(k_sweep<kTV, kTW, 1, kStages>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
+    configured |= 1ull << (dev & 63);
+  }
   if (s.vpl == 2)
-    k_sweep<kTV, kTW, 2><<<ntiles * 8 * s.nchunk, kTV * kTW * 32, 0, st>>>(s, diag, ntw);
+    k_sweep<kTV, kTW, 2, kStages><<<ntiles * 8 * s.nchunk, kTV * kTW * 32, sm2, st>>>(s, diag, ntw);
   else
-    k_sweep<kTV, kTW, 1><<<ntiles * 8 * s.nchunk, kTV * kTW * 32, 0, st>>>(s, diag, ntw);
+    k_sweep<kTV, kTW, 1, kStages><<<ntiles * 8 * s.nchunk, kTV * kTW * 32, sm1, st>>>(s, diag, ntw);
 }
 
 void launch_commit(const DevState &s, cudaStream_t st) {
