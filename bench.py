@@ -291,7 +291,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-iters", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--n", type=int, default=None,
+                    help="image edge (default 128); smaller edges are for profiling captures, not bench lines")
     args = ap.parse_args()
+    if args.n:
+        WORKLOAD["n"] = args.n
     world, rank, local = dist_setup(args)
     try:
         if args.impl == "reference":

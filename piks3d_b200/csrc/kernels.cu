@@ -82,7 +82,6 @@ template <int TV, int TW, int VPL, int D>
 struct SweepSmem {
   static constexpr int NP = TV * TW, NV = 32 * VPL;
   double ring[3][NP][NV];
-  double P[9][NV];            // c*(2/ds), c*(1/ds), c*(-0.5/ds) for c = cx, cy, cz
   double Dn[8][NV];           // denominators by first-order class (fx | fy<<1 | fz<<2)
   double Rc[8][NV];           // their correctly rounded reciprocals
   struct Stage {
@@ -90,9 +89,11 @@ struct SweepSmem {
     double st[4][NV];         // static upwind values (y1, y2, z1, z2)
     double mom[4];            // Rho, Ux, Uy, Uz
   } pipe[NP][D];
-  int meta[NP][D][2];         // node, flags (fy, fz, label<<8, source kinds <<16)
+  int meta[NP][D][2];         // node, flags
 };
 
+// flags of a pencil position: bit 0 fy, bit 1 fz (first order in y / z), bits 2..5 which
+// of y1, y2, z1, z2 come from the ring, bits 8..15 the voxel label.
 template <int TV, int TW, int VPL, int D>
 __global__ void __launch_bounds__(TV * TW * 32, 1)
 k_sweep(const DevState a, int diag, int ntw) {
@@ -117,24 +118,28 @@ k_sweep(const DevState a, int diag, int ntw) {
   for (int e = threadIdx.x; e < NV; e += blockDim.x) {
     const int l = lbase + e;
     const bool ok = l < Nc8;
-    const double cx = ok ? a.cx[l] : 0.0, cy = ok ? a.cy[l] : 0.0, cz = ok ? a.cz[l] : 0.0;
-    S.P[0][e] = dmul(cx, a.c20); S.P[1][e] = dmul(cx, a.c10); S.P[2][e] = dmul(cx, a.c05);
-    S.P[3][e] = dmul(cy, a.c20); S.P[4][e] = dmul(cy, a.c10); S.P[5][e] = dmul(cy, a.c05);
-    S.P[6][e] = dmul(cz, a.c20); S.P[7][e] = dmul(cz, a.c10); S.P[8][e] = dmul(cz, a.c05);
     for (int cls = 0; cls < 8; ++cls) {
       S.Dn[cls][e] = ok ? a.dtab[(size_t)cls * Nc8 + l] : 1.0;
       S.Rc[cls][e] = ok ? a.rtab[(size_t)cls * Nc8 + l] : 1.0;
     }
   }
-  // this lane's velocities: e = lane*VPL + q (contiguous pairs for 16-byte copies)
-  double cxv[VPL], cyv[VPL], czv[VPL], wv[VPL];
+  // this lane's velocities: e = lane*VPL + q (contiguous pairs for 16-byte copies).
+  // fEq needs +-c*U: multiplying by the signed velocity component rounds identically.
+  double scx[VPL], scy[VPL], scz[VPL], wv[VPL];
+  double px2[VPL], px1[VPL], pxh[VPL], py2[VPL], py1[VPL], pyh[VPL], pz2[VPL], pz1[VPL], pzh[VPL];
   bool lv[VPL];
 #pragma unroll
   for (int q = 0; q < VPL; ++q) {
     const int l = lbase + lane * VPL + q;
     lv[q] = l < Nc8;
-    cxv[q] = lv[q] ? a.cx[l] : 0.0; cyv[q] = lv[q] ? a.cy[l] : 0.0;
-    czv[q] = lv[q] ? a.cz[l] : 0.0; wv[q] = lv[q] ? a.w[l] : 0.0;
+    const double cx = lv[q] ? a.cx[l] : 0.0, cy = lv[q] ? a.cy[l] : 0.0, cz = lv[q] ? a.cz[l] : 0.0;
+    scx[q] = sx > 0 ? cx : -cx; scy[q] = sy > 0 ? cy : -cy; scz[q] = sz > 0 ? cz : -cz;
+    wv[q] = lv[q] ? a.w[l] : 0.0;
+    // coefficient products c*C of the upwind terms: second-order C1 = 2/ds, first-order
+    // C1 = 1/ds, second-order C2 = -0.5/ds (physicalGrid.F90:1259-1297)
+    px2[q] = dmul(cx, a.c20); px1[q] = dmul(cx, a.c10); pxh[q] = dmul(cx, a.c05);
+    py2[q] = dmul(cy, a.c20); py1[q] = dmul(cy, a.c10); pyh[q] = dmul(cy, a.c05);
+    pz2[q] = dmul(cz, a.c20); pz1[q] = dmul(cz, a.c10); pzh[q] = dmul(cz, a.c05);
   }
   const bool lane_ok = lv[0];  // VPL = 2 is used only when Nc8 is a multiple of 64
   const uint8_t xbit = sx > 0 ? FACE_E : FACE_W;
@@ -149,8 +154,7 @@ k_sweep(const DevState a, int diag, int ntw) {
   const int Nx = a.Nx;
   const bool intile[4] = {pv >= 1, pv >= 2, pw >= 1, pw >= 2};
 
-  // Node-map block: lane i describes position u = ub + i of this pencil: node, label,
-  // whether y1/z1 face the node (first-order flags), and the four upwind sources.
+  // Node-map block: lane i describes position u = ub + i of this pencil.
   struct Block { int m, flags, src[4]; };
   auto load_block = [&](int ubase, Block &B) {
     const int u = ubase + lane;
@@ -162,22 +166,25 @@ k_sweep(const DevState a, int diag, int ntw) {
     const int lab = __ldg(a.label + g);
     const bool fy = (v == 1) || (c_face[__ldg(a.label + g - SY)] & ybit);
     const bool fz = (w == 1) || (c_face[__ldg(a.label + g - SZ)] & zbit);
-    B.flags = (fy ? 1 : 0) | (fz ? 2 : 0) | (lab << 8);
-    if (!(B.m >= 0 && B.m < a.NF) || u < 1) return;
-    const long gq[4] = {g - SY, g - 2 * SY, g - SZ, g - 2 * SZ};
+    int fl = (fy ? 1 : 0) | (fz ? 2 : 0) | (lab << 8);
+    if (B.m >= 0 && B.m < a.NF && u >= 1) {
+      const long gq[4] = {g - SY, g - 2 * SY, g - SZ, g - 2 * SZ};
 #pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      const int mr = __ldg(a.nodemap + gq[r]);
-      int code = kSrcZero;
-      if (mr >= 0 && mr < a.NF) {
-        code = intile[r] ? kSrcRing : mr * 8 + o;
-      } else if (mr >= a.NF) {
-        const int bb = mr - a.NF;
-        const int src = (__ldg(a.roles + (size_t)bb * 8 + o) >> (4 * r)) & 15;
-        code = src < 8 ? mr * 8 + src : (kSrcFw | (__ldg(a.bcorner + bb) * 8 + o));
+      for (int r = 0; r < 4; ++r) {
+        const int mr = __ldg(a.nodemap + gq[r]);
+        int code = kSrcZero;
+        if (mr >= 0 && mr < a.NF) {
+          if (intile[r]) { code = kSrcRing; fl |= 4 << r; }
+          else code = mr * 8 + o;
+        } else if (mr >= a.NF) {
+          const int bb = mr - a.NF;
+          const int src = (__ldg(a.roles + (size_t)bb * 8 + o) >> (4 * r)) & 15;
+          code = src < 8 ? mr * 8 + src : (kSrcFw | (__ldg(a.bcorner + bb) * 8 + o));
+        }
+        B.src[r] = code;
       }
-      B.src[r] = code;
     }
+    B.flags = fl;
   };
   Block cur, nxt;
   int ub = 0;
@@ -195,15 +202,9 @@ k_sweep(const DevState a, int diag, int ntw) {
       const int s = ui - ub;
       const int m = __shfl_sync(0xffffffffu, cur.m, s);
       const int fl = __shfl_sync(0xffffffffu, cur.flags, s);
-      int src[4];
-#pragma unroll
-      for (int r = 0; r < 4; ++r) src[r] = __shfl_sync(0xffffffffu, cur.src[r], s);
       const int slot = ui % D;
       typename SM::Stage &st = S.pipe[wid][slot];
-      int kinds = 0;
-#pragma unroll
-      for (int r = 0; r < 4; ++r) kinds |= (src[r] == kSrcRing ? 1 : src[r] == kSrcZero ? 2 : 0) << (2 * r);
-      if (lane == 0) { S.meta[wid][slot][0] = m; S.meta[wid][slot][1] = fl | (kinds << 16); }
+      if (lane == 0) { S.meta[wid][slot][0] = m; S.meta[wid][slot][1] = fl; }
       if (m >= 0 && lane_ok) {
         const double *gp = a.h + hidx(m, o, Nc8, lbase + lane * VPL);
         if (VPL == 2) cp_async16(&st.fold[lane * 2], gp); else cp_async8(&st.fold[lane], gp);
@@ -215,9 +216,9 @@ k_sweep(const DevState a, int diag, int ntw) {
         }
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
-          if (src[r] < 0 || !lane_ok) continue;
-          const double *gp = (src[r] & kSrcFw) ? a.fw + (size_t)(src[r] & ~kSrcFw) * Nc8
-                                               : a.h + (size_t)src[r] * Nc8;
+          const int sr = __shfl_sync(0xffffffffu, cur.src[r], s);
+          if (sr < 0 || !lane_ok) continue;
+          const double *gp = (sr & kSrcFw) ? a.fw + (size_t)(sr & ~kSrcFw) * Nc8 : a.h + (size_t)sr * Nc8;
           gp += lbase + lane * VPL;
           if (VPL == 2) cp_async16(&st.st[r][lane * 2], gp); else cp_async8(&st.st[r][lane], gp);
         }
@@ -225,10 +226,17 @@ k_sweep(const DevState a, int diag, int ntw) {
     }
     cp_async_commit();
   };
+  // mu*(fEq - 0.5*f) of the node in a stage (solver.F90:206-207), computed one step ahead
+  auto base_of = [&](const typename SM::Stage &st, int q) {
+    const int e = lane * VPL + q;
+    const double ex = dmul(scx[q], st.mom[1]), ey = dmul(scy[q], st.mom[2]), ez = dmul(scz[q], st.mom[3]);
+    const double feq = dmul(wv[q], dadd(st.mom[0], dadd(dadd(ex, ey), ez)));
+    return dmul(mu, dsub(feq, dmul(0.5, st.fold[e])));
+  };
 
-  double xm1[VPL], xm2[VPL];
+  double xm1[VPL], xm2[VPL], base[VPL];
 #pragma unroll
-  for (int q = 0; q < VPL; ++q) { xm1[q] = 0.0; xm2[q] = 0.0; }
+  for (int q = 0; q < VPL; ++q) { xm1[q] = 0.0; xm2[q] = 0.0; base[q] = 0.0; }
   int labprev = L_GHOST;
   if (active) {
     issue(0);
@@ -240,6 +248,12 @@ k_sweep(const DevState a, int diag, int ntw) {
     labprev = S.meta[wid][0][1] >> 8 & 0xff;
     __syncwarp();
     for (int ui = 1; ui < D; ++ui) issue(ui);
+    cp_async_wait<D - 2>();  // position 1 landed
+    __syncwarp();
+    if (S.meta[wid][1 % D][0] >= 0 && S.meta[wid][1 % D][0] < a.NF) {
+#pragma unroll
+      for (int q = 0; q < VPL; ++q) base[q] = base_of(S.pipe[wid][1 % D], q);
+    }
   }
   __syncthreads();  // tables in shared memory
 
@@ -248,7 +262,7 @@ k_sweep(const DevState a, int diag, int ntw) {
     const int u = t - pv - pw + 1;
     if (active && u >= 1 && u <= Nx - 1) {
       issue(u + D - 1);
-      cp_async_wait<D - 1>();
+      cp_async_wait<D - 2>();  // positions <= u + 1 landed
       __syncwarp();
       const int slot = u % D;
       const typename SM::Stage &st = S.pipe[wid][slot];
@@ -258,31 +272,24 @@ k_sweep(const DevState a, int diag, int ntw) {
       if (m >= 0 && m < a.NF) {
         const bool fx = (u == 1) || (c_face[labprev] & xbit);
         const bool fy = fl & 1, fz = fl & 2;
-        const int kinds = fl >> 16;
         const int cls = (fx ? 1 : 0) | (fy ? 2 : 0) | (fz ? 4 : 0);
-        const double rho = st.mom[0], ux = st.mom[1], uy = st.mom[2], uz = st.mom[3];
 #pragma unroll
         for (int q = 0; q < VPL; ++q) {
           const int e = lane * VPL + q;
-          double ex = dmul(cxv[q], ux); if (sx < 0) ex = -ex;
-          double ey = dmul(cyv[q], uy); if (sy < 0) ey = -ey;
-          double ez = dmul(czv[q], uz); if (sz < 0) ez = -ez;
-          const double feq = dmul(wv[q], dadd(rho, dadd(dadd(ex, ey), ez)));
-          double num = dmul(mu, dsub(feq, dmul(0.5, st.fold[e])));
-          num = dadd(num, dmul(S.P[fx ? 1 : 0][e], xm1[q]));
-          if (!fx) num = dadd(num, dmul(S.P[2][e], xm2[q]));
-          double up[4];
-#pragma unroll
-          for (int r = 0; r < 4; ++r) {
-            const int kd = (kinds >> (2 * r)) & 3;
-            const int pn = wid - (r == 0 ? 1 : r == 1 ? 2 : r == 2 ? TV : 2 * TV);
-            const int rs = (r == 0 || r == 2) ? (t + 2) % 3 : (t + 1) % 3;
-            up[r] = kd == 1 ? S.ring[rs][pn][e] : kd == 2 ? 0.0 : st.st[r][e];
+          double num = dadd(base[q], dmul(fx ? px1[q] : px2[q], xm1[q]));
+          if (!fx) num = dadd(num, dmul(pxh[q], xm2[q]));
+          const double y1 = (fl & 4) ? S.ring[(t + 2) % 3][wid - 1][e] : st.st[0][e];
+          num = dadd(num, dmul(fy ? py1[q] : py2[q], y1));
+          if (!fy) {
+            const double y2 = (fl & 8) ? S.ring[(t + 1) % 3][wid - 2][e] : st.st[1][e];
+            num = dadd(num, dmul(pyh[q], y2));
           }
-          num = dadd(num, dmul(S.P[fy ? 4 : 3][e], up[0]));
-          if (!fy) num = dadd(num, dmul(S.P[5][e], up[1]));
-          num = dadd(num, dmul(S.P[fz ? 7 : 6][e], up[2]));
-          if (!fz) num = dadd(num, dmul(S.P[8][e], up[3]));
+          const double z1 = (fl & 16) ? S.ring[(t + 2) % 3][wid - TV][e] : st.st[2][e];
+          num = dadd(num, dmul(fz ? pz1[q] : pz2[q], z1));
+          if (!fz) {
+            const double z2 = (fl & 32) ? S.ring[(t + 1) % 3][wid - 2 * TV][e] : st.st[3][e];
+            num = dadd(num, dmul(pzh[q], z2));
+          }
           out[q] = markstein_div(num, S.Dn[cls][e], S.Rc[cls][e]);
           S.ring[t % 3][wid][e] = out[q];
         }
@@ -299,6 +306,15 @@ k_sweep(const DevState a, int diag, int ntw) {
 #pragma unroll
       for (int q = 0; q < VPL; ++q) { xm2[q] = xm1[q]; xm1[q] = out[q]; }
       labprev = fl >> 8 & 0xff;
+      // next position's base while this step's results drain
+      if (u + 1 <= Nx - 1) {
+        const int sn = (u + 1) % D;
+        const int mn = S.meta[wid][sn][0];
+        if (mn >= 0 && mn < a.NF) {
+#pragma unroll
+          for (int q = 0; q < VPL; ++q) base[q] = base_of(S.pipe[wid][sn], q);
+        }
+      }
       __syncwarp();
     }
     __syncthreads();
