@@ -211,6 +211,7 @@ class Solver:
         return f, fw[: inf["nCorner"] * inf["Nc8"] * 8]
 
     _GEO_DTYPES = {"label": np.uint8, "sym_flag": np.uint8, "roles": np.uint16, "wall_e": np.float64,
+                   "hyper_start": np.int64,
                    "cx": np.float64, "cy": np.float64, "cz": np.float64, "w": np.float64}
 
     def geometry_array(self, name):

@@ -136,10 +136,10 @@ void enqueue_iteration(piks_ctx *c) {
   cudaStream_t st = c->stream;
   const int n = c->iStep + 1;          // the iteration being run (1-based)
   const int cap = n & 1, prev = (n - 1) & 1;
-  const int nd = sweep_num_diagonals(s);
   {
     Timed t(c, KT_SWEEP);
-    for (int d = 0; d < nd; ++d) launch_sweep_diagonal(s, d, st);
+    const auto &hs = c->geo.hyper_start;
+    for (size_t h = 0; h + 1 < hs.size(); ++h) launch_sweep_hyperplane(s, hs[h], hs[h + 1] - hs[h], st);
   }
   { Timed t(c, KT_COMMIT); launch_commit(s, st); }
   { Timed t(c, KT_CAPTURE); launch_capture(s, cap, st); }
@@ -236,8 +236,8 @@ piks_status piks_setup_physical_grid(piks_ctx *c, const uint8_t *raw, int64_t nb
   s = DevState{};
   s.Nx = g.Nx; s.Ny = g.Ny; s.Nz = g.Nz; s.GX = g.GX; s.GXY = g.GX * g.GY;
   s.NF = g.NF; s.NB = g.NB; s.Nc8 = v.Nc8;
-  s.vpl = (v.Nc8 % 64 == 0) ? 2 : 1;
-  s.nchunk = (v.Nc8 + 32 * s.vpl - 1) / (32 * s.vpl);
+  s.lpt = v.Nc8 >= 32 ? 32 : 8;   // lanes per sweep task (2 velocities per lane when 32)
+  s.nchunk = s.lpt == 32 ? (v.Nc8 + 63) / 64 : (v.Nc8 + 7) / 8;
   const double ds = c->setup.ds;
   s.mu = c->setup.mu;
   s.c15 = 1.5 / ds; s.c20 = 2.0 / ds; s.c05 = -0.5 / ds; s.c10 = 1.0 / ds;
@@ -257,21 +257,29 @@ piks_status piks_setup_physical_grid(piks_ctx *c, const uint8_t *raw, int64_t nb
   UP(g.sym_node, sym_node, pi); UP(g.sym_flag, sym_flag, pu8);
   UP(g.flux_list, flux_list, pi);
   {
-    // sweep denominators 0.5*mu + cx*C0x + cy*C0y + cz*C0z (solver.F90:214) by first-order
-    // class, with C0 = 1.5/ds (second order) or 1/ds (first order), and their reciprocals
-    std::vector<double> dt((size_t)8 * v.Nc8), rt((size_t)8 * v.Nc8);
-    const double c15 = 1.5 / ds, c10 = 1.0 / ds;
-    for (int cls = 0; cls < 8; ++cls)
-      for (int l = 0; l < v.Nc8; ++l) {
+    // per-velocity sweep constants: cx cy cz w; the products c*C of the upwind terms
+    // (C1 = 2/ds second order, 1/ds first order; C2 = -0.5/ds) for x, y, z; the
+    // denominators 0.5*mu + cx*C0x + cy*C0y + cz*C0z (solver.F90:214) by first-order
+    // class (C0 = 1.5/ds or 1/ds) and their correctly rounded reciprocals
+    std::vector<double> vt((size_t)kVtab * v.Nc8);
+    const double c15 = 1.5 / ds, c20 = 2.0 / ds, c05 = -0.5 / ds, c10 = 1.0 / ds;
+    for (int l = 0; l < v.Nc8; ++l) {
+      double *t = &vt[(size_t)l * kVtab];
+      t[0] = v.cx[l]; t[1] = v.cy[l]; t[2] = v.cz[l]; t[3] = v.w[l];
+      t[4] = v.cx[l] * c20; t[5] = v.cx[l] * c10; t[6] = v.cx[l] * c05;
+      t[7] = v.cy[l] * c20; t[8] = v.cy[l] * c10; t[9] = v.cy[l] * c05;
+      t[10] = v.cz[l] * c20; t[11] = v.cz[l] * c10; t[12] = v.cz[l] * c05;
+      for (int cls = 0; cls < 8; ++cls) {
         double den = 0.5 * s.mu;
         den = den + v.cx[l] * ((cls & 1) ? c10 : c15);
         den = den + v.cy[l] * ((cls & 2) ? c10 : c15);
         den = den + v.cz[l] * ((cls & 4) ? c10 : c15);
-        dt[(size_t)cls * v.Nc8 + l] = den;
-        rt[(size_t)cls * v.Nc8 + l] = 1.0 / den;
+        t[13 + cls] = den;
+        t[21 + cls] = 1.0 / den;
       }
-    UP(dt, dtab, pd);
-    UP(rt, rtab, pd);
+    }
+    UP(vt, vtab, pd);
+    UP(g.tasks, tasks, pi);
   }
 #undef UP
   s.nWall = g.nWall;
@@ -485,7 +493,7 @@ piks_status piks_geometry_array(piks_ctx *c, const char *name, void *out, int64_
   ARR("wall_nb", g.wall_nb) ARR("wall_order", g.wall_order) ARR("level_start", g.level_start)
   ARR("bcorner", g.bcorner) ARR("roles", g.roles) ARR("commit", g.commit) ARR("plane_x1", g.plane_x1)
   ARR("plane_xN", g.plane_xN) ARR("sym_node", g.sym_node) ARR("sym_flag", g.sym_flag)
-  ARR("flux_list", g.flux_list) ARR("cx", c->vel.cx) ARR("cy", c->vel.cy) ARR("cz", c->vel.cz) ARR("w", c->vel.w)
+  ARR("flux_list", g.flux_list) ARR("tasks", g.tasks) ARR("hyper_start", g.hyper_start) ARR("cx", c->vel.cx) ARR("cy", c->vel.cy) ARR("cz", c->vel.cz) ARR("w", c->vel.w)
 #undef ARR
   if (nm == "flux_groups") { src = g.flux_groups; n = 10; esz = sizeof(int32_t); }
   if (!esz) return fail(PIKS_ERR_ARG, "unknown geometry array " + nm);
@@ -536,7 +544,8 @@ piks_status piks_kernel_times(piks_ctx *c, double *out, int32_t n, int32_t reset
 piks_status piks_launches_per_iteration(piks_ctx *c, int64_t *n) {
   if (!c || !n || !c->have_geometry) return fail(PIKS_ERR_STATE, "no geometry");
   const DevState &s = c->ds;
-  int64_t k = sweep_num_diagonals(s);
+  int64_t k = 0;
+  for (size_t h = 0; h + 1 < c->geo.hyper_start.size(); ++h) k += c->geo.hyper_start[h + 1] > c->geo.hyper_start[h];
   k += (s.ncommit > 0) + 1 /*capture*/ + (int64_t)(c->geo.level_start.size() - 1) + 1 /*inlet*/ +
        (s.nsym > 0) + (s.NF > 0);
   *n = k;

@@ -542,6 +542,59 @@ piks_status preprocess(const Setup &s, const uint8_t *raw, int64_t nbytes, Geome
     }
   }
 
+  // Sweep tasks ordered by hyperplane (see Geometry::tasks).
+  {
+    const int nhyper = (Nx - 1) + (Ny - 1) + (Nz - 1) - 2;  // u+v+w from 3 to Nx+Ny+Nz-3
+    std::vector<int64_t> count(nhyper + 1, 0);
+    auto local = [&](int i, int n, int sgn) { return sgn > 0 ? i - 1 : n - i; };
+    auto upwind_code = [&](int i, int j, int k, int o, int role, bool first_order_zero) -> int32_t {
+      // role: 0/1 x1/x2 (slot o as is), 2..5 y1, y2, z1, z2 (resolved switch roles)
+      if (first_order_zero) return -2;
+      if (!real(i, j, k)) return -2;
+      const int32_t n = g.nodemap[g.ghost_index(i, j, k)];
+      if (n < 0) return -2;  // never read with a non-zero coefficient
+      if (n < g.NF) return n * 8 + o;
+      if (role < 2) return n * 8 + o;
+      const int src = (g.roles[(size_t)(n - g.NF) * 8 + o] >> (4 * (role - 2))) & 15;
+      if (src < 8) return n * 8 + src;
+      return (int32_t)(1 << 30) | (g.bcorner[n - g.NF] * 8 + o);
+    };
+    for (int pass = 0; pass < 2; ++pass) {
+      std::vector<int64_t> fillpos;
+      if (pass == 1) {
+        g.hyper_start.assign(nhyper + 1, 0);
+        for (int h = 0; h < nhyper; ++h) g.hyper_start[h + 1] = g.hyper_start[h] + count[h];
+        g.tasks.assign((size_t)g.hyper_start[nhyper] * 8, 0);
+        fillpos.assign(g.hyper_start.begin(), g.hyper_start.end() - 1);
+      }
+      for (int o = 0; o < 8; ++o) {
+        const int sx = oct_sx(o), sy = oct_sy(o), sz = oct_sz(o);
+        for (int k = 1; k <= Nz; ++k)
+          for (int j = 1; j <= Ny; ++j)
+            for (int i = 1; i <= Nx; ++i) {
+              if (LAB(i, j, k) != L_FLUID) continue;
+              const int u = local(i, Nx, sx), v = local(j, Ny, sy), w = local(k, Nz, sz);
+              if (u < 1 || v < 1 || w < 1) continue;  // inflow planes are not swept
+              const int h = u + v + w - 3;
+              if (pass == 0) { count[h]++; continue; }
+              // first-order flags (physicalGrid.F90:1269-1298 and the seven sibling blocks)
+              const bool fx = (u == 1) || (face_mask(LAB(i - sx, j, k)) & (sx > 0 ? FACE_E : FACE_W));
+              const bool fy = (v == 1) || (face_mask(LAB(i, j - sy, k)) & (sy > 0 ? FACE_N : FACE_S));
+              const bool fz = (w == 1) || (face_mask(LAB(i, j, k - sz)) & (sz > 0 ? FACE_F : FACE_B));
+              int32_t *t = &g.tasks[(size_t)fillpos[h]++ * 8];
+              t[0] = g.nodemap[g.ghost_index(i, j, k)];
+              t[1] = o | (fx ? 8 : 0) | (fy ? 16 : 0) | (fz ? 32 : 0);
+              t[2] = upwind_code(i - sx, j, k, o, 0, false);
+              t[3] = upwind_code(i - 2 * sx, j, k, o, 1, fx);
+              t[4] = upwind_code(i, j - sy, k, o, 2, false);
+              t[5] = upwind_code(i, j - 2 * sy, k, o, 3, fy);
+              t[6] = upwind_code(i, j, k - sz, o, 4, false);
+              t[7] = upwind_code(i, j, k - 2 * sz, o, 5, fz);
+            }
+      }
+    }
+  }
+
   // x = 1 / x = Nx planes (inlet/outlet targets and halo sources), symmetry planes
   g.plane_x1.assign((size_t)Ny * Nz, -1);
   g.plane_xN.assign((size_t)Ny * Nz, -1);

@@ -32,298 +32,97 @@ __device__ __forceinline__ int plane_slot(int o) { return o >> 1; }
 // ---------------------------------------------------------------------------------------
 // Octant sweeps (solver.F90:176-526).
 //
-// One CTA = one tile of TV x TW pencils of one octant and one chunk of 32*VPL velocities
-// (VPL per lane). Warp (pv, pw) owns pencil (v, w) of the octant's local frame (u, v, w
-// increase along the sweep) and walks u = 1 .. Nx-1 keeping the two x-upwind values in
-// registers. Pencils advance on a diagonal schedule, pencil (pv, pw) handling u at step
-// t = u - 1 + pv + pw, so a node's y/z-upwind values inside the tile were produced one or
-// two steps earlier and sit in a 3-deep shared-memory ring. Tiles of one launch lie on one
-// anti-diagonal of the tile grid; their y/z-upwind tiles finished in earlier launches.
+// In octant o's frame (u, v, w increase along the sweep) a node depends on the nodes one
+// and two cells upwind along each axis, so all swept nodes with the same u+v+w are
+// independent, for all eight octants at once. The host lists one task per (swept fluid
+// node, octant) ordered by that hyperplane index; one launch runs one hyperplane. A task
+// is a warp-sized group of lanes over the octant's velocities; every value it reads was
+// written by an earlier launch (or is a boundary value the sweep never writes), so the
+// loads of a task are independent and the warp issues them all before any arithmetic.
 //
-// Everything a step reads from global memory (node map rows, the old value, the moments,
-// upwind values that are not produced inside the tile) is fetched one step ahead, node-map
-// rows 32 positions at a time, so a step waits only for the ring and its own arithmetic.
-//
-// Arithmetic (solver.F90:206-214) in the reference's order. Written in the octant's local
-// frame every term is added with a non-negative-octant coefficient: for a negative
-// velocity axis the reference subtracts (c * -C) * f, which is bit-identical to adding
-// (c * C) * f. The coefficient products c*C and the denominators depend only on the
-// velocity and on the first/second-order flags of the three axes, so they are tabulated
-// (same operations, same rounding); the division num/den is evaluated from the correctly
-// rounded reciprocal y = RN(1/den) by Markstein's correction q = RN(q0 + RN-exact(num -
-// den*q0) * y) with q0 = RN(num*y), which returns RN(num/den) (Markstein, IBM J. Res. Dev.
-// 34 (1990); see piks_selftest_division for the check against __ddiv_rn).
+// Arithmetic (solver.F90:206-214) in the reference's order. In the octant's frame every
+// upwind term is added with the coefficient of the positive-velocity octant: for a
+// negative velocity axis the reference subtracts (c * -C) * f, which is bit-identical to
+// adding (c * C) * f, and fEq's +-c*U equals the product with the signed component. The
+// denominators depend only on the velocity and the first/second-order class, so they
+// are tabulated with the same operations; the division num/den is evaluated from the
+// correctly rounded reciprocal y = RN(1/den) by Markstein's correction
+// q = RN(q0 + RN-exact(num - den*q0) * y), q0 = RN(num*y), which returns RN(num/den)
+// (Markstein, IBM J. Res. Dev. 34 (1990); piks_selftest_division checks it).
 __device__ __forceinline__ double markstein_div(double num, double den, double y) {
   const double q0 = __dmul_rn(num, y);
   const double r = __fma_rn(-q0, den, num);
   return __fma_rn(r, y, q0);
 }
 
-// Asynchronous global->shared copies (cp.async): 16-byte L2-only and 8-byte variants.
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+constexpr int kFwBit = 1 << 30;
 
-// Where a fluid node's y1/y2/z1/z2 upwind value comes from, resolved when the node-map
-// block is loaded: kSrcRing (fluid node of this tile: shared ring), kSrcZero (ghost layer,
-// only ever multiplied by 0), or a static slot: node*8 + slot of h, or with kSrcFw set,
-// corner*8 + octant of fw (a wall slot as switched in the reference, solver.F90:184-204).
-constexpr int kSrcRing = -1, kSrcZero = -2, kSrcFw = 1 << 30;
-
-template <int TV, int TW, int VPL, int D>
-struct SweepSmem {
-  static constexpr int NP = TV * TW, NV = 32 * VPL;
-  double ring[3][NP][NV];
-  double Dn[8][NV];           // denominators by first-order class (fx | fy<<1 | fz<<2)
-  double Rc[8][NV];           // their correctly rounded reciprocals
-  struct Stage {
-    double fold[NV];          // old value of the node (or slot o of a solid node)
-    double st[4][NV];         // static upwind values (y1, y2, z1, z2)
-    double mom[4];            // Rho, Ux, Uy, Uz
-  } pipe[NP][D];
-  int meta[NP][D][2];         // node, flags
-};
-
-// flags of a pencil position: bit 0 fy, bit 1 fz (first order in y / z), bits 2..5 which
-// of y1, y2, z1, z2 come from the ring, bits 8..15 the voxel label.
-template <int TV, int TW, int VPL, int D>
-__global__ void __launch_bounds__(TV * TW * 32, 1)
-k_sweep(const DevState a, int diag, int ntw) {
-  using SM = SweepSmem<TV, TW, VPL, D>;
-  constexpr int NV = SM::NV;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  SM &S = *reinterpret_cast<SM *>(smem_raw);
-  const int per_tile = 8 * a.nchunk;
-  const int tile = blockIdx.x / per_tile;
-  const int rem = blockIdx.x - tile * per_tile;
-  const int o = rem / a.nchunk;
-  const int chunk = rem - o * a.nchunk;
-  const int b = max(0, diag - (ntw - 1)) + tile;
-  const int c = diag - b;
-  const int sx = dsx(o), sy = dsy(o), sz = dsz(o);
-  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int pv = wid % TV, pw = wid / TV;
-  const int v = 1 + b * TV + pv, w = 1 + c * TW + pw;
-  const bool active = v <= a.Ny - 1 && w <= a.Nz - 1;
-  const int Nc8 = a.Nc8;
-  const int lbase = chunk * NV;
-  for (int e = threadIdx.x; e < NV; e += blockDim.x) {
-    const int l = lbase + e;
-    const bool ok = l < Nc8;
-    for (int cls = 0; cls < 8; ++cls) {
-      S.Dn[cls][e] = ok ? a.dtab[(size_t)cls * Nc8 + l] : 1.0;
-      S.Rc[cls][e] = ok ? a.rtab[(size_t)cls * Nc8 + l] : 1.0;
-    }
+template <int VPL>
+__device__ __forceinline__ void load_row(const DevState &a, int code, size_t l0, double (&v)[VPL]) {
+  const double *base = (code & kFwBit) ? a.fw : a.h;
+  const double *p = base + (size_t)(code & ~kFwBit) * (size_t)a.Nc8 + l0;
+  if (VPL == 2) {
+    const double2 t = __ldcg(reinterpret_cast<const double2 *>(p));
+    v[0] = t.x; v[VPL - 1] = t.y;
+  } else {
+    v[0] = __ldcg(p);
   }
-  // this lane's velocities: e = lane*VPL + q (contiguous pairs for 16-byte copies).
-  // fEq needs +-c*U: multiplying by the signed velocity component rounds identically.
-  double scx[VPL], scy[VPL], scz[VPL], wv[VPL];
-  double px2[VPL], px1[VPL], pxh[VPL], py2[VPL], py1[VPL], pyh[VPL], pz2[VPL], pz1[VPL], pzh[VPL];
-  bool lv[VPL];
+}
+
+// LPT lanes per task (32, or 8 when an octant has 8 velocities), VPL velocities per lane.
+template <int LPT, int VPL>
+__global__ void __launch_bounds__(256)
+k_sweep(const DevState a, long t0, long ntask) {
+  constexpr int TPW = 32 / LPT;  // tasks per warp
+  const long gl = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long slot = gl / LPT;                 // (task, chunk) slot of this lane group
+  const int sub = (int)(gl % LPT);
+  const long ti = slot / a.nchunk;
+  const int chunk = (int)(slot - ti * a.nchunk);
+  if (ti >= ntask) return;
+  const int Nc8 = a.Nc8;
+  const int lfirst = chunk * LPT * VPL + sub * VPL;
+  if (lfirst >= Nc8) return;
+  const int4 *rec = reinterpret_cast<const int4 *>(a.tasks + (size_t)(t0 + ti) * 8);
+  const int4 r0 = __ldg(rec), r1 = __ldg(rec + 1);
+  const int m = r0.x, fl = r0.y;
+  const int o = fl & 7;
+  const bool fx = fl & 8, fy = fl & 16, fz = fl & 32;
+  const size_t l0 = (size_t)lfirst;
+  // loads first: own value, moments, upwind values
+  double fold[VPL], x1[VPL], x2[VPL], y1[VPL], y2[VPL], z1[VPL], z2[VPL];
+  load_row<VPL>(a, m * 8 + o, l0, fold);
+  load_row<VPL>(a, r0.z, l0, x1);
+  load_row<VPL>(a, r1.x, l0, y1);
+  load_row<VPL>(a, r1.z, l0, z1);
+  if (!fx) load_row<VPL>(a, r0.w, l0, x2);
+  if (!fy) load_row<VPL>(a, r1.y, l0, y2);
+  if (!fz) load_row<VPL>(a, r1.w, l0, z2);
+  const double rho = __ldg(a.rho + m), ux = __ldg(a.ux + m), uy = __ldg(a.uy + m), uz = __ldg(a.uz + m);
+  const int cls = (fx ? 1 : 0) | (fy ? 2 : 0) | (fz ? 4 : 0);
+  const bool nx_ = dsx(o) < 0, ny_ = dsy(o) < 0, nz_ = dsz(o) < 0;
+  double out[VPL];
 #pragma unroll
   for (int q = 0; q < VPL; ++q) {
-    const int l = lbase + lane * VPL + q;
-    lv[q] = l < Nc8;
-    const double cx = lv[q] ? a.cx[l] : 0.0, cy = lv[q] ? a.cy[l] : 0.0, cz = lv[q] ? a.cz[l] : 0.0;
-    scx[q] = sx > 0 ? cx : -cx; scy[q] = sy > 0 ? cy : -cy; scz[q] = sz > 0 ? cz : -cz;
-    wv[q] = lv[q] ? a.w[l] : 0.0;
-    // coefficient products c*C of the upwind terms: second-order C1 = 2/ds, first-order
-    // C1 = 1/ds, second-order C2 = -0.5/ds (physicalGrid.F90:1259-1297)
-    px2[q] = dmul(cx, a.c20); px1[q] = dmul(cx, a.c10); pxh[q] = dmul(cx, a.c05);
-    py2[q] = dmul(cy, a.c20); py1[q] = dmul(cy, a.c10); pyh[q] = dmul(cy, a.c05);
-    pz2[q] = dmul(cz, a.c20); pz1[q] = dmul(cz, a.c10); pzh[q] = dmul(cz, a.c05);
+    const int l = lfirst + q;
+    const double *vt = a.vtab + (size_t)l * kVtab;  // cx cy cz w, products, dens, recips
+    const double cx = __ldg(vt + 0), cy = __ldg(vt + 1), cz = __ldg(vt + 2), wl = __ldg(vt + 3);
+    const double ex = dmul(nx_ ? -cx : cx, ux), ey = dmul(ny_ ? -cy : cy, uy), ez = dmul(nz_ ? -cz : cz, uz);
+    const double feq = dmul(wl, dadd(rho, dadd(dadd(ex, ey), ez)));
+    double num = dmul(a.mu, dsub(feq, dmul(0.5, fold[q])));
+    num = dadd(num, dmul(__ldg(vt + (fx ? 5 : 4)), x1[q]));
+    if (!fx) num = dadd(num, dmul(__ldg(vt + 6), x2[q]));
+    num = dadd(num, dmul(__ldg(vt + (fy ? 8 : 7)), y1[q]));
+    if (!fy) num = dadd(num, dmul(__ldg(vt + 9), y2[q]));
+    num = dadd(num, dmul(__ldg(vt + (fz ? 11 : 10)), z1[q]));
+    if (!fz) num = dadd(num, dmul(__ldg(vt + 12), z2[q]));
+    out[q] = markstein_div(num, __ldg(vt + 13 + cls), __ldg(vt + 21 + cls));
   }
-  const bool lane_ok = lv[0];  // VPL = 2 is used only when Nc8 is a multiple of 64
-  const uint8_t xbit = sx > 0 ? FACE_E : FACE_W;
-  const uint8_t ybit = sy > 0 ? FACE_N : FACE_S;
-  const uint8_t zbit = sz > 0 ? FACE_F : FACE_B;
-  const int j = sy > 0 ? v + 1 : a.Ny - v;
-  const int k = sz > 0 ? w + 1 : a.Nz - w;
-  const int i0 = sx > 0 ? 1 : a.Nx;
-  const long gbase = (long)(i0 + 1) + (long)(j + 1) * a.GX + (long)(k + 1) * a.GXY;
-  const long SY = (long)sy * a.GX, SZ = (long)sz * a.GXY;
-  const double mu = a.mu;
-  const int Nx = a.Nx;
-  const bool intile[4] = {pv >= 1, pv >= 2, pw >= 1, pw >= 2};
-
-  // Node-map block: lane i describes position u = ub + i of this pencil.
-  struct Block { int m, flags, src[4]; };
-  auto load_block = [&](int ubase, Block &B) {
-    const int u = ubase + lane;
-    B.m = -2; B.flags = 0;
-    B.src[0] = B.src[1] = B.src[2] = B.src[3] = kSrcZero;
-    if (!active || u > Nx - 1) return;
-    const long g = gbase + (long)sx * u;
-    B.m = __ldg(a.nodemap + g);
-    const int lab = __ldg(a.label + g);
-    const bool fy = (v == 1) || (c_face[__ldg(a.label + g - SY)] & ybit);
-    const bool fz = (w == 1) || (c_face[__ldg(a.label + g - SZ)] & zbit);
-    int fl = (fy ? 1 : 0) | (fz ? 2 : 0) | (lab << 8);
-    if (B.m >= 0 && B.m < a.NF && u >= 1) {
-      const long gq[4] = {g - SY, g - 2 * SY, g - SZ, g - 2 * SZ};
-#pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        const int mr = __ldg(a.nodemap + gq[r]);
-        int code = kSrcZero;
-        if (mr >= 0 && mr < a.NF) {
-          if (intile[r]) { code = kSrcRing; fl |= 4 << r; }
-          else code = mr * 8 + o;
-        } else if (mr >= a.NF) {
-          const int bb = mr - a.NF;
-          const int src = (__ldg(a.roles + (size_t)bb * 8 + o) >> (4 * r)) & 15;
-          code = src < 8 ? mr * 8 + src : (kSrcFw | (__ldg(a.bcorner + bb) * 8 + o));
-        }
-        B.src[r] = code;
-      }
-    }
-    B.flags = fl;
-  };
-  Block cur, nxt;
-  int ub = 0;
-  load_block(0, cur);
-  load_block(32, nxt);
-
-  // Issue the copies of position ui into pipeline stage ui % D (one commit group).
-  auto issue = [&](int ui) {
-    if (ui <= Nx - 1) {
-      if (ui - ub >= 32) {
-        ub += 32;
-        cur = nxt;
-        load_block(ub + 32, nxt);
-      }
-      const int s = ui - ub;
-      const int m = __shfl_sync(0xffffffffu, cur.m, s);
-      const int fl = __shfl_sync(0xffffffffu, cur.flags, s);
-      const int slot = ui % D;
-      typename SM::Stage &st = S.pipe[wid][slot];
-      if (lane == 0) { S.meta[wid][slot][0] = m; S.meta[wid][slot][1] = fl; }
-      if (m >= 0 && lane_ok) {
-        const double *gp = a.h + hidx(m, o, Nc8, lbase + lane * VPL);
-        if (VPL == 2) cp_async16(&st.fold[lane * 2], gp); else cp_async8(&st.fold[lane], gp);
-      }
-      if (m >= 0 && m < a.NF && ui >= 1) {
-        if (lane < 4) {
-          const double *mp = lane == 0 ? a.rho : lane == 1 ? a.ux : lane == 2 ? a.uy : a.uz;
-          cp_async8(&st.mom[lane], mp + m);
-        }
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-          const int sr = __shfl_sync(0xffffffffu, cur.src[r], s);
-          if (sr < 0 || !lane_ok) continue;
-          const double *gp = (sr & kSrcFw) ? a.fw + (size_t)(sr & ~kSrcFw) * Nc8 : a.h + (size_t)sr * Nc8;
-          gp += lbase + lane * VPL;
-          if (VPL == 2) cp_async16(&st.st[r][lane * 2], gp); else cp_async8(&st.st[r][lane], gp);
-        }
-      }
-    }
-    cp_async_commit();
-  };
-  // mu*(fEq - 0.5*f) of the node in a stage (solver.F90:206-207), computed one step ahead
-  auto base_of = [&](const typename SM::Stage &st, int q) {
-    const int e = lane * VPL + q;
-    const double ex = dmul(scx[q], st.mom[1]), ey = dmul(scy[q], st.mom[2]), ez = dmul(scz[q], st.mom[3]);
-    const double feq = dmul(wv[q], dadd(st.mom[0], dadd(dadd(ex, ey), ez)));
-    return dmul(mu, dsub(feq, dmul(0.5, st.fold[e])));
-  };
-
-  double xm1[VPL], xm2[VPL], base[VPL];
-#pragma unroll
-  for (int q = 0; q < VPL; ++q) { xm1[q] = 0.0; xm2[q] = 0.0; base[q] = 0.0; }
-  int labprev = L_GHOST;
-  if (active) {
-    issue(0);
-    cp_async_wait<0>();
-    __syncwarp();
-    const int m0 = S.meta[wid][0][0];
-#pragma unroll
-    for (int q = 0; q < VPL; ++q) xm1[q] = (m0 >= 0) ? S.pipe[wid][0].fold[lane * VPL + q] : 0.0;
-    labprev = S.meta[wid][0][1] >> 8 & 0xff;
-    __syncwarp();
-    for (int ui = 1; ui < D; ++ui) issue(ui);
-    cp_async_wait<D - 2>();  // position 1 landed
-    __syncwarp();
-    if (S.meta[wid][1 % D][0] >= 0 && S.meta[wid][1 % D][0] < a.NF) {
-#pragma unroll
-      for (int q = 0; q < VPL; ++q) base[q] = base_of(S.pipe[wid][1 % D], q);
-    }
-  }
-  __syncthreads();  // tables in shared memory
-
-  const int nsteps = (Nx - 1) + (TV - 1) + (TW - 1);
-  for (int t = 0; t < nsteps; ++t) {
-    const int u = t - pv - pw + 1;
-    if (active && u >= 1 && u <= Nx - 1) {
-      issue(u + D - 1);
-      cp_async_wait<D - 2>();  // positions <= u + 1 landed
-      __syncwarp();
-      const int slot = u % D;
-      const typename SM::Stage &st = S.pipe[wid][slot];
-      const int m = S.meta[wid][slot][0];
-      const int fl = S.meta[wid][slot][1];
-      double out[VPL];
-      if (m >= 0 && m < a.NF) {
-        const bool fx = (u == 1) || (c_face[labprev] & xbit);
-        const bool fy = fl & 1, fz = fl & 2;
-        const int cls = (fx ? 1 : 0) | (fy ? 2 : 0) | (fz ? 4 : 0);
-#pragma unroll
-        for (int q = 0; q < VPL; ++q) {
-          const int e = lane * VPL + q;
-          double num = dadd(base[q], dmul(fx ? px1[q] : px2[q], xm1[q]));
-          if (!fx) num = dadd(num, dmul(pxh[q], xm2[q]));
-          const double y1 = (fl & 4) ? S.ring[(t + 2) % 3][wid - 1][e] : st.st[0][e];
-          num = dadd(num, dmul(fy ? py1[q] : py2[q], y1));
-          if (!fy) {
-            const double y2 = (fl & 8) ? S.ring[(t + 1) % 3][wid - 2][e] : st.st[1][e];
-            num = dadd(num, dmul(pyh[q], y2));
-          }
-          const double z1 = (fl & 16) ? S.ring[(t + 2) % 3][wid - TV][e] : st.st[2][e];
-          num = dadd(num, dmul(fz ? pz1[q] : pz2[q], z1));
-          if (!fz) {
-            const double z2 = (fl & 32) ? S.ring[(t + 1) % 3][wid - 2 * TV][e] : st.st[3][e];
-            num = dadd(num, dmul(pzh[q], z2));
-          }
-          out[q] = markstein_div(num, S.Dn[cls][e], S.Rc[cls][e]);
-          S.ring[t % 3][wid][e] = out[q];
-        }
-        if (lane_ok) {
-          double *hp = a.h + hidx(m, o, Nc8, lbase + lane * VPL);
-          if (VPL == 2) *reinterpret_cast<double2 *>(hp) = make_double2(out[0], out[VPL - 1]);
-          else hp[0] = out[0];
-        }
-      } else {
-        // solid node read by the solver: x readers see its slot o unswitched; others 0
-#pragma unroll
-        for (int q = 0; q < VPL; ++q) out[q] = (m >= 0) ? st.fold[lane * VPL + q] : 0.0;
-      }
-#pragma unroll
-      for (int q = 0; q < VPL; ++q) { xm2[q] = xm1[q]; xm1[q] = out[q]; }
-      labprev = fl >> 8 & 0xff;
-      // next position's base while this step's results drain
-      if (u + 1 <= Nx - 1) {
-        const int sn = (u + 1) % D;
-        const int mn = S.meta[wid][sn][0];
-        if (mn >= 0 && mn < a.NF) {
-#pragma unroll
-          for (int q = 0; q < VPL; ++q) base[q] = base_of(S.pipe[wid][sn], q);
-        }
-      }
-      __syncwarp();
-    }
-    __syncthreads();
-  }
-  cp_async_wait<0>();
+  double *hp = a.h + ((size_t)m * 8 + o) * (size_t)Nc8 + l0;
+  if (VPL == 2) *reinterpret_cast<double2 *>(hp) = make_double2(out[0], out[VPL - 1]);
+  else hp[0] = out[0];
+  (void)TPW;
 }
-
-template <int TV, int TW, int VPL, int D>
-size_t sweep_smem_bytes() { return sizeof(SweepSmem<TV, TW, VPL, D>); }
 
 // Post-sweep content of switched wall slots: slot o of a wall ends the reference's sweep
 // holding the last value switched into it (z-upwind reader, else y-upwind reader).
@@ -596,33 +395,15 @@ void upload_tables() {
   cudaMemcpyToSymbol(c_incoming, kIncoming, sizeof(int) * 24);
 }
 
-int sweep_num_diagonals(const DevState &s) {
-  const int ntv = (s.Ny - 1 + kTV - 1) / kTV, ntw = (s.Nz - 1 + kTW - 1) / kTW;
-  return ntv + ntw - 1;
-}
-
-constexpr int kStages = 4;
-
-void launch_sweep_diagonal(const DevState &s, int diag, cudaStream_t st) {
-  const int ntv = (s.Ny - 1 + kTV - 1) / kTV, ntw = (s.Nz - 1 + kTW - 1) / kTW;
-  const int blo = diag - (ntw - 1) > 0 ? diag - (ntw - 1) : 0;
-  const int bhi = diag < ntv - 1 ? diag : ntv - 1;
-  const int ntiles = bhi - blo + 1;
-  if (ntiles <= 0) return;
-  static unsigned long long configured = 0;  // one bit per device
-  const size_t sm2 = sweep_smem_bytes<kTV, kTW, 2, kStages>();
-  const size_t sm1 = sweep_smem_bytes<kTV, kTW, 1, kStages>();
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (!(configured >> (dev & 63) & 1ull)) {
-    cudaFuncSetAttribute(k_sweep<kTV, kTW, 2, kStages>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2);
-    cudaFuncSetAttribute(k_sweep<kTV, kTW, 1, kStages>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
-    configured |= 1ull << (dev & 63);
+void launch_sweep_hyperplane(const DevState &s, long t0, long ntask, cudaStream_t st) {
+  if (ntask <= 0) return;
+  if (s.lpt == 32) {
+    const size_t threads = (size_t)ntask * s.nchunk * 32;
+    k_sweep<32, 2><<<blocks_for(threads, 256), 256, 0, st>>>(s, t0, ntask);
+  } else {
+    const size_t threads = (size_t)ntask * s.nchunk * 8;
+    k_sweep<8, 1><<<blocks_for(threads, 256), 256, 0, st>>>(s, t0, ntask);
   }
-  if (s.vpl == 2)
-    k_sweep<kTV, kTW, 2, kStages><<<ntiles * 8 * s.nchunk, kTV * kTW * 32, sm2, st>>>(s, diag, ntw);
-  else
-    k_sweep<kTV, kTW, 1, kStages><<<ntiles * 8 * s.nchunk, kTV * kTW * 32, sm1, st>>>(s, diag, ntw);
 }
 
 void launch_commit(const DevState &s, cudaStream_t st) {

@@ -8,7 +8,7 @@ namespace piks {
 // Everything the kernels read, as device pointers (one struct passed by value).
 struct DevState {
   int Nx, Ny, Nz, GX, GXY;      // interior extents; ghosted row / plane strides
-  int NF, NB, Nc8, nchunk, vpl; // fluid nodes, read solid nodes, velocities per octant, sweep chunks, velocities per lane
+  int NF, NB, Nc8, nchunk, lpt; // fluid nodes, read solid nodes, velocities per octant, sweep chunks, lanes per task
   const int32_t *nodemap;       // ghosted: >=0 node, -1 unread solid, -2 ghost
   const uint8_t *label;         // ghosted labels
   double *h;                    // [node][octant][Nc8] distribution function
@@ -20,7 +20,8 @@ struct DevState {
   double mu;                    // sqrt(pi/2)/Kn
   double c15, c20, c05, c10;    // 1.5/ds, 2/ds, -0.5/ds, 1/ds (physicalGrid.F90:1259-1297)
   double accom, pressDrop, DiffFlux;
-  const double *dtab, *rtab;    // [8][Nc8] sweep denominators by first-order class, reciprocals
+  const double *vtab;           // [Nc8][kVtab] per-velocity sweep constants (see kernels.cu)
+  const int32_t *tasks;         // sweep task records, 8 int32 each
   // walls
   int nWall;
   const int32_t *wall_node, *wall_label, *wall_corner, *wall_nb, *wall_order;
@@ -41,10 +42,10 @@ struct DevState {
   double *flux_out;             // [1]
 };
 
-// Tile of the sweep: TV x TW pencils (warps) per CTA.
-constexpr int kTV = 4, kTW = 4;
-int sweep_num_diagonals(const DevState &s);
-void launch_sweep_diagonal(const DevState &s, int diag, cudaStream_t st);
+// Per-velocity sweep constants: cx cy cz w, then c*C products (x: 2/ds, 1/ds, -0.5/ds;
+// y: same; z: same), the 8 denominators by first-order class and their reciprocals.
+constexpr int kVtab = 29;
+void launch_sweep_hyperplane(const DevState &s, long t0, long ntask, cudaStream_t st);
 void launch_commit(const DevState &s, cudaStream_t st);
 void launch_capture(const DevState &s, int buf, cudaStream_t st);
 void launch_walls(const DevState &s, int begin, int end, int gbuf, cudaStream_t st);

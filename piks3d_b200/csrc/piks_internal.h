@@ -78,6 +78,13 @@ struct Geometry {
   std::vector<int32_t> sym_node;   // nodes on the y/z boundary planes
   std::vector<uint8_t> sym_flag;   // bit0 y=1, bit1 y=Ny, bit2 z=1, bit3 z=Nz
   std::vector<int32_t> flux_list;  // x=2 plane entries in chkConverge's summation order
+  // Sweep tasks: one per (swept fluid node, octant), ordered by the hyperplane index
+  // u+v+w of the octant's frame; tasks of one hyperplane are independent.
+  // Record (8 x int32): node, flags (octant | fx<<3 | fy<<4 | fz<<5), then the value
+  // source of the x1, x2, y1, y2, z1, z2 upwind neighbours (row node*8+slot of h, or with
+  // bit 30 set row corner*8+octant of fw, or -2 for a ghost that is only multiplied by 0).
+  std::vector<int32_t> tasks;
+  std::vector<int64_t> hyper_start;   // task offset of each hyperplane (+1 end entry)
   int32_t flux_groups[10] = {0};   // offsets of the 9 partial sums
   int64_t ghost_index(int i, int j, int k) const {
     return (int64_t)(i + 1) + (int64_t)(j + 1) * GX + (int64_t)(k + 1) * GX * GY;

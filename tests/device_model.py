@@ -72,6 +72,8 @@ class DeviceModel:
         self.sym_node, self.sym_flag = g("sym_node"), g("sym_flag")
         self.flux_list, self.flux_groups = g("flux_list"), g("flux_groups")
         self.cx, self.cy, self.cz, self.w = g("cx"), g("cy"), g("cz"), g("w")
+        self.tasks = g("tasks").reshape(-1, 8)
+        self.hyper_start = g("hyper_start")
         fl = params.fluidlayer
         self.ds = 1.0 / (self.Nx - 1 - 2 * fl)
         self.mu = math.sqrt((math.atan(1.0) * 4.0) / 2.0) / params.Kn
@@ -156,6 +158,51 @@ class DeviceModel:
                         den = den + t if s > 0 else den - t
                     self.h[m, o] = num / den
 
+    def _row(self, code):
+        if code == -2:
+            return None
+        if code & (1 << 30):
+            c = code & ~(1 << 30)
+            return self.fw[c // 8, c % 8]
+        return self.h[code // 8, code % 8]
+
+    def sweep_tasks(self):
+        """All eight octant sweeps from the library's task list, hyperplane by hyperplane."""
+        c15, c10 = 1.5 / self.ds, 1.0 / self.ds
+        P = {"x2": self.cx * (2.0 / self.ds), "x1": self.cx * c10, "xh": self.cx * (-0.5 / self.ds),
+             "y2": self.cy * (2.0 / self.ds), "y1": self.cy * c10, "yh": self.cy * (-0.5 / self.ds),
+             "z2": self.cz * (2.0 / self.ds), "z1": self.cz * c10, "zh": self.cz * (-0.5 / self.ds)}
+        dens = {}
+        for cls in range(8):
+            d = 0.5 * self.mu + self.cx * (c10 if cls & 1 else c15)
+            d = d + self.cy * (c10 if cls & 2 else c15)
+            dens[cls] = d + self.cz * (c10 if cls & 4 else c15)
+        for h in range(len(self.hyper_start) - 1):
+            rows = self.tasks[self.hyper_start[h]:self.hyper_start[h + 1]]
+            new = []
+            for t in rows:
+                m, fl = int(t[0]), int(t[1])
+                o = fl & 7
+                fx, fy, fz = bool(fl & 8), bool(fl & 16), bool(fl & 32)
+                ex = (-self.cx if SX[o] < 0 else self.cx) * self.mom[1, m]
+                ey = (-self.cy if SY[o] < 0 else self.cy) * self.mom[2, m]
+                ez = (-self.cz if SZ[o] < 0 else self.cz) * self.mom[3, m]
+                feq = self.w * (self.mom[0, m] + ((ex + ey) + ez))
+                num = self.mu * (feq - 0.5 * self.h[m, o])
+                num = num + (P["x1"] if fx else P["x2"]) * self._row(int(t[2]))
+                if not fx:
+                    num = num + P["xh"] * self._row(int(t[3]))
+                num = num + (P["y1"] if fy else P["y2"]) * self._row(int(t[4]))
+                if not fy:
+                    num = num + P["yh"] * self._row(int(t[5]))
+                num = num + (P["z1"] if fz else P["z2"]) * self._row(int(t[6]))
+                if not fz:
+                    num = num + P["zh"] * self._row(int(t[7]))
+                cls = (1 if fx else 0) | (2 if fy else 0) | (4 if fz else 0)
+                new.append((m, o, num / dens[cls]))
+            for m, o, val in new:   # a hyperplane's tasks are independent
+                self.h[m, o] = val
+
     # --- the rest of one iteration -------------------------------------------------------
     def _far(self, code, o, gbuf):
         if code >= 0:
@@ -205,12 +252,15 @@ class DeviceModel:
                     else:
                         self.fw[corner, dst_o - 1] = v
 
-    def iterate(self, n=1):
+    def iterate(self, n=1, schedule="tasks"):
         for _ in range(n):
             it = self.iStep + 1
             cap, prev = it & 1, (it - 1) & 1
-            for o in range(8):
-                self.sweep(o)
+            if schedule == "tasks":
+                self.sweep_tasks()
+            else:
+                for o in range(8):
+                    self.sweep(o)
             for node, o, src in self.commit:
                 self.h[node, o] = self.h[node, src] if src < 8 else self.fw[self.bcorner[node - self.NF], o]
             for r in range(self.Ny * self.Nz):
