@@ -155,22 +155,24 @@ __global__ void k_capture(const DevState a, int buf) {
   a.ghostE[buf][idx] = nE >= 0 ? a.h[hidx(nE, oE, a.Nc8, l)] : 0.0;
 }
 
-// Value at a wall's +2d extrapolation point: a node, zero (y/z ghost layers), or a ghost
-// plane x = 0 / x = Nx+1 (code -(2+2r) / -(3+2r) for plane row r).
-__device__ __forceinline__ double ext_far(const DevState &a, int code, int o, int l, int gbuf) {
-  if (code >= 0) return a.h[hidx(code, o, a.Nc8, l)];
-  if (code == -1) return 0.0;
-  const int c = -code - 2;
-  const size_t r = (size_t)(c >> 1);
-  const double *plane = (c & 1) ? a.ghostE[gbuf] : a.ghostW[gbuf];
-  return plane[(r * 4 + plane_slot(o)) * a.Nc8 + l];
+// Diffuse wall (solver.F90:761-1826): one warp per wall, lanes over velocities (VPL per
+// lane). The wall program (wall_table.inc) lists, per fluid-side face, the 4 extrapolated
+// incoming octants and then the re-emission writes in the reference's statement order.
+// All neighbour values are loaded before any arithmetic; the density sums run serially
+// over l in the reference's order by passing the per-velocity terms through the warp.
+template <int VPL>
+__device__ __forceinline__ void ld_vpl(const double *p, double (&v)[VPL]) {
+  if (VPL == 2) { const double2 t = __ldcg(reinterpret_cast<const double2 *>(p)); v[0] = t.x; v[VPL - 1] = t.y; }
+  else v[0] = __ldcg(p);
+}
+template <int VPL>
+__device__ __forceinline__ void st_vpl(double *p, const double (&v)[VPL]) {
+  if (VPL == 2) *reinterpret_cast<double2 *>(p) = make_double2(v[0], v[VPL - 1]);
+  else p[0] = v[0];
 }
 
-// Diffuse wall (solver.F90:761-1826): one warp per wall, lanes over velocities. The
-// wall program (wall_table.inc) lists, per fluid-side face, the 4 extrapolated incoming
-// octants and then the re-emission writes in the reference's statement order. The
-// density sums run serially over l in lane order to keep the reference's rounding.
-__global__ void k_walls(const DevState a, int begin, int end, int gbuf) {
+template <int VPL>
+__global__ void __launch_bounds__(256) k_walls(const DevState a, int begin, int end, int gbuf) {
   const int widx = begin + (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   if (widx >= end) return;  // whole warp
   const int lane = threadIdx.x & 31;
@@ -181,54 +183,99 @@ __global__ void k_walls(const DevState a, int begin, int end, int gbuf) {
   const double e1 = a.wall_e[2 * q], e2 = a.wall_e[2 * q + 1];
   const int Nc8 = a.Nc8;
   const int *nb = a.wall_nb + 6 * q;
-  double rho[3] = {0.0, 0.0, 0.0};
-  for (int l0 = 0; l0 < Nc8; l0 += 32) {
-    const int l = l0 + lane;
-    const bool lv = l < Nc8;
-    double tface[3] = {0.0, 0.0, 0.0};
-    for (int fi = 0; fi < P.nface; ++fi) {
-      const int dir = P.face[fi].dir, st = P.face[fi].store;
-      double vals[4];
+  const int nface = P.nface;
+  const int chunkw = 32 * VPL;
+  double rho0 = 0.0, rho1 = 0.0, rho2 = 0.0;
+  for (int fi = 0; fi < nface; ++fi) {
+    const int dir = P.face[fi].dir, st = P.face[fi].store;
+    const int n1 = nb[2 * fi], code = nb[2 * fi + 1];
+    const double *plane = nullptr;
+    size_t prow = 0;
+    if (code < -1) {
+      const int cc = -code - 2;
+      plane = (cc & 1) ? a.ghostE[gbuf] : a.ghostW[gbuf];
+      prow = (size_t)(cc >> 1) * 4;
+    }
+    double racc = 0.0;
+    for (int l0 = 0; l0 < Nc8; l0 += chunkw) {
+      const int lf = l0 + lane * VPL;
+      const bool lv = lf < Nc8;
+      double near_[4][VPL], far_[4][VPL];
+#pragma unroll
       for (int mm = 0; mm < 4; ++mm) {
         const int oo = c_incoming[dir][mm] - 1;
-        double v = 0.0;
-        if (lv) {
-          v = dadd(dmul(e1, a.h[hidx(nb[2 * fi], oo, Nc8, l)]), dmul(e2, ext_far(a, nb[2 * fi + 1], oo, l, gbuf)));
-          if (st == ST_F) a.h[hidx(node, oo, Nc8, l)] = v;
-          else if (st == ST_W) a.fw[hidx(corner, oo, Nc8, l)] = v;
-        }
-        vals[mm] = v;
+#pragma unroll
+        for (int v = 0; v < VPL; ++v) { near_[mm][v] = 0.0; far_[mm][v] = 0.0; }
+        if (!lv) continue;
+        ld_vpl<VPL>(a.h + hidx(n1, oo, Nc8, lf), near_[mm]);
+        if (code >= 0) ld_vpl<VPL>(a.h + hidx(code, oo, Nc8, lf), far_[mm]);
+        else if (plane) ld_vpl<VPL>(plane + (prow + plane_slot(oo)) * Nc8 + lf, far_[mm]);
       }
-      if (lv) {
-        const double ca = dir < 2 ? a.cx[l] : dir < 4 ? a.cy[l] : a.cz[l];
-        tface[fi] = dmul(ca, dadd(dadd(dadd(vals[0], vals[1]), vals[2]), vals[3]));
+      double ext[4][VPL];
+#pragma unroll
+      for (int mm = 0; mm < 4; ++mm) {
+        const int oo = c_incoming[dir][mm] - 1;
+#pragma unroll
+        for (int v = 0; v < VPL; ++v) ext[mm][v] = dadd(dmul(e1, near_[mm][v]), dmul(e2, far_[mm][v]));
+        if (lv) {
+          if (st == ST_F) st_vpl<VPL>(a.h + hidx(node, oo, Nc8, lf), ext[mm]);
+          else if (st == ST_W) st_vpl<VPL>(a.fw + hidx(corner, oo, Nc8, lf), ext[mm]);
+        }
+      }
+      double tface[VPL];
+#pragma unroll
+      for (int v = 0; v < VPL; ++v) {
+        const int l = lf + v;
+        const double ca = !lv ? 0.0 : dir < 2 ? __ldg(a.cx + l) : dir < 4 ? __ldg(a.cy + l) : __ldg(a.cz + l);
+        tface[v] = dmul(ca, dadd(dadd(dadd(ext[0][v], ext[1][v]), ext[2][v]), ext[3][v]));
+      }
+      const int nl = min(chunkw, Nc8 - l0);
+      for (int sidx = 0; sidx < nl; ++sidx) {
+        const int srcl = sidx / VPL, v = sidx % VPL;
+        racc = dadd(racc, __shfl_sync(0xffffffffu, (VPL == 2 && v == 1) ? tface[VPL - 1] : tface[0], srcl));
       }
     }
-    const int nl = min(32, Nc8 - l0);
-    for (int s = 0; s < nl; ++s)
-      for (int fi = 0; fi < 3; ++fi) {
-        const double tv = __shfl_sync(0xffffffffu, tface[fi], s);
-        if (fi < P.nface) rho[fi] = dadd(rho[fi], tv);
-      }
+    if (fi == 0) rho0 = racc; else if (fi == 1) rho1 = racc; else rho2 = racc;
   }
-  for (int fi = 0; fi < P.nface; ++fi) rho[fi] = __ddiv_rn(rho[fi], a.DiffFlux);
+  rho0 = __ddiv_rn(rho0, a.DiffFlux);
+  if (nface > 1) rho1 = __ddiv_rn(rho1, a.DiffFlux);
+  if (nface > 2) rho2 = __ddiv_rn(rho2, a.DiffFlux);
   const double one_m = dsub(1.0, a.accom);
   int zface = -1;
-  for (int fi = 0; fi < P.nface; ++fi) if (P.face[fi].store == ST_Z) zface = fi;
-  for (int l0 = 0; l0 < Nc8; l0 += 32) {
-    const int l = l0 + lane;
-    if (l >= Nc8) continue;
-    const double aw = dmul(a.accom, a.w[l]);
+  for (int fi = 0; fi < nface; ++fi) if (P.face[fi].store == ST_Z) zface = fi;
+  for (int l0 = 0; l0 < Nc8; l0 += chunkw) {
+    const int lf = l0 + lane * VPL;
+    if (lf >= Nc8) continue;
+    double aw[VPL];
+#pragma unroll
+    for (int v = 0; v < VPL; ++v) aw[v] = dmul(a.accom, __ldg(a.w + lf + v));
     for (int r = 0; r < P.nwr; ++r) {
       const WWrite &W = P.wr[r];
       const int so = W.src_o - 1, dso = W.dst_o - 1;
-      double src;
-      if (W.src_store == ST_F) src = a.h[hidx(node, so, Nc8, l)];
-      else if (W.src_store == ST_W) src = a.fw[hidx(corner, so, Nc8, l)];
-      else src = dadd(dmul(e1, a.h[hidx(nb[2 * zface], so, Nc8, l)]), dmul(e2, ext_far(a, nb[2 * zface + 1], so, l, gbuf)));
-      const double v = dadd(dmul(aw, rho[W.face]), dmul(one_m, src));
-      if (W.dst_store == ST_F) a.h[hidx(node, dso, Nc8, l)] = v;
-      else a.fw[hidx(corner, dso, Nc8, l)] = v;
+      double src[VPL];
+      if (W.src_store == ST_F) ld_vpl<VPL>(a.h + hidx(node, so, Nc8, lf), src);
+      else if (W.src_store == ST_W) ld_vpl<VPL>(a.fw + hidx(corner, so, Nc8, lf), src);
+      else {
+        double n1v[VPL], farv[VPL];
+        ld_vpl<VPL>(a.h + hidx(nb[2 * zface], so, Nc8, lf), n1v);
+        const int code = nb[2 * zface + 1];
+#pragma unroll
+        for (int v = 0; v < VPL; ++v) farv[v] = 0.0;
+        if (code >= 0) ld_vpl<VPL>(a.h + hidx(code, so, Nc8, lf), farv);
+        else if (code != -1) {
+          const int cc = -code - 2;
+          const double *plane = (cc & 1) ? a.ghostE[gbuf] : a.ghostW[gbuf];
+          ld_vpl<VPL>(plane + ((size_t)(cc >> 1) * 4 + plane_slot(so)) * Nc8 + lf, farv);
+        }
+#pragma unroll
+        for (int v = 0; v < VPL; ++v) src[v] = dadd(dmul(e1, n1v[v]), dmul(e2, farv[v]));
+      }
+      double val[VPL];
+      const double rf = W.face == 0 ? rho0 : W.face == 1 ? rho1 : rho2;
+#pragma unroll
+      for (int v = 0; v < VPL; ++v) val[v] = dadd(dmul(aw[v], rf), dmul(one_m, src[v]));
+      if (W.dst_store == ST_F) st_vpl<VPL>(a.h + hidx(node, dso, Nc8, lf), val);
+      else st_vpl<VPL>(a.fw + hidx(corner, dso, Nc8, lf), val);
     }
   }
 }
@@ -272,71 +319,73 @@ __global__ void k_symmetry(const DevState a) {
 }
 
 // Moments Rho, Ux, Uy, Uz (solver.F90:1923-1938). One lane per fluid node runs the four
-// sums serially over (l, octant) in the reference's order; a warp stages its 32 nodes'
-// values 8 velocities at a time in shared memory with coalesced 64-byte row loads.
-constexpr int kMomWarps = 2;
-constexpr int kMomL = 8;
-constexpr int kMomStride = 8 * kMomL + 1;  // odd stride in doubles: conflict-free lane reads
-__global__ void __launch_bounds__(kMomWarps * 32) k_moments(const DevState a) {
-  __shared__ double sm[kMomWarps][32 * kMomStride];
-  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int node0 = (blockIdx.x * kMomWarps + wid) * 32;
-  if (node0 >= a.NF) return;  // whole warp
+// sums serially over (l, octant) in the reference's order, reading its node's values
+// directly; consecutive velocities of an octant share a 32-byte sector, so after the
+// first load of a sector the next three come from L1.
+__global__ void __launch_bounds__(128) k_moments(const DevState a) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= a.NF) return;
   const int Nc8 = a.Nc8;
-  const int my = node0 + lane;
-  const bool valid = my < a.NF;
+  const double *hp = a.h + (size_t)n * 8 * Nc8;
   double r = 0.0, ux = 0.0, uy = 0.0, uz = 0.0;
-  double *buf = sm[wid];
-  for (int l0 = 0; l0 < Nc8; l0 += kMomL) {
-    // 32 nodes x 8 octants rows of kMomL values; lane group g (4 groups of 8 lanes) loads a row
-    const int sub = lane & 7, grp = lane >> 3;
-    for (int row = grp; row < 32 * 8; row += 4) {
-      const int nn = row >> 3, o = row & 7;
-      const int node = node0 + nn;
-      double val = 0.0;
-      if (node < a.NF && l0 + sub < Nc8) val = __ldcs(a.h + hidx(node, o, Nc8, l0 + sub));
-      buf[nn * kMomStride + o * kMomL + sub] = val;
-    }
-    __syncwarp();
-    const int nl = min(kMomL, Nc8 - l0);
-    const double *mine = buf + lane * kMomStride;
-    for (int s = 0; s < nl; ++s) {
-      const double f1 = mine[0 * kMomL + s], f2 = mine[1 * kMomL + s], f3 = mine[2 * kMomL + s], f4 = mine[3 * kMomL + s];
-      const double f5 = mine[4 * kMomL + s], f6 = mine[5 * kMomL + s], f7 = mine[6 * kMomL + s], f8 = mine[7 * kMomL + s];
-      r = dadd(dadd(dadd(dadd(dadd(dadd(dadd(dadd(r, f1), f2), f3), f4), f5), f6), f7), f8);
-      const double dx = dadd(dsub(dsub(dadd(dadd(dsub(dsub(f1, f2), f3), f4), f5), f6), f7), f8);
-      const double dy = dsub(dsub(dadd(dadd(dsub(dsub(dadd(f1, f2), f3), f4), f5), f6), f7), f8);
-      const double dz = dsub(dsub(dsub(dsub(dadd(dadd(dadd(f1, f2), f3), f4), f5), f6), f7), f8);
-      ux = dadd(ux, dmul(__ldg(a.cx + l0 + s), dx));
-      uy = dadd(uy, dmul(__ldg(a.cy + l0 + s), dy));
-      uz = dadd(uz, dmul(__ldg(a.cz + l0 + s), dz));
-    }
-    __syncwarp();
+  for (int l = 0; l < Nc8; ++l) {
+    const double f1 = __ldca(hp + 0 * Nc8 + l), f2 = __ldca(hp + 1 * Nc8 + l), f3 = __ldca(hp + 2 * Nc8 + l),
+                 f4 = __ldca(hp + 3 * Nc8 + l), f5 = __ldca(hp + 4 * Nc8 + l), f6 = __ldca(hp + 5 * Nc8 + l),
+                 f7 = __ldca(hp + 6 * Nc8 + l), f8 = __ldca(hp + 7 * Nc8 + l);
+    r = dadd(dadd(dadd(dadd(dadd(dadd(dadd(dadd(r, f1), f2), f3), f4), f5), f6), f7), f8);
+    const double dx = dadd(dsub(dsub(dadd(dadd(dsub(dsub(f1, f2), f3), f4), f5), f6), f7), f8);
+    const double dy = dsub(dsub(dadd(dadd(dsub(dsub(dadd(f1, f2), f3), f4), f5), f6), f7), f8);
+    const double dz = dsub(dsub(dsub(dsub(dadd(dadd(dadd(f1, f2), f3), f4), f5), f6), f7), f8);
+    ux = dadd(ux, dmul(__ldg(a.cx + l), dx));
+    uy = dadd(uy, dmul(__ldg(a.cy + l), dy));
+    uz = dadd(uz, dmul(__ldg(a.cz + l), dz));
   }
-  if (valid) { a.rho[my] = r; a.ux[my] = ux; a.uy[my] = uy; a.uz[my] = uz; }
+  a.rho[n] = r; a.ux[n] = ux; a.uy[n] = uy; a.uz[n] = uz;
 }
 
-// Mass flux through x = 2 (output.F90:90-142) in the reference's summation order; one
-// thread, the plane has only Ny*Nz terms.
-__global__ void k_flux(const DevState a, double ds, double sqrt_half, double inv_refl2) {
-  if (blockIdx.x != 0 || threadIdx.x != 0) return;
-  double part[9];
-  for (int gi = 0; gi < 9; ++gi) {
-    double s = 0.0;
-    for (int e = a.flux_groups[gi]; e < a.flux_groups[gi + 1]; ++e) {
-      const int n = a.flux_list[e];
-      const double u = n >= 0 ? a.ux[n] : 0.0;
-      double term = dmul(dmul(u, ds), ds);
-      if (gi >= 1 && gi <= 4) term = dmul(term, 0.5);
-      else if (gi >= 5) term = dmul(term, 0.25);
-      s = gi <= 4 ? dadd(s, term) : term;
+// Mass flux through x = 2 (output.F90:90-142) in the reference's summation order: the
+// block gathers the plane's Ux values into shared memory in parallel, one thread then
+// accumulates them serially. Runs over the plane in tiles of kFluxTile entries.
+constexpr int kFluxTile = 4096;
+__global__ void __launch_bounds__(256) k_flux(const DevState a, double ds, double sqrt_half, double inv_refl2) {
+  __shared__ double ux[kFluxTile];
+  __shared__ double part[9];
+  __shared__ int gi_s;
+  __shared__ double acc_s;
+  const int total = a.flux_groups[9];
+  if (threadIdx.x == 0) { gi_s = 0; acc_s = 0.0; }
+  for (int base = 0; base < total; base += kFluxTile) {
+    const int cnt = min(kFluxTile, total - base);
+    __syncthreads();
+    for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
+      const int n = a.flux_list[base + e];
+      ux[e] = n >= 0 ? a.ux[n] : 0.0;
     }
-    part[gi] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int gi = gi_s;
+      double s = acc_s;
+      for (int e = 0; e < cnt; ++e) {
+        const int idx = base + e;
+        while (idx >= a.flux_groups[gi + 1]) { part[gi] = s; ++gi; s = 0.0; }
+        double term = dmul(dmul(ux[e], ds), ds);
+        if (gi >= 1 && gi <= 4) term = dmul(term, 0.5);
+        else if (gi >= 5) term = dmul(term, 0.25);
+        s = gi <= 4 ? dadd(s, term) : term;
+      }
+      gi_s = gi;
+      acc_s = s;
+    }
   }
-  double m = part[0];
-  for (int gi = 1; gi < 9; ++gi) m = dadd(m, part[gi]);
-  m = __ddiv_rn(__ddiv_rn(dmul(m, sqrt_half), a.pressDrop), inv_refl2);
-  a.flux_out[0] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int gi = gi_s;
+    double s = acc_s;
+    while (gi < 9) { part[gi] = s; ++gi; s = 0.0; }
+    double m = part[0];
+    for (int g = 1; g < 9; ++g) m = dadd(m, part[g]);
+    a.flux_out[0] = __ddiv_rn(__ddiv_rn(dmul(m, sqrt_half), a.pressDrop), inv_refl2);
+  }
 }
 
 inline unsigned blocks_for(size_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
@@ -430,17 +479,18 @@ void launch_symmetry(const DevState &s, cudaStream_t st) {
 
 void launch_moments(const DevState &s, cudaStream_t st) {
   if (s.NF == 0) return;
-  k_moments<<<blocks_for((size_t)s.NF, kMomWarps * 32), kMomWarps * 32, 0, st>>>(s);
+  k_moments<<<blocks_for((size_t)s.NF, 128), 128, 0, st>>>(s);
 }
 
 void launch_walls(const DevState &s, int begin, int end, int gbuf, cudaStream_t st) {
   if (end <= begin) return;
   const size_t threads = (size_t)(end - begin) * 32;
-  k_walls<<<blocks_for(threads, 256), 256, 0, st>>>(s, begin, end, gbuf);
+  if (s.Nc8 % 64 == 0) k_walls<2><<<blocks_for(threads, 256), 256, 0, st>>>(s, begin, end, gbuf);
+  else k_walls<1><<<blocks_for(threads, 256), 256, 0, st>>>(s, begin, end, gbuf);
 }
 
 void launch_flux(const DevState &s, double ds, double sqrt_half, double inv_refl2, cudaStream_t st) {
-  k_flux<<<1, 32, 0, st>>>(s, ds, sqrt_half, inv_refl2);
+  k_flux<<<1, 256, 0, st>>>(s, ds, sqrt_half, inv_refl2);
 }
 
 }  // namespace piks
