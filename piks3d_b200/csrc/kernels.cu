@@ -26,6 +26,14 @@ __device__ __forceinline__ size_t hidx(int node, int o, int Nc8, int l) {
 __device__ __forceinline__ int dsx(int o) { return (o == 0 || o == 3 || o == 4 || o == 7) ? 1 : -1; }
 __device__ __forceinline__ int dsy(int o) { return (o == 0 || o == 1 || o == 4 || o == 5) ? 1 : -1; }
 __device__ __forceinline__ int dsz(int o) { return o < 4 ? 1 : -1; }
+// Asynchronous global->shared copies (cp.async, 8 bytes through L1) with commit groups.
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 // octant -> slot within a ghost plane (cx>0 octants 0,3,4,7 ; cx<0 octants 1,2,5,6)
 __device__ __forceinline__ int plane_slot(int o) { return o >> 1; }
 
@@ -318,29 +326,66 @@ __global__ void k_symmetry(const DevState a) {
   if (f & 8) { hp[4 * S] = hp[0 * S]; hp[5 * S] = hp[1 * S]; hp[6 * S] = hp[2 * S]; hp[7 * S] = hp[3 * S]; }
 }
 
-// Moments Rho, Ux, Uy, Uz (solver.F90:1923-1938). One lane per fluid node runs the four
-// sums serially over (l, octant) in the reference's order, reading its node's values
-// directly; consecutive velocities of an octant share a 32-byte sector, so after the
-// first load of a sector the next three come from L1.
-__global__ void __launch_bounds__(128) k_moments(const DevState a) {
-  const int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= a.NF) return;
+// Moments Rho, Ux, Uy, Uz (solver.F90:1923-1938). A warp owns 32 fluid nodes; lane n
+// runs node n's four sums serially over (l, octant) in the reference's order. The values
+// move through shared memory kMomL velocities at a time, double-buffered with cp.async:
+// each copy is an 8-byte piece of a 32-byte (node, octant) segment, so a warp request
+// covers 8 whole segments.
+constexpr int kMomWarps = 4;
+constexpr int kMomL = 4;
+constexpr int kMomStride = 8 * kMomL + 1;  // odd stride: lane-per-node reads hit distinct banks
+struct MomSmem { double buf[kMomWarps][2][32 * kMomStride]; };
+
+__global__ void __launch_bounds__(kMomWarps * 32) k_moments(const DevState a) {
+  extern __shared__ __align__(16) unsigned char mom_raw[];
+  MomSmem &S = *reinterpret_cast<MomSmem *>(mom_raw);
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int node0 = (blockIdx.x * kMomWarps + wid) * 32;
+  if (node0 >= a.NF) return;  // whole warp
   const int Nc8 = a.Nc8;
-  const double *hp = a.h + (size_t)n * 8 * Nc8;
+  const int nvalid = min(32, a.NF - node0);
+  // copy assignment: piece p = lane + 32*r (r < 32) of the 1024 pieces of a stage:
+  // segment (nn, o) = p / kMomL, velocity lc = p % kMomL
+  auto issue = [&](int l0, int b) {
+    double *dst = S.buf[wid][b];
+    for (int r = 0; r < 32; ++r) {
+      const int piece = lane + 32 * r;
+      const int seg = piece / kMomL, lc = piece % kMomL;
+      const int nn = seg >> 3, o = seg & 7;
+      if (nn < nvalid && l0 + lc < Nc8)
+        cp_async8(dst + nn * kMomStride + o * kMomL + lc, a.h + hidx(node0 + nn, o, Nc8, l0 + lc));
+    }
+    cp_async_commit();
+  };
   double r = 0.0, ux = 0.0, uy = 0.0, uz = 0.0;
-  for (int l = 0; l < Nc8; ++l) {
-    const double f1 = __ldca(hp + 0 * Nc8 + l), f2 = __ldca(hp + 1 * Nc8 + l), f3 = __ldca(hp + 2 * Nc8 + l),
-                 f4 = __ldca(hp + 3 * Nc8 + l), f5 = __ldca(hp + 4 * Nc8 + l), f6 = __ldca(hp + 5 * Nc8 + l),
-                 f7 = __ldca(hp + 6 * Nc8 + l), f8 = __ldca(hp + 7 * Nc8 + l);
-    r = dadd(dadd(dadd(dadd(dadd(dadd(dadd(dadd(r, f1), f2), f3), f4), f5), f6), f7), f8);
-    const double dx = dadd(dsub(dsub(dadd(dadd(dsub(dsub(f1, f2), f3), f4), f5), f6), f7), f8);
-    const double dy = dsub(dsub(dadd(dadd(dsub(dsub(dadd(f1, f2), f3), f4), f5), f6), f7), f8);
-    const double dz = dsub(dsub(dsub(dsub(dadd(dadd(dadd(f1, f2), f3), f4), f5), f6), f7), f8);
-    ux = dadd(ux, dmul(__ldg(a.cx + l), dx));
-    uy = dadd(uy, dmul(__ldg(a.cy + l), dy));
-    uz = dadd(uz, dmul(__ldg(a.cz + l), dz));
+  issue(0, 0);
+  int b = 0;
+  for (int l0 = 0; l0 < Nc8; l0 += kMomL) {
+    if (l0 + kMomL < Nc8) { issue(l0 + kMomL, b ^ 1); cp_async_wait<1>(); }
+    else cp_async_wait<0>();
+    __syncwarp();
+    const double *mine = S.buf[wid][b] + lane * kMomStride;
+    const int nl = min(kMomL, Nc8 - l0);
+    if (lane < nvalid) {
+      for (int s2 = 0; s2 < nl; ++s2) {
+        const double f1 = mine[0 * kMomL + s2], f2 = mine[1 * kMomL + s2], f3 = mine[2 * kMomL + s2], f4 = mine[3 * kMomL + s2];
+        const double f5 = mine[4 * kMomL + s2], f6 = mine[5 * kMomL + s2], f7 = mine[6 * kMomL + s2], f8 = mine[7 * kMomL + s2];
+        r = dadd(dadd(dadd(dadd(dadd(dadd(dadd(dadd(r, f1), f2), f3), f4), f5), f6), f7), f8);
+        const double dx = dadd(dsub(dsub(dadd(dadd(dsub(dsub(f1, f2), f3), f4), f5), f6), f7), f8);
+        const double dy = dsub(dsub(dadd(dadd(dsub(dsub(dadd(f1, f2), f3), f4), f5), f6), f7), f8);
+        const double dz = dsub(dsub(dsub(dsub(dadd(dadd(dadd(f1, f2), f3), f4), f5), f6), f7), f8);
+        ux = dadd(ux, dmul(__ldg(a.cx + l0 + s2), dx));
+        uy = dadd(uy, dmul(__ldg(a.cy + l0 + s2), dy));
+        uz = dadd(uz, dmul(__ldg(a.cz + l0 + s2), dz));
+      }
+    }
+    __syncwarp();
+    b ^= 1;
   }
-  a.rho[n] = r; a.ux[n] = ux; a.uy[n] = uy; a.uz[n] = uz;
+  if (lane < nvalid) {
+    const int n = node0 + lane;
+    a.rho[n] = r; a.ux[n] = ux; a.uy[n] = uy; a.uz[n] = uz;
+  }
 }
 
 // Mass flux through x = 2 (output.F90:90-142) in the reference's summation order: the
@@ -479,7 +524,14 @@ void launch_symmetry(const DevState &s, cudaStream_t st) {
 
 void launch_moments(const DevState &s, cudaStream_t st) {
   if (s.NF == 0) return;
-  k_moments<<<blocks_for((size_t)s.NF, 128), 128, 0, st>>>(s);
+  static unsigned long long configured = 0;  // one bit per device
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!(configured >> (dev & 63) & 1ull)) {
+    cudaFuncSetAttribute(k_moments, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MomSmem));
+    configured |= 1ull << (dev & 63);
+  }
+  k_moments<<<blocks_for((size_t)s.NF, kMomWarps * 32), kMomWarps * 32, sizeof(MomSmem), st>>>(s);
 }
 
 void launch_walls(const DevState &s, int begin, int end, int gbuf, cudaStream_t st) {
