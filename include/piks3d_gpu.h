@@ -126,6 +126,19 @@ piks_status piks_launches_per_iteration(piks_ctx *ctx, int64_t *n);
  * random operand pairs. Expected 0. */
 piks_status piks_selftest_division(int32_t device, int64_t samples, uint64_t seed, int64_t *mismatches);
 
+/* The same self-test for hosts that cannot allocate device memory when they want to run
+ * it: a program that runs under a fixed device-memory budget, or that hands every device
+ * allocation to its own pool and does not allow other allocators, can still check the
+ * division. This entry point calls no allocator: its scratch is a static device buffer
+ * compiled into the library (8 KB of per-block counts and a total, held on every GPU
+ * that loads the library until the process exits). It accepts at most 16,777,216
+ * samples and returns PIKS_ERR_ARG with a message above that. The first call on a device
+ * looks up the buffer's device address, so make it before any stream capture. All calls
+ * share the buffer: calls that overlap on the GPU race, so do not run two at once. Runs on
+ * the default stream and returns after the result is on the host.
+ * Has no counterpart in the reference, which has no device code. */
+piks_status piks_selftest_division_noalloc(int32_t device, int64_t samples, uint64_t seed, int64_t *mismatches);
+
 piks_status piks_synchronize(piks_ctx *ctx);
 piks_status piks_destroy(piks_ctx *ctx);
 const char *piks_last_error(void);

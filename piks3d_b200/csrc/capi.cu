@@ -520,6 +520,15 @@ piks_status piks_selftest_division(int32_t device, int64_t samples, uint64_t see
   return st;
 }
 
+piks_status piks_selftest_division_noalloc(int32_t device, int64_t samples, uint64_t seed, int64_t *mismatches) {
+  if (!mismatches) return fail(PIKS_ERR_ARG, "null mismatches");
+  const char *err = "";
+  const int rc = division_selftest_noalloc(device, samples, seed, mismatches, &err);
+  if (rc == 1) return fail(PIKS_ERR_ARG, err);
+  if (rc) return fail(PIKS_ERR_CUDA, err);
+  return PIKS_OK;
+}
+
 piks_status piks_set_stream(piks_ctx *c, void *stream) {
   if (!c) return fail(PIKS_ERR_ARG, "null context");
   c->stream = stream ? static_cast<cudaStream_t>(stream) : c->own_stream;

@@ -468,6 +468,85 @@ __global__ void k_division_selftest(int64_t samples, uint64_t seed, unsigned lon
 
 }  // namespace
 
+// ---------------------------------------------------------------------------------------
+// Allocation-free variant of the division self-test (piks_selftest_division_noalloc).
+// Its scratch is this file-scope device array: one mismatch count per block of the test
+// grid and a final total. Every GPU that loads the library holds it (8 KB + 8 bytes) until
+// the process exits; all calls share it and it keeps the last call's contents.
+constexpr int kNoAllocBlocks = 1024;
+constexpr int kNoAllocThreads = 256;
+constexpr int64_t kNoAllocPerBlock = (int64_t)kNoAllocThreads * 64;   // samples per block
+static __device__ __align__(256) unsigned long long g_noalloc_scratch[kNoAllocBlocks + 1];
+
+__device__ __forceinline__ bool division_sample_differs(int64_t i, uint64_t seed) {
+  const uint64_t r1 = splitmix64(seed ^ (uint64_t)(2 * i)), r2 = splitmix64(seed ^ (uint64_t)(2 * i + 1));
+  const double num = random_double(r1, -40, 80);
+  double den = random_double(r2, -40, 80);
+  if (i & 1) den = fabs(random_double(r2, -2, 9));
+  const double y = __ddiv_rn(1.0, den);
+  return __double_as_longlong(markstein_div(num, den, y)) != __double_as_longlong(__ddiv_rn(num, den));
+}
+
+// Each block counts the mismatches of its own sample range and writes its slot; no slot
+// is read before this launch writes it, so nothing has to be cleared between calls.
+__global__ void __launch_bounds__(kNoAllocThreads)
+k_division_selftest_blocks(int64_t samples, uint64_t seed, unsigned long long *partial) {
+  __shared__ unsigned int warp_bad[kNoAllocThreads / 32];
+  const int64_t lo = (int64_t)blockIdx.x * kNoAllocPerBlock;
+  const int64_t hi = min(samples, lo + kNoAllocPerBlock);
+  unsigned int bad = 0;
+  for (int64_t i = lo + threadIdx.x; i < hi; i += kNoAllocThreads) bad += division_sample_differs(i, seed) ? 1u : 0u;
+  for (int off = 16; off > 0; off >>= 1) bad += __shfl_down_sync(0xffffffffu, bad, off);
+  if ((threadIdx.x & 31) == 0) warp_bad[threadIdx.x >> 5] = bad;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long t = 0;
+    for (int w = 0; w < kNoAllocThreads / 32; ++w) t += warp_bad[w];
+    partial[blockIdx.x] = t;
+  }
+}
+
+__global__ void k_sum_partials(const unsigned long long *partial, int n, unsigned long long *total) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    unsigned long long t = 0;
+    for (int b = 0; b < n; ++b) t += partial[b];
+    *total = t;
+  }
+}
+
+int division_selftest_noalloc(int device, int64_t samples, uint64_t seed, int64_t *mismatches, const char **err) {
+  static unsigned long long *scratch_of_device[64] = {nullptr};
+  if (device < 0 || device >= 64) { *err = "device index out of range"; return 1; }
+  if (samples <= 0) { *err = "samples must be positive"; return 1; }
+  const int64_t max_samples = (int64_t)kNoAllocBlocks * kNoAllocPerBlock;
+  if (samples > max_samples) {
+    *err = "samples exceeds 16777216, the most this allocation-free self-test runs with its static scratch";
+    return 1;
+  }
+  if (cudaSetDevice(device) != cudaSuccess) { *err = "cudaSetDevice failed"; return 4; }
+  if (!scratch_of_device[device]) {
+    // the host-side symbol is not a device address: look the device address up once per
+    // device, with that device current
+    void *ptr = nullptr;
+    if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) {
+      *err = "cudaGetSymbolAddress of the self-test scratch failed";
+      return 4;
+    }
+    scratch_of_device[device] = static_cast<unsigned long long *>(ptr);
+  }
+  unsigned long long *scratch = scratch_of_device[device];
+  const int blocks = (int)((samples + kNoAllocPerBlock - 1) / kNoAllocPerBlock);
+  k_division_selftest_blocks<<<blocks, kNoAllocThreads>>>(samples, seed, scratch);
+  k_sum_partials<<<1, 32>>>(scratch, blocks, scratch + kNoAllocBlocks);
+  unsigned long long total = 0;
+  if (cudaMemcpy(&total, scratch + kNoAllocBlocks, sizeof total, cudaMemcpyDeviceToHost) != cudaSuccess) {
+    *err = "self-test launch or copy failed";
+    return 4;
+  }
+  *mismatches = (int64_t)total;
+  return 0;
+}
+
 void launch_division_selftest(int64_t samples, uint64_t seed, unsigned long long *mismatches) {
   k_division_selftest<<<148 * 8, 256>>>(samples, seed, mismatches);
 }

@@ -55,5 +55,6 @@ void launch_moments(const DevState &s, cudaStream_t st);
 void launch_flux(const DevState &s, double ds, double sqrt_half, double inv_refl2, cudaStream_t st);
 void upload_tables();
 void launch_division_selftest(int64_t samples, uint64_t seed, unsigned long long *mismatches);
+int division_selftest_noalloc(int device, int64_t samples, uint64_t seed, int64_t *mismatches, const char **err);
 
 }  // namespace piks
