@@ -279,6 +279,19 @@ piks_status piks_setup_physical_grid(piks_ctx *c, const uint8_t *raw, int64_t nb
       }
     }
     UP(vt, vtab, pd);
+    if (v.Nc8 % 2 == 0) {
+      std::vector<double> v2((size_t)kVtab * v.Nc8);
+      for (int l = 0; l < v.Nc8; l += 2)
+        for (int k = 0; k < kVtab; ++k) {
+          v2[((size_t)(l / 2) * kVtab + k) * 2 + 0] = vt[(size_t)l * kVtab + k];
+          v2[((size_t)(l / 2) * kVtab + k) * 2 + 1] = vt[(size_t)(l + 1) * kVtab + k];
+        }
+      const double *pv2 = nullptr;
+      st = upload(c, v2, &pd);
+      if (st) return st;
+      pv2 = pd;
+      s.vtab2 = reinterpret_cast<const double2 *>(pv2);
+    }
     UP(g.tasks, tasks, pi);
   }
 #undef UP
@@ -289,10 +302,7 @@ piks_status piks_setup_physical_grid(piks_ctx *c, const uint8_t *raw, int64_t nb
   const size_t hsize = nnodes * 8 * (size_t)v.Nc8;
   if ((st = zeros(c, hsize, &s.h))) return st;                                   // flow.F90:92 f = 0
   if ((st = zeros(c, (size_t)g.nCorner * 8 * v.Nc8, &s.fw))) return st;         // physicalGrid.F90:1624
-  if ((st = zeros(c, (size_t)g.NF, &s.rho))) return st;
-  if ((st = zeros(c, (size_t)g.NF, &s.ux))) return st;
-  if ((st = zeros(c, (size_t)g.NF, &s.uy))) return st;
-  if ((st = zeros(c, (size_t)g.NF, &s.uz))) return st;
+  if ((st = zeros(c, (size_t)g.NF * 4, &s.mom))) return st;
   const size_t plane = (size_t)g.Ny * g.Nz * 4 * v.Nc8;
   for (int b = 0; b < 2; ++b) {                                                  // flow.F90:151-162
     if ((st = zeros(c, plane, &s.ghostW[b]))) return st;
@@ -347,20 +357,19 @@ piks_status piks_get_macro(piks_ctx *c, double *rho, double *ux, double *uy, dou
   if (!c || !c->have_geometry) return fail(PIKS_ERR_STATE, "no geometry");
   cudaSetDevice(c->device);
   const Geometry &g = c->geo;
-  std::vector<double> tmp(g.NF);
+  std::vector<double> tmp((size_t)g.NF * 4);
   double *dst[4] = {rho, ux, uy, uz};
-  double *src[4] = {c->ds.rho, c->ds.ux, c->ds.uy, c->ds.uz};
   const size_t box = (size_t)g.Nx * g.Ny * g.Nz;
+  piks_status st = cuda_check(cudaMemcpyAsync(tmp.data(), c->ds.mom, tmp.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "macro D2H");
+  if (!st) st = cuda_check(cudaStreamSynchronize(c->stream), "macro sync");
+  if (st) return st;
   for (int q = 0; q < 4; ++q) {
     if (!dst[q]) continue;
-    piks_status st = cuda_check(cudaMemcpyAsync(tmp.data(), src[q], g.NF * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "macro D2H");
-    if (!st) st = cuda_check(cudaStreamSynchronize(c->stream), "macro sync");
-    if (st) return st;
     std::memset(dst[q], 0, box * sizeof(double));
     for (int32_t n = 0; n < g.NF; ++n) {
       int64_t gi = g.node_g[n];
       int i = (int)(gi % g.GX) - 1, j = (int)((gi / g.GX) % g.GY) - 1, k = (int)(gi / ((int64_t)g.GX * g.GY)) - 1;
-      dst[q][(size_t)(i - 1) + (size_t)(j - 1) * g.Nx + (size_t)(k - 1) * g.Nx * g.Ny] = tmp[n];
+      dst[q][(size_t)(i - 1) + (size_t)(j - 1) * g.Nx + (size_t)(k - 1) * g.Nx * g.Ny] = tmp[(size_t)n * 4 + q];
     }
   }
   return PIKS_OK;

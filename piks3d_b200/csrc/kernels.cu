@@ -106,25 +106,39 @@ k_sweep(const DevState a, long t0, long ntask) {
   if (!fx) load_row<VPL>(a, r0.w, l0, x2);
   if (!fy) load_row<VPL>(a, r1.y, l0, y2);
   if (!fz) load_row<VPL>(a, r1.w, l0, z2);
-  const double rho = __ldg(a.rho + m), ux = __ldg(a.ux + m), uy = __ldg(a.uy + m), uz = __ldg(a.uz + m);
+  const double2 m01 = __ldg(reinterpret_cast<const double2 *>(a.mom) + 2 * (size_t)m);
+  const double2 m23 = __ldg(reinterpret_cast<const double2 *>(a.mom) + 2 * (size_t)m + 1);
+  const double rho = m01.x, ux = m01.y, uy = m23.x, uz = m23.y;
   const int cls = (fx ? 1 : 0) | (fy ? 2 : 0) | (fz ? 4 : 0);
   const bool nx_ = dsx(o) < 0, ny_ = dsy(o) < 0, nz_ = dsz(o) < 0;
+  // per-velocity constants: one 16-byte load gives both velocities of a lane (VPL = 2)
+  double K[kVtab][VPL];
+  if (VPL == 2) {
+    const double2 *vt = a.vtab2 + (size_t)(lfirst >> 1) * kVtab;
+#pragma unroll
+    for (int k = 0; k < 13; ++k) { const double2 t = __ldg(vt + k); K[k][0] = t.x; K[k][VPL - 1] = t.y; }
+    const double2 dn = __ldg(vt + 13 + cls), rc = __ldg(vt + 21 + cls);
+    K[13][0] = dn.x; K[13][VPL - 1] = dn.y; K[21][0] = rc.x; K[21][VPL - 1] = rc.y;
+  } else {
+    const double *vt = a.vtab + (size_t)lfirst * kVtab;
+#pragma unroll
+    for (int k = 0; k < 13; ++k) K[k][0] = __ldg(vt + k);
+    K[13][0] = __ldg(vt + 13 + cls); K[21][0] = __ldg(vt + 21 + cls);
+  }
   double out[VPL];
 #pragma unroll
   for (int q = 0; q < VPL; ++q) {
-    const int l = lfirst + q;
-    const double *vt = a.vtab + (size_t)l * kVtab;  // cx cy cz w, products, dens, recips
-    const double cx = __ldg(vt + 0), cy = __ldg(vt + 1), cz = __ldg(vt + 2), wl = __ldg(vt + 3);
+    const double cx = K[0][q], cy = K[1][q], cz = K[2][q], wl = K[3][q];
     const double ex = dmul(nx_ ? -cx : cx, ux), ey = dmul(ny_ ? -cy : cy, uy), ez = dmul(nz_ ? -cz : cz, uz);
     const double feq = dmul(wl, dadd(rho, dadd(dadd(ex, ey), ez)));
     double num = dmul(a.mu, dsub(feq, dmul(0.5, fold[q])));
-    num = dadd(num, dmul(__ldg(vt + (fx ? 5 : 4)), x1[q]));
-    if (!fx) num = dadd(num, dmul(__ldg(vt + 6), x2[q]));
-    num = dadd(num, dmul(__ldg(vt + (fy ? 8 : 7)), y1[q]));
-    if (!fy) num = dadd(num, dmul(__ldg(vt + 9), y2[q]));
-    num = dadd(num, dmul(__ldg(vt + (fz ? 11 : 10)), z1[q]));
-    if (!fz) num = dadd(num, dmul(__ldg(vt + 12), z2[q]));
-    out[q] = markstein_div(num, __ldg(vt + 13 + cls), __ldg(vt + 21 + cls));
+    num = dadd(num, dmul(fx ? K[5][q] : K[4][q], x1[q]));
+    if (!fx) num = dadd(num, dmul(K[6][q], x2[q]));
+    num = dadd(num, dmul(fy ? K[8][q] : K[7][q], y1[q]));
+    if (!fy) num = dadd(num, dmul(K[9][q], y2[q]));
+    num = dadd(num, dmul(fz ? K[11][q] : K[10][q], z1[q]));
+    if (!fz) num = dadd(num, dmul(K[12][q], z2[q]));
+    out[q] = markstein_div(num, K[13][q], K[21][q]);
   }
   double *hp = a.h + ((size_t)m * 8 + o) * (size_t)Nc8 + l0;
   if (VPL == 2) *reinterpret_cast<double2 *>(hp) = make_double2(out[0], out[VPL - 1]);
@@ -384,7 +398,9 @@ __global__ void __launch_bounds__(kMomWarps * 32) k_moments(const DevState a) {
   }
   if (lane < nvalid) {
     const int n = node0 + lane;
-    a.rho[n] = r; a.ux[n] = ux; a.uy[n] = uy; a.uz[n] = uz;
+    double2 *mp = reinterpret_cast<double2 *>(a.mom) + 2 * (size_t)n;
+    mp[0] = make_double2(r, ux);
+    mp[1] = make_double2(uy, uz);
   }
 }
 
@@ -404,7 +420,7 @@ __global__ void __launch_bounds__(256) k_flux(const DevState a, double ds, doubl
     __syncthreads();
     for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
       const int n = a.flux_list[base + e];
-      ux[e] = n >= 0 ? a.ux[n] : 0.0;
+      ux[e] = n >= 0 ? a.mom[4 * (size_t)n + 1] : 0.0;
     }
     __syncthreads();
     if (threadIdx.x == 0) {

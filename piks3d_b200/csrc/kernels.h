@@ -15,12 +15,13 @@ struct DevState {
   double *fw;                   // [corner][octant][Nc8] 3-fold corner storage
   const int32_t *bcorner;       // [NB] corner of a solid node or -1
   const uint16_t *roles;        // [NB][8] sources seen by y1/y2/z1/z2 readers
-  double *rho, *ux, *uy, *uz;   // [NF] moments
+  double *mom;                  // [NF][4] moments Rho, Ux, Uy, Uz
   const double *cx, *cy, *cz, *w;  // [Nc8]
   double mu;                    // sqrt(pi/2)/Kn
   double c15, c20, c05, c10;    // 1.5/ds, 2/ds, -0.5/ds, 1/ds (physicalGrid.F90:1259-1297)
   double accom, pressDrop, DiffFlux;
   const double *vtab;           // [Nc8][kVtab] per-velocity sweep constants (see kernels.cu)
+  const double2 *vtab2;         // [Nc8/2][kVtab] the same for velocity pairs (l, l+1), even Nc8
   const int32_t *tasks;         // sweep task records, 8 int32 each
   // walls
   int nWall;
