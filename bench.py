@@ -2,8 +2,10 @@
 """Benchmark of the B200 source-iteration solver (one JSON line on rank 0).
 
 Workload (N = 1, per rank): the 128^3 Boolean sphere pack (porosity 0.40, radii uniform
-in 4-8 voxels, seed 12345), 512 discrete velocities (Nc_fundamental = 4, half-range
-Gauss-Hermite), Kn = 0.5, plain FP64 solve. A step is one source iteration (8 octant
+in 4-8 voxels, seed 12345) with two fluid layers at inlet and outlet (fluidlayer = 2: with
+walls next to the periodic inlet/outlet planes the scheme's second-order wall
+extrapolation diverges), 512 discrete velocities (Nc_fundamental = 4, half-range
+Gauss-Hermite), Kn = 0.5, plain FP64 solve (--precision fp32: FP32 sweep). A step is one source iteration (8 octant
 sweeps, halo, wall, inlet/outlet and symmetry boundary conditions, moments). The metric
 is fluid voxel-velocity updates per second (N_fluid * Nv per iteration), whole job.
 
@@ -26,7 +28,7 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-WORKLOAD = dict(n=128, porosity=0.40, rmin=4.0, rmax=8.0, seed=12345, Nc_fundamental=4, Kn=0.5)
+WORKLOAD = dict(n=128, porosity=0.40, rmin=4.0, rmax=8.0, seed=12345, Nc_fundamental=4, Kn=0.5, fluidlayer=2)
 METRIC = "fluid voxel-velocity updates/s (plain FP64 source iteration)"
 UNIT = "Gupd/s"
 
@@ -40,13 +42,14 @@ def workload_image():
 def workload_params(pk):
     w = WORKLOAD
     return pk.default_params(Nx=w["n"], Ny=w["n"], Nz=w["n"], Nc_fundamental=w["Nc_fundamental"],
-                             Kn=w["Kn"], pressDrop=1.0, eps=1e-8, chkConvergeStep=10, maxStep=100000)
+                             Kn=w["Kn"], pressDrop=1.0, eps=1e-8, chkConvergeStep=10, maxStep=100000,
+                             fluidlayer=w["fluidlayer"])
 
 
 def config_dict(extra=None):
     w = WORKLOAD
-    d = {"workload": "sphere-pack %d^3 porosity %.2f radii %g-%g seed %d, Nv=%d, Kn=%g, FP64" % (
-        w["n"], w["porosity"], w["rmin"], w["rmax"], w["seed"], 8 * w["Nc_fundamental"] ** 3, w["Kn"]),
+    d = {"workload": "sphere-pack %d^3 porosity %.2f radii %g-%g seed %d, fluidlayer %d, Nv=%d, Kn=%g" % (
+        w["n"], w["porosity"], w["rmin"], w["rmax"], w["seed"], w["fluidlayer"], 8 * w["Nc_fundamental"] ** 3, w["Kn"]),
          "image": "%dx%dx%d uint8" % (w["n"], w["n"], w["n"]), "velocities": 8 * w["Nc_fundamental"] ** 3,
          "Kn": w["Kn"], "l2": "inputs larger than L2 (distribution function > 4 GB per rank)"}
     if extra:
@@ -184,7 +187,10 @@ def run_ours(args, world, rank, local):
     p = workload_params(pk)
 
     # --- device-resident run: value, roofline ---------------------------------------------
+    prec = pk.PREC_FP32 if args.precision == "fp32" else pk.PREC_FP64
+    esz = 4 if prec == pk.PREC_FP32 else 8
     s = pk.Solver(p, device=local)
+    s.set_precision(prec)
     s.setup_physical_grid(img)
     info = s.info()
     stream = torch.cuda.Stream(device=device)
@@ -203,8 +209,8 @@ def run_ours(args, world, rank, local):
                 f = f[:, 1:, :] if sy > 0 else f[:, :-1, :]
                 f = f[:, :, 1:] if sx > 0 else f[:, :, :-1]
                 swept += int(f.sum())
-    sweep_bytes = 16 * nc8 * swept + 32 * nf          # h read + write per swept update, moments read once
-    iter_bytes = 2 * 8 * nv * (nf + info["nWall"]) + 2 * 32 * nf
+    sweep_bytes = 2 * esz * nc8 * swept + 32 * nf     # h read + write per swept update, moments read once
+    iter_bytes = 2 * esz * nv * (nf + info["nWall"]) + 2 * 32 * nf
 
     s.iterate(args.warmup)
     s.synchronize()
@@ -235,6 +241,7 @@ def run_ours(args, world, rank, local):
     barrier(world, device)
     t0 = time.perf_counter()
     s2 = pk.Solver(p, device=local)
+    s2.set_precision(prec)
     s2.setup_physical_grid(img)                 # H2D: image -> geometry tables + zeroed state
     s2.iterate(args.steps)
     mass, perm, err = s2.chk_converge()          # D2H: mass flux
@@ -261,8 +268,10 @@ def run_ours(args, world, rank, local):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": config_dict({"Nfluid": nf, "nWall": info["nWall"], "parallelism": "replicas x%d" % world}),
+        "vs_baseline": None, "dtype": "f64" if esz == 8 else "f32 (moments, wall densities, flux f64)",
+        "data": "synthetic",
+        "config": config_dict({"Nfluid": nf, "nWall": info["nWall"], "parallelism": "replicas x%d" % world,
+                               "precision": args.precision}),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": None,
                      "kernel": "k_sweep (all tile-diagonal launches of one iteration)",
@@ -291,6 +300,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-iters", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],
+                    help="fp32: FP32 f and sweep, FP64 moments / wall densities / flux")
     ap.add_argument("--n", type=int, default=None,
                     help="image edge (default 128); smaller edges are for profiling captures, not bench lines")
     args = ap.parse_args()

@@ -96,7 +96,8 @@ piks_status piks_save_fields(piks_ctx *ctx, const char *dir, int32_t format);
  * 1 solid, 20..73 wall labels of physicalGrid.F90:127-134. */
 piks_status piks_get_labels(piks_ctx *ctx, int32_t *labels);
 
-/* Sizes: [Nx, Ny, Nz, Nc8, Nfluid, nWall, nCorner, nNodes, iStep, nWallLevels]. */
+/* Sizes: [Nx, Ny, Nz, Nc8, Nfluid, nWall, nCorner, nNodes, iStep, nWallLevels,
+ * device bytes held by the context]. */
 piks_status piks_get_info(piks_ctx *ctx, int64_t *info, int32_t n);
 
 /* Distribution function in the reference's layout f(Ntotal, Nc8, 8) over the ghosted box
@@ -138,6 +139,27 @@ piks_status piks_selftest_division(int32_t device, int64_t samples, uint64_t see
  * the default stream and returns after the result is on the host.
  * Has no counterpart in the reference, which has no device code. */
 piks_status piks_selftest_division_noalloc(int32_t device, int64_t samples, uint64_t seed, int64_t *mismatches);
+
+/* Storage and sweep precision of a context. PIKS_PREC_FP64 (the default) is the
+ * reference's arithmetic, operation for operation. PIKS_PREC_FP32 stores f, the 3-fold
+ * corner slots and the x ghost planes in FP32 and sweeps in FP32, while the moments
+ * (Rho, U), the diffuse-wall densities, the mass flux and the convergence test stay FP64.
+ * Switching a context that holds a state converts it on the device (FP32 -> FP64 widens
+ * exactly), so an FP32 solve can be continued in FP64: the refinement phase of
+ * piks_run_refined. Has no counterpart in the reference, which computes in FP64 only. */
+enum { PIKS_PREC_FP64 = 0, PIKS_PREC_FP32 = 1 };
+piks_status piks_set_precision(piks_ctx *ctx, int32_t precision);
+piks_status piks_get_precision(piks_ctx *ctx, int32_t *precision);
+
+/* FP32 solve with FP64 refinement: runs FP32 iterations with chkConverge every
+ * chkConvergeStep until error <= switch_eps (or until the error has not reached a new
+ * minimum for 5 checks in a row: the FP32 iterate has stopped improving), widens the state
+ * to FP64 and continues main.F90's loop in FP64 until error <= eps or maxStep iterations
+ * in total. Same files and stdout lines as piks_run; *steps32 receives the FP32
+ * iterations, *steps all iterations. No counterpart in the reference (FP64 only). */
+piks_status piks_run_refined(piks_ctx *ctx, const char *results_path, const char *out_dir, int32_t verbose,
+                             double switch_eps, int32_t *steps32, int32_t *steps, double *permeability,
+                             double *seconds);
 
 piks_status piks_synchronize(piks_ctx *ctx);
 piks_status piks_destroy(piks_ctx *ctx);

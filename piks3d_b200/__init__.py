@@ -83,6 +83,10 @@ def load_library(path=LIB_PATH):
         "piks_kernel_names": (ctypes.c_char_p, []),
         "piks_enable_timing": (i32, [c_void_p, i32]),
         "piks_launches_per_iteration": (i32, [c_void_p, P(i64)]),
+        "piks_set_precision": (i32, [c_void_p, i32]),
+        "piks_get_precision": (i32, [c_void_p, P(i32)]),
+        "piks_run_refined": (i32, [c_void_p, ctypes.c_char_p, ctypes.c_char_p, i32, dbl, P(i32), P(i32), P(dbl),
+                                   P(dbl)]),
         "piks_synchronize": (i32, [c_void_p]),
         "piks_destroy": (i32, [c_void_p]),
         "piks_last_error": (ctypes.c_char_p, []),
@@ -122,6 +126,8 @@ def read_params(path):
 def _dptr(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
 
+
+PREC_FP64, PREC_FP32 = 0, 1
 
 KERNEL_NAMES = ("sweep", "commit", "capture", "walls", "inlet_outlet", "symmetry", "moments", "flux")
 
@@ -177,14 +183,36 @@ class Solver:
                                  ctypes.byref(steps), ctypes.byref(perm), ctypes.byref(secs)))
         return steps.value, perm.value, secs.value
 
+    def run_refined(self, switch_eps=1e-6, results_path=None, out_dir=None, verbose=False):
+        """FP32 iterations until error <= switch_eps (or the FP32 error stops improving), then
+        FP64 iterations until error <= eps -> (fp32_steps, steps, permeability, seconds)."""
+        s32, steps, perm, secs = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_double(), ctypes.c_double()
+        _check(self.lib.piks_run_refined(self._ctx, os.fsencode(results_path) if results_path else None,
+                                         os.fsencode(out_dir) if out_dir else None, int(bool(verbose)),
+                                         float(switch_eps), ctypes.byref(s32), ctypes.byref(steps),
+                                         ctypes.byref(perm), ctypes.byref(secs)))
+        return s32.value, steps.value, perm.value, secs.value
+
+    def set_precision(self, precision):
+        """PREC_FP64 (reference arithmetic) or PREC_FP32 (FP32 f and sweep, FP64 moments,
+        wall densities and flux); converts a live state on the device."""
+        _check(self.lib.piks_set_precision(self._ctx, int(precision)))
+
+    @property
+    def precision(self):
+        v = ctypes.c_int32()
+        _check(self.lib.piks_get_precision(self._ctx, ctypes.byref(v)))
+        return v.value
+
     def synchronize(self):
         _check(self.lib.piks_synchronize(self._ctx))
 
     # -- data out -----------------------------------------------------------------------
     def info(self):
-        a = (ctypes.c_int64 * 10)()
-        _check(self.lib.piks_get_info(self._ctx, a, 10))
-        keys = ("Nx", "Ny", "Nz", "Nc8", "Nfluid", "nWall", "nCorner", "nNodes", "iStep", "nWallLevels")
+        a = (ctypes.c_int64 * 11)()
+        _check(self.lib.piks_get_info(self._ctx, a, 11))
+        keys = ("Nx", "Ny", "Nz", "Nc8", "Nfluid", "nWall", "nCorner", "nNodes", "iStep", "nWallLevels",
+                "device_bytes")
         return dict(zip(keys, list(a)))
 
     def get_macro(self):

@@ -2,6 +2,7 @@
 // the per-iteration launch schedule and the host-facing getters / writers.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -44,7 +45,9 @@ struct piks_ctx {
   bool have_geometry = false;       // device state ready
   bool have_host_geometry = false;  // preprocessing done
   DevState ds{};
-  std::vector<void *> allocations;
+  std::vector<std::pair<void *, size_t>> allocations;  // device buffers and their bytes
+  size_t dev_bytes = 0;
+  int prec = PIKS_PREC_FP64;        // storage / sweep precision of the state
   int iStep = 0;
   double mass = 1.0, error = 1.0, permeability = 0.0;
   bool timing = false;
@@ -69,7 +72,8 @@ piks_status upload(piks_ctx *c, const std::vector<T> &v, T **out, size_t min_cou
   void *p = nullptr;
   piks_status st = cuda_check(cudaMalloc(&p, n * sizeof(T)), "cudaMalloc");
   if (st) return st;
-  c->allocations.push_back(p);
+  c->allocations.push_back({p, n * sizeof(T)});
+  c->dev_bytes += n * sizeof(T);
   if (!v.empty()) {
     st = cuda_check(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, c->stream), "upload");
     if (st) return st;
@@ -83,7 +87,8 @@ piks_status zeros(piks_ctx *c, size_t n, T **out) {
   void *p = nullptr;
   piks_status st = cuda_check(cudaMalloc(&p, (n ? n : 1) * sizeof(T)), "cudaMalloc");
   if (st) return st;
-  c->allocations.push_back(p);
+  c->allocations.push_back({p, (n ? n : 1) * sizeof(T)});
+  c->dev_bytes += (n ? n : 1) * sizeof(T);
   st = cuda_check(cudaMemsetAsync(p, 0, (n ? n : 1) * sizeof(T), c->stream), "memset");
   if (st) return st;
   *out = static_cast<T *>(p);
@@ -91,9 +96,65 @@ piks_status zeros(piks_ctx *c, size_t n, T **out) {
 }
 
 void free_device(piks_ctx *c) {
-  for (void *p : c->allocations) cudaFree(p);
+  for (auto &a : c->allocations) cudaFree(a.first);
   c->allocations.clear();
+  c->dev_bytes = 0;
   c->have_geometry = false;
+}
+
+void release(piks_ctx *c, void *p) {
+  for (size_t i = 0; i < c->allocations.size(); ++i)
+    if (c->allocations[i].first == p) {
+      cudaFree(p);
+      c->dev_bytes -= c->allocations[i].second;
+      c->allocations.erase(c->allocations.begin() + (long)i);
+      return;
+    }
+}
+
+// Sizes of the precision-dependent state: f, fw and one ghost plane (in elements).
+struct StateSizes { size_t h, fw, plane; };
+StateSizes state_sizes(const piks_ctx *c) {
+  const Geometry &g = c->geo;
+  const size_t Nc8 = (size_t)c->vel.Nc8;
+  return {((size_t)g.NF + g.NB) * 8 * Nc8, (size_t)g.nCorner * 8 * Nc8, (size_t)g.Ny * g.Nz * 4 * Nc8};
+}
+
+// Allocates (zeroed) f, fw and the two pairs of ghost planes in precision `prec`
+// (flow.F90:92 f = 0, physicalGrid.F90:1624 fw = 0, flow.F90:151-162 ghosts = 0).
+piks_status alloc_state(piks_ctx *c, int prec) {
+  DevState &s = c->ds;
+  const StateSizes z = state_sizes(c);
+  piks_status st;
+  if (prec == PIKS_PREC_FP64) {
+    if ((st = zeros(c, z.h, &s.h))) return st;
+    if ((st = zeros(c, z.fw, &s.fw))) return st;
+    for (int b = 0; b < 2; ++b) {
+      if ((st = zeros(c, z.plane, &s.ghostW[b]))) return st;
+      if ((st = zeros(c, z.plane, &s.ghostE[b]))) return st;
+    }
+  } else {
+    if ((st = zeros(c, z.h, &s.h32))) return st;
+    if ((st = zeros(c, z.fw, &s.fw32))) return st;
+    for (int b = 0; b < 2; ++b) {
+      if ((st = zeros(c, z.plane, &s.ghostW32[b]))) return st;
+      if ((st = zeros(c, z.plane, &s.ghostE32[b]))) return st;
+    }
+  }
+  return PIKS_OK;
+}
+
+void free_state(piks_ctx *c, int prec) {
+  DevState &s = c->ds;
+  if (prec == PIKS_PREC_FP64) {
+    release(c, s.h); release(c, s.fw);
+    for (int b = 0; b < 2; ++b) { release(c, s.ghostW[b]); release(c, s.ghostE[b]); s.ghostW[b] = s.ghostE[b] = nullptr; }
+    s.h = s.fw = nullptr;
+  } else {
+    release(c, s.h32); release(c, s.fw32);
+    for (int b = 0; b < 2; ++b) { release(c, s.ghostW32[b]); release(c, s.ghostE32[b]); s.ghostW32[b] = s.ghostE32[b] = nullptr; }
+    s.h32 = s.fw32 = nullptr;
+  }
 }
 
 // Event-timed launch of one kernel group when timing is on.
@@ -136,21 +197,28 @@ void enqueue_iteration(piks_ctx *c) {
   cudaStream_t st = c->stream;
   const int n = c->iStep + 1;          // the iteration being run (1-based)
   const int cap = n & 1, prev = (n - 1) & 1;
+  const bool f32 = c->prec == PIKS_PREC_FP32;
   {
     Timed t(c, KT_SWEEP);
     const auto &hs = c->geo.hyper_start;
-    for (size_t h = 0; h + 1 < hs.size(); ++h) launch_sweep_hyperplane(s, hs[h], hs[h + 1] - hs[h], st);
+    for (size_t h = 0; h + 1 < hs.size(); ++h) {
+      if (f32) launch_sweep_hyperplane32(s, hs[h], hs[h + 1] - hs[h], st);
+      else launch_sweep_hyperplane(s, hs[h], hs[h + 1] - hs[h], st);
+    }
   }
-  { Timed t(c, KT_COMMIT); launch_commit(s, st); }
-  { Timed t(c, KT_CAPTURE); launch_capture(s, cap, st); }
+  { Timed t(c, KT_COMMIT); f32 ? launch_commit32(s, st) : launch_commit(s, st); }
+  { Timed t(c, KT_CAPTURE); f32 ? launch_capture32(s, cap, st) : launch_capture(s, cap, st); }
   {
     Timed t(c, KT_WALLS);
     const auto &ls = c->geo.level_start;
-    for (size_t L = 0; L + 1 < ls.size(); ++L) launch_walls(s, ls[L], ls[L + 1], prev, st);
+    for (size_t L = 0; L + 1 < ls.size(); ++L) {
+      if (f32) launch_walls32(s, ls[L], ls[L + 1], prev, st);
+      else launch_walls(s, ls[L], ls[L + 1], prev, st);
+    }
   }
-  { Timed t(c, KT_INLET); launch_inlet_outlet(s, prev, st); }
-  { Timed t(c, KT_SYM); launch_symmetry(s, st); }
-  { Timed t(c, KT_MOM); launch_moments(s, st); }
+  { Timed t(c, KT_INLET); f32 ? launch_inlet_outlet32(s, prev, st) : launch_inlet_outlet(s, prev, st); }
+  { Timed t(c, KT_SYM); f32 ? launch_symmetry32(s, st) : launch_symmetry(s, st); }
+  { Timed t(c, KT_MOM); f32 ? launch_moments32(s, st) : launch_moments(s, st); }
   c->iStep = n;
   if (c->timing && c->pending.size() > 4096) drain_timing(c);
 }
@@ -215,6 +283,7 @@ piks_status piks_create(const piks_params *p, int32_t device, piks_ctx **out) {
   if (st) { delete c; return st; }
   c->stream = c->own_stream;
   upload_tables();
+  upload_tables_fp32();
   st = cuda_check(cudaGetLastError(), "upload_tables");
   if (st) { cudaStreamDestroy(c->own_stream); delete c; return st; }
   *out = c;
@@ -279,6 +348,12 @@ piks_status piks_setup_physical_grid(piks_ctx *c, const uint8_t *raw, int64_t nb
       }
     }
     UP(vt, vtab, pd);
+    {
+      std::vector<float> v32(vt.begin(), vt.end());
+      float *pf = nullptr;
+      if ((st = upload(c, v32, &pf))) return st;
+      s.vtab32 = pf;
+    }
     if (v.Nc8 % 2 == 0) {
       std::vector<double> v2((size_t)kVtab * v.Nc8);
       for (int l = 0; l < v.Nc8; l += 2)
@@ -299,15 +374,9 @@ piks_status piks_setup_physical_grid(piks_ctx *c, const uint8_t *raw, int64_t nb
   s.ncommit = (int)(g.commit.size() / 3);
   s.nsym = (int)g.sym_node.size();
   for (int i = 0; i < 10; ++i) s.flux_groups[i] = g.flux_groups[i];
-  const size_t hsize = nnodes * 8 * (size_t)v.Nc8;
-  if ((st = zeros(c, hsize, &s.h))) return st;                                   // flow.F90:92 f = 0
-  if ((st = zeros(c, (size_t)g.nCorner * 8 * v.Nc8, &s.fw))) return st;         // physicalGrid.F90:1624
-  if ((st = zeros(c, (size_t)g.NF * 4, &s.mom))) return st;
-  const size_t plane = (size_t)g.Ny * g.Nz * 4 * v.Nc8;
-  for (int b = 0; b < 2; ++b) {                                                  // flow.F90:151-162
-    if ((st = zeros(c, plane, &s.ghostW[b]))) return st;
-    if ((st = zeros(c, plane, &s.ghostE[b]))) return st;
-  }
+  (void)nnodes;
+  if ((st = alloc_state(c, c->prec))) return st;
+  if ((st = zeros(c, (size_t)g.NF * 4, &s.mom))) return st;                      // flow.F90:93-96
   if ((st = zeros(c, (size_t)1, &s.flux_out))) return st;
   st = cuda_check(cudaStreamSynchronize(c->stream), "setup");
   if (st) return st;
@@ -388,9 +457,10 @@ piks_status piks_get_labels(piks_ctx *c, int32_t *labels) {
 piks_status piks_get_info(piks_ctx *c, int64_t *info, int32_t n) {
   if (!c || !info) return fail(PIKS_ERR_ARG, "null argument");
   const Geometry &g = c->geo;
-  int64_t v[10] = {c->setup.Nx, c->setup.Ny, c->setup.Nz, c->vel.Nc8, g.NF, g.nWall, g.nCorner,
-                   (int64_t)g.NF + g.NB, c->iStep, (int64_t)(g.level_start.empty() ? 0 : g.level_start.size() - 1)};
-  for (int i = 0; i < n && i < 10; ++i) info[i] = v[i];
+  int64_t v[11] = {c->setup.Nx, c->setup.Ny, c->setup.Nz, c->vel.Nc8, g.NF, g.nWall, g.nCorner,
+                   (int64_t)g.NF + g.NB, c->iStep, (int64_t)(g.level_start.empty() ? 0 : g.level_start.size() - 1),
+                   (int64_t)c->dev_bytes};
+  for (int i = 0; i < n && i < 11; ++i) info[i] = v[i];
   return PIKS_OK;
 }
 
@@ -401,11 +471,20 @@ piks_status piks_get_f(piks_ctx *c, double *f_ref, double *fw) {
   const int Nc8 = c->vel.Nc8;
   const size_t nnodes = (size_t)g.NF + g.NB;
   piks_status st;
+  const bool f32 = c->prec == PIKS_PREC_FP32;
   if (f_ref) {
     std::vector<double> h(nnodes * 8 * Nc8);
-    st = cuda_check(cudaMemcpyAsync(h.data(), c->ds.h, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "f D2H");
-    if (!st) st = cuda_check(cudaStreamSynchronize(c->stream), "f sync");
-    if (st) return st;
+    if (f32) {
+      std::vector<float> h32(h.size());
+      st = cuda_check(cudaMemcpyAsync(h32.data(), c->ds.h32, h32.size() * sizeof(float), cudaMemcpyDeviceToHost, c->stream), "f D2H");
+      if (!st) st = cuda_check(cudaStreamSynchronize(c->stream), "f sync");
+      if (st) return st;
+      std::copy(h32.begin(), h32.end(), h.begin());
+    } else {
+      st = cuda_check(cudaMemcpyAsync(h.data(), c->ds.h, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "f D2H");
+      if (!st) st = cuda_check(cudaStreamSynchronize(c->stream), "f sync");
+      if (st) return st;
+    }
     const size_t Ntot = (size_t)g.GX * g.GY * g.GZ;
     std::memset(f_ref, 0, Ntot * Nc8 * 8 * sizeof(double));
     for (size_t n = 0; n < nnodes; ++n)
@@ -415,9 +494,17 @@ piks_status piks_get_f(piks_ctx *c, double *f_ref, double *fw) {
   }
   if (fw && g.nCorner > 0) {
     std::vector<double> t((size_t)g.nCorner * 8 * Nc8);
-    st = cuda_check(cudaMemcpyAsync(t.data(), c->ds.fw, t.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "fw D2H");
-    if (!st) st = cuda_check(cudaStreamSynchronize(c->stream), "fw sync");
-    if (st) return st;
+    if (f32) {
+      std::vector<float> t32(t.size());
+      st = cuda_check(cudaMemcpyAsync(t32.data(), c->ds.fw32, t32.size() * sizeof(float), cudaMemcpyDeviceToHost, c->stream), "fw D2H");
+      if (!st) st = cuda_check(cudaStreamSynchronize(c->stream), "fw sync");
+      if (st) return st;
+      std::copy(t32.begin(), t32.end(), t.begin());
+    } else {
+      st = cuda_check(cudaMemcpyAsync(t.data(), c->ds.fw, t.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "fw D2H");
+      if (!st) st = cuda_check(cudaStreamSynchronize(c->stream), "fw sync");
+      if (st) return st;
+    }
     for (int cc = 0; cc < g.nCorner; ++cc)
       for (int o = 0; o < 8; ++o)
         for (int l = 0; l < Nc8; ++l)
@@ -440,38 +527,74 @@ piks_status piks_save_fields(piks_ctx *c, const char *dir, int32_t format) {
   return PIKS_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// chkConverge at `step` with main.F90's stdout line (:104-107) and Results.dat line
+// (output.F90:157-159).
+piks_status check_and_report(piks_ctx *c, int step, const char *results_path, int verbose) {
+  const piks_params &p = c->setup.p;
+  piks_status st = piks_chk_converge(c, nullptr, nullptr, nullptr);
+  if (st) return st;
+  if (verbose)
+    std::printf("%10d%s%s%s\n", step, fortran_es15_6(c->mass).c_str(), fortran_es15_6(c->permeability).c_str(),
+                fortran_es15_6(c->error).c_str());
+  if (results_path && results_path[0]) {
+    FILE *fh = std::fopen(results_path, "a");
+    if (!fh) return fail(PIKS_ERR_IO, std::string("cannot open ") + results_path);
+    std::fprintf(fh, "%s%s%s%s%15d\n", fortran_es15_6(p.Kn).c_str(), fortran_es15_6(c->mass).c_str(),
+                 fortran_es15_6(c->permeability).c_str(), fortran_es15_6(c->error).c_str(), step);
+    std::fclose(fh);
+  }
+  return PIKS_OK;
+}
+
+// main.F90:98-121 from iteration first_step on; stops at error <= eps, at maxStep, or (when
+// stop_on_stall) once the error has gone 5 checks without a new minimum. Returns the last
+// iteration run in *last.
+piks_status run_loop(piks_ctx *c, int first_step, double eps, bool stop_on_stall, const char *results_path,
+                     const char *out_dir, int verbose, int *last) {
+  const piks_params &p = c->setup.p;
+  piks_status st;
+  double best = HUGE_VAL;
+  int since_best = 0;
+  int step = first_step;
+  for (; step <= p.maxStep; ++step) {
+    if ((st = piks_iterate(c, 1))) return st;
+    if (step % p.chkConvergeStep == 0) {
+      if ((st = check_and_report(c, step, results_path, verbose))) return st;
+      if (c->error < best) { best = c->error; since_best = 0; } else ++since_best;
+    }
+    if (out_dir && p.saveStep > 0 && step % p.saveStep == 0)
+      if ((st = piks_save_fields(c, out_dir, p.saveFormat))) return st;
+    if (c->error <= eps) {
+      if (step < p.chkConvergeStep) {
+        if ((st = piks_chk_converge(c, nullptr, nullptr, nullptr))) return st;
+      }
+      break;
+    }
+    if (stop_on_stall && since_best >= 5) break;
+  }
+  *last = step > p.maxStep ? p.maxStep : step;
+  return PIKS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 piks_status piks_run(piks_ctx *c, const char *results_path, const char *out_dir, int32_t verbose,
                      int32_t *steps, double *perm, double *seconds) {
   if (!c || !c->have_geometry) return fail(PIKS_ERR_STATE, "no geometry");
   const piks_params &p = c->setup.p;
   c->error = 1.0;  // main.F90:95
   auto t0 = std::chrono::steady_clock::now();
-  int step;
-  piks_status st;
-  for (step = 1; step <= p.maxStep; ++step) {
-    if ((st = piks_iterate(c, 1))) return st;
-    if (step % p.chkConvergeStep == 0) {
-      if ((st = piks_chk_converge(c, nullptr, nullptr, nullptr))) return st;
-      if (verbose)
-        std::printf("%10d%s%s%s\n", step, fortran_es15_6(c->mass).c_str(), fortran_es15_6(c->permeability).c_str(),
-                    fortran_es15_6(c->error).c_str());
-      if (results_path && results_path[0]) {
-        FILE *fh = std::fopen(results_path, "a");
-        if (!fh) return fail(PIKS_ERR_IO, std::string("cannot open ") + results_path);
-        std::fprintf(fh, "%s%s%s%s%15d\n", fortran_es15_6(p.Kn).c_str(), fortran_es15_6(c->mass).c_str(),
-                     fortran_es15_6(c->permeability).c_str(), fortran_es15_6(c->error).c_str(), step);
-        std::fclose(fh);
-      }
-    }
-    if (out_dir && p.saveStep > 0 && step % p.saveStep == 0)
-      if ((st = piks_save_fields(c, out_dir, p.saveFormat))) return st;
-    if (c->error <= p.eps) {
-      if (step < p.chkConvergeStep) {
-        if ((st = piks_chk_converge(c, nullptr, nullptr, nullptr))) return st;
-      }
-      break;
-    }
-  }
+  int step = 0;
+  piks_status st = run_loop(c, 1, p.eps, false, results_path, out_dir, verbose, &step);
+  if (st) return st;
+  // the reference's loop variable ends one past maxStep when the loop runs out
+  if (c->error > p.eps) step = p.maxStep + 1;
   cudaStreamSynchronize(c->stream);
   double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   if (verbose) {
@@ -481,6 +604,80 @@ piks_status piks_run(piks_ctx *c, const char *results_path, const char *out_dir,
   }
   if (out_dir && p.saveLast)
     if ((st = piks_save_fields(c, out_dir, p.saveFormat))) return st;
+  if (steps) *steps = step;
+  if (perm) *perm = c->permeability;
+  if (seconds) *seconds = secs;
+  return PIKS_OK;
+}
+
+piks_status piks_set_precision(piks_ctx *c, int32_t precision) {
+  if (!c) return fail(PIKS_ERR_ARG, "null context");
+  if (precision != PIKS_PREC_FP64 && precision != PIKS_PREC_FP32) return fail(PIKS_ERR_ARG, "unknown precision");
+  if (c->device < 0 || !c->have_geometry || precision == c->prec) { c->prec = precision; return PIKS_OK; }
+  cudaSetDevice(c->device);
+  piks_status st = cuda_check(cudaStreamSynchronize(c->stream), "precision sync");
+  if (st) return st;
+  if ((st = alloc_state(c, precision))) { free_state(c, precision); return st; }
+  DevState &s = c->ds;
+  const StateSizes z = state_sizes(c);
+  if (precision == PIKS_PREC_FP64) {
+    launch_widen(s.h32, s.h, z.h, c->stream);
+    launch_widen(s.fw32, s.fw, z.fw, c->stream);
+    for (int b = 0; b < 2; ++b) {
+      launch_widen(s.ghostW32[b], s.ghostW[b], z.plane, c->stream);
+      launch_widen(s.ghostE32[b], s.ghostE[b], z.plane, c->stream);
+    }
+  } else {
+    launch_narrow(s.h, s.h32, z.h, c->stream);
+    launch_narrow(s.fw, s.fw32, z.fw, c->stream);
+    for (int b = 0; b < 2; ++b) {
+      launch_narrow(s.ghostW[b], s.ghostW32[b], z.plane, c->stream);
+      launch_narrow(s.ghostE[b], s.ghostE32[b], z.plane, c->stream);
+    }
+  }
+  st = cuda_check(cudaGetLastError(), "precision convert");
+  if (!st) st = cuda_check(cudaStreamSynchronize(c->stream), "precision convert");
+  if (st) return st;
+  free_state(c, c->prec);
+  c->prec = precision;
+  return PIKS_OK;
+}
+
+piks_status piks_get_precision(piks_ctx *c, int32_t *precision) {
+  if (!c || !precision) return fail(PIKS_ERR_ARG, "null argument");
+  *precision = c->prec;
+  return PIKS_OK;
+}
+
+piks_status piks_run_refined(piks_ctx *c, const char *results_path, const char *out_dir, int32_t verbose,
+                             double switch_eps, int32_t *steps32, int32_t *steps, double *perm, double *seconds) {
+  if (!c || !c->have_geometry) return fail(PIKS_ERR_STATE, "no geometry");
+  if (!(switch_eps >= 0.0)) return fail(PIKS_ERR_ARG, "switch_eps < 0");
+  const piks_params &p = c->setup.p;
+  c->error = 1.0;
+  auto t0 = std::chrono::steady_clock::now();
+  piks_status st = piks_set_precision(c, PIKS_PREC_FP32);
+  if (st) return st;
+  int last32 = 0, step = 0;
+  const int first = c->iStep + 1;
+  if ((st = run_loop(c, first, std::max(switch_eps, p.eps), true, results_path, out_dir, verbose, &last32))) return st;
+  const int n32 = last32 - first + 1;
+  if ((st = piks_set_precision(c, PIKS_PREC_FP64))) return st;
+  step = last32;
+  if (last32 < p.maxStep) {
+    // the FP64 phase starts from the widened FP32 iterate and applies the reference's test
+    if ((st = run_loop(c, last32 + 1, p.eps, false, results_path, out_dir, verbose, &step))) return st;
+  }
+  cudaStreamSynchronize(c->stream);
+  const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  if (verbose) {
+    char wt[32];
+    std::snprintf(wt, sizeof wt, "%11.3E", secs);
+    std::printf("Walltime= %s, Steps= %6d, K= %s\n", wt, step, fortran_es15_6(c->permeability).c_str());
+  }
+  if (out_dir && p.saveLast)
+    if ((st = piks_save_fields(c, out_dir, p.saveFormat))) return st;
+  if (steps32) *steps32 = n32;
   if (steps) *steps = step;
   if (perm) *perm = c->permeability;
   if (seconds) *seconds = secs;

@@ -41,6 +41,11 @@ struct DevState {
   const int32_t *flux_list;
   int flux_groups[10];
   double *flux_out;             // [1]
+  // FP32 storage of the same state (used instead of h/fw/ghost* when the context runs the
+  // FP32 sweep); moments, wall densities and the flux stay FP64
+  float *h32, *fw32;
+  float *ghostW32[2], *ghostE32[2];
+  const float *vtab32;          // [Nc8][kVtab] sweep constants rounded to FP32
 };
 
 // Per-velocity sweep constants: cx cy cz w, then c*C products (x: 2/ds, 1/ds, -0.5/ds;
@@ -55,6 +60,17 @@ void launch_symmetry(const DevState &s, cudaStream_t st);
 void launch_moments(const DevState &s, cudaStream_t st);
 void launch_flux(const DevState &s, double ds, double sqrt_half, double inv_refl2, cudaStream_t st);
 void upload_tables();
+// FP32 path (kernels_fp32.cu)
+void upload_tables_fp32();
+void launch_sweep_hyperplane32(const DevState &s, long t0, long ntask, cudaStream_t st);
+void launch_commit32(const DevState &s, cudaStream_t st);
+void launch_capture32(const DevState &s, int buf, cudaStream_t st);
+void launch_walls32(const DevState &s, int begin, int end, int gbuf, cudaStream_t st);
+void launch_inlet_outlet32(const DevState &s, int buf, cudaStream_t st);
+void launch_symmetry32(const DevState &s, cudaStream_t st);
+void launch_moments32(const DevState &s, cudaStream_t st);
+void launch_widen(const float *src, double *dst, size_t n, cudaStream_t st);
+void launch_narrow(const double *src, float *dst, size_t n, cudaStream_t st);
 void launch_division_selftest(int64_t samples, uint64_t seed, unsigned long long *mismatches);
 int division_selftest_noalloc(int device, int64_t samples, uint64_t seed, int64_t *mismatches, const char **err);
 

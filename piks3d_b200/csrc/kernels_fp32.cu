@@ -1,0 +1,330 @@
+// FP32 path of the source iteration: the distribution function, the wall slots, the
+// 3-fold corner storage and the ghost planes are stored and swept in FP32; the moments
+// (Rho, U), the diffuse-wall densities, the mass flux and the convergence test stay FP64
+// (the moments and the flux reuse the FP64 arrays of DevState). The data flow is the one
+// of kernels.cu (same tasks, roles, commits, wall programs and boundary order); only the
+// arithmetic type differs, so the FP32 iterate approximates the FP64 one.
+#include <cuda_runtime.h>
+
+#include "kernels.h"
+#include "piks_internal.h"
+
+namespace piks {
+
+namespace {
+
+__constant__ WProg c32_prog[26];
+__constant__ int8_t c32_prog_of[128];
+__constant__ int c32_incoming[6][4];
+
+__device__ __forceinline__ size_t hidx(int node, int o, int Nc8, int l) {
+  return ((size_t)node * 8 + o) * (size_t)Nc8 + l;
+}
+__device__ __forceinline__ int plane_slot(int o) { return o >> 1; }
+constexpr int kFwBit = 1 << 30;
+
+template <int VPL>
+__device__ __forceinline__ void ld32(const float *p, float (&v)[VPL]) {
+  if (VPL == 2) { const float2 t = __ldcg(reinterpret_cast<const float2 *>(p)); v[0] = t.x; v[VPL - 1] = t.y; }
+  else v[0] = __ldcg(p);
+}
+template <int VPL>
+__device__ __forceinline__ void st32(float *p, const float (&v)[VPL]) {
+  if (VPL == 2) *reinterpret_cast<float2 *>(p) = make_float2(v[0], v[VPL - 1]);
+  else p[0] = v[0];
+}
+
+// Hyperplane sweep task (same task records as the FP64 kernel); upwind rows from h32/fw32.
+template <int LPT, int VPL>
+__global__ void __launch_bounds__(256)
+k_sweep32(const DevState a, long t0, long ntask) {
+  const long gl = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long slot = gl / LPT;
+  const int sub = (int)(gl % LPT);
+  const long ti = slot / a.nchunk;
+  const int chunk = (int)(slot - ti * a.nchunk);
+  if (ti >= ntask) return;
+  const int Nc8 = a.Nc8;
+  const int lfirst = chunk * LPT * VPL + sub * VPL;
+  if (lfirst >= Nc8) return;
+  const int4 *rec = reinterpret_cast<const int4 *>(a.tasks + (size_t)(t0 + ti) * 8);
+  const int4 r0 = __ldg(rec), r1 = __ldg(rec + 1);
+  const int m = r0.x, fl = r0.y;
+  const int o = fl & 7;
+  const bool fx = fl & 8, fy = fl & 16, fz = fl & 32;
+  auto row = [&](int code, float (&v)[VPL]) {
+    const float *base = (code & kFwBit) ? a.fw32 : a.h32;
+    ld32<VPL>(base + (size_t)(code & ~kFwBit) * (size_t)Nc8 + lfirst, v);
+  };
+  float fold[VPL], x1[VPL], x2[VPL], y1[VPL], y2[VPL], z1[VPL], z2[VPL];
+  row(m * 8 + o, fold);
+  row(r0.z, x1);
+  row(r1.x, y1);
+  row(r1.z, z1);
+  if (!fx) row(r0.w, x2);
+  if (!fy) row(r1.y, y2);
+  if (!fz) row(r1.w, z2);
+  const double2 m01 = __ldg(reinterpret_cast<const double2 *>(a.mom) + 2 * (size_t)m);
+  const double2 m23 = __ldg(reinterpret_cast<const double2 *>(a.mom) + 2 * (size_t)m + 1);
+  const float rho = (float)m01.x, ux = (float)m01.y, uy = (float)m23.x, uz = (float)m23.y;
+  const int cls = (fx ? 1 : 0) | (fy ? 2 : 0) | (fz ? 4 : 0);
+  const float sxf = (o == 0 || o == 3 || o == 4 || o == 7) ? 1.f : -1.f;
+  const float syf = (o == 0 || o == 1 || o == 4 || o == 5) ? 1.f : -1.f;
+  const float szf = o < 4 ? 1.f : -1.f;
+  const float mu = (float)a.mu;
+  float out[VPL];
+#pragma unroll
+  for (int q = 0; q < VPL; ++q) {
+    const float *vt = a.vtab32 + (size_t)(lfirst + q) * kVtab;
+    const float cx = __ldg(vt + 0), cy = __ldg(vt + 1), cz = __ldg(vt + 2), wl = __ldg(vt + 3);
+    const float feq = wl * (rho + (sxf * cx * ux + syf * cy * uy + szf * cz * uz));
+    float num = mu * (feq - 0.5f * fold[q]);
+    num += __ldg(vt + (fx ? 5 : 4)) * x1[q];
+    if (!fx) num += __ldg(vt + 6) * x2[q];
+    num += __ldg(vt + (fy ? 8 : 7)) * y1[q];
+    if (!fy) num += __ldg(vt + 9) * y2[q];
+    num += __ldg(vt + (fz ? 11 : 10)) * z1[q];
+    if (!fz) num += __ldg(vt + 12) * z2[q];
+    out[q] = num * __ldg(vt + 21 + cls);
+  }
+  st32<VPL>(a.h32 + ((size_t)m * 8 + o) * (size_t)Nc8 + lfirst, out);
+}
+
+__global__ void k_commit32(const DevState a) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (size_t)a.ncommit * a.Nc8) return;
+  const int e = (int)(idx / a.Nc8), l = (int)(idx % a.Nc8);
+  const int node = a.commit[3 * e], o = a.commit[3 * e + 1], src = a.commit[3 * e + 2];
+  a.h32[hidx(node, o, a.Nc8, l)] = src < 8 ? a.h32[hidx(node, src, a.Nc8, l)]
+                                           : a.fw32[hidx(a.bcorner[node - a.NF], o, a.Nc8, l)];
+}
+
+__global__ void k_capture32(const DevState a, int buf) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (size_t)a.Ny * a.Nz * 4 * a.Nc8) return;
+  const int l = (int)(idx % a.Nc8);
+  const int q = (int)((idx / a.Nc8) % 4);
+  const size_t r = idx / ((size_t)a.Nc8 * 4);
+  const int oW = q == 0 ? 0 : q == 1 ? 3 : q == 2 ? 4 : 7;
+  const int oE = q == 0 ? 1 : q == 1 ? 2 : q == 2 ? 5 : 6;
+  const int nW = a.plane_xN[r], nE = a.plane_x1[r];
+  a.ghostW32[buf][idx] = nW >= 0 ? a.h32[hidx(nW, oW, a.Nc8, l)] : 0.f;
+  a.ghostE32[buf][idx] = nE >= 0 ? a.h32[hidx(nE, oE, a.Nc8, l)] : 0.f;
+}
+
+// Walls: extrapolation and re-emission in FP32, the wall densities summed in FP64 (in the
+// reference's order over l) and the re-emitted value formed in FP64 before rounding.
+template <int VPL>
+__global__ void __launch_bounds__(256) k_walls32(const DevState a, int begin, int end, int gbuf) {
+  const int widx = begin + (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  if (widx >= end) return;
+  const int lane = threadIdx.x & 31;
+  const int q = a.wall_order[widx];
+  const int node = a.wall_node[q];
+  const int corner = a.wall_corner[q];
+  const WProg &P = c32_prog[c32_prog_of[a.wall_label[q]]];
+  const float e1 = (float)a.wall_e[2 * q], e2 = (float)a.wall_e[2 * q + 1];
+  const int Nc8 = a.Nc8;
+  const int *nb = a.wall_nb + 6 * q;
+  const int nface = P.nface;
+  const int chunkw = 32 * VPL;
+  auto far_ptr = [&](int code, int oo, int lf) -> const float * {
+    if (code >= 0) return a.h32 + hidx(code, oo, Nc8, lf);
+    if (code == -1) return nullptr;
+    const int cc = -code - 2;
+    const float *plane = (cc & 1) ? a.ghostE32[gbuf] : a.ghostW32[gbuf];
+    return plane + ((size_t)(cc >> 1) * 4 + plane_slot(oo)) * Nc8 + lf;
+  };
+  double rho0 = 0.0, rho1 = 0.0, rho2 = 0.0;
+  for (int fi = 0; fi < nface; ++fi) {
+    const int dir = P.face[fi].dir, st = P.face[fi].store;
+    const int n1 = nb[2 * fi], code = nb[2 * fi + 1];
+    double racc = 0.0;
+    for (int l0 = 0; l0 < Nc8; l0 += chunkw) {
+      const int lf = l0 + lane * VPL;
+      const bool lv = lf < Nc8;
+      float ext[4][VPL];
+#pragma unroll
+      for (int mm = 0; mm < 4; ++mm) {
+        const int oo = c32_incoming[dir][mm] - 1;
+        float nv[VPL], fv[VPL];
+#pragma unroll
+        for (int v = 0; v < VPL; ++v) { nv[v] = 0.f; fv[v] = 0.f; }
+        if (lv) {
+          ld32<VPL>(a.h32 + hidx(n1, oo, Nc8, lf), nv);
+          const float *fp = far_ptr(code, oo, lf);
+          if (fp) ld32<VPL>(fp, fv);
+        }
+#pragma unroll
+        for (int v = 0; v < VPL; ++v) ext[mm][v] = e1 * nv[v] + e2 * fv[v];
+        if (lv) {
+          if (st == ST_F) st32<VPL>(a.h32 + hidx(node, oo, Nc8, lf), ext[mm]);
+          else if (st == ST_W) st32<VPL>(a.fw32 + hidx(corner, oo, Nc8, lf), ext[mm]);
+        }
+      }
+      double tface[VPL];
+#pragma unroll
+      for (int v = 0; v < VPL; ++v) {
+        const int l = lf + v;
+        const double ca = !lv ? 0.0 : dir < 2 ? __ldg(a.cx + l) : dir < 4 ? __ldg(a.cy + l) : __ldg(a.cz + l);
+        tface[v] = ca * (((double)ext[0][v] + (double)ext[1][v]) + (double)ext[2][v] + (double)ext[3][v]);
+      }
+      const int nl = min(chunkw, Nc8 - l0);
+      for (int sidx = 0; sidx < nl; ++sidx) {
+        const int srcl = sidx / VPL, v = sidx % VPL;
+        racc += __shfl_sync(0xffffffffu, (VPL == 2 && v == 1) ? tface[VPL - 1] : tface[0], srcl);
+      }
+    }
+    if (fi == 0) rho0 = racc; else if (fi == 1) rho1 = racc; else rho2 = racc;
+  }
+  rho0 /= a.DiffFlux; rho1 /= a.DiffFlux; rho2 /= a.DiffFlux;
+  const double one_m = 1.0 - a.accom;
+  int zface = -1;
+  for (int fi = 0; fi < nface; ++fi) if (P.face[fi].store == ST_Z) zface = fi;
+  for (int l0 = 0; l0 < Nc8; l0 += chunkw) {
+    const int lf = l0 + lane * VPL;
+    if (lf >= Nc8) continue;
+    for (int r = 0; r < P.nwr; ++r) {
+      const WWrite &W = P.wr[r];
+      const int so = W.src_o - 1, dso = W.dst_o - 1;
+      float src[VPL];
+      if (W.src_store == ST_F) ld32<VPL>(a.h32 + hidx(node, so, Nc8, lf), src);
+      else if (W.src_store == ST_W) ld32<VPL>(a.fw32 + hidx(corner, so, Nc8, lf), src);
+      else {
+        float nv[VPL], fv[VPL];
+        ld32<VPL>(a.h32 + hidx(nb[2 * zface], so, Nc8, lf), nv);
+#pragma unroll
+        for (int v = 0; v < VPL; ++v) fv[v] = 0.f;
+        const float *fp = far_ptr(nb[2 * zface + 1], so, lf);
+        if (fp) ld32<VPL>(fp, fv);
+#pragma unroll
+        for (int v = 0; v < VPL; ++v) src[v] = e1 * nv[v] + e2 * fv[v];
+      }
+      const double rf = W.face == 0 ? rho0 : W.face == 1 ? rho1 : rho2;
+      float val[VPL];
+#pragma unroll
+      for (int v = 0; v < VPL; ++v) val[v] = (float)(a.accom * __ldg(a.w + lf + v) * rf + one_m * (double)src[v]);
+      if (W.dst_store == ST_F) st32<VPL>(a.h32 + hidx(node, dso, Nc8, lf), val);
+      else st32<VPL>(a.fw32 + hidx(corner, dso, Nc8, lf), val);
+    }
+  }
+}
+
+__global__ void k_inlet_outlet32(const DevState a, int gbuf) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (size_t)a.Ny * a.Nz * 4 * a.Nc8) return;
+  const int l = (int)(idx % a.Nc8);
+  const int q = (int)((idx / a.Nc8) % 4);
+  const size_t r = idx / ((size_t)a.Nc8 * 4);
+  const float wdp = (float)(a.w[l] * a.pressDrop);
+  const int n1 = a.plane_x1[r], nN = a.plane_xN[r];
+  if (n1 >= 0) a.h32[hidx(n1, q == 0 ? 0 : q == 1 ? 3 : q == 2 ? 4 : 7, a.Nc8, l)] = a.ghostW32[gbuf][idx] + wdp;
+  if (nN >= 0) a.h32[hidx(nN, q == 0 ? 1 : q == 1 ? 2 : q == 2 ? 5 : 6, a.Nc8, l)] = a.ghostE32[gbuf][idx] - wdp;
+}
+
+__global__ void k_symmetry32(const DevState a) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (size_t)a.nsym * a.Nc8) return;
+  const int s = (int)(idx / a.Nc8), l = (int)(idx % a.Nc8);
+  const uint8_t f = a.sym_flag[s];
+  float *hp = a.h32 + (size_t)a.sym_node[s] * 8 * a.Nc8 + l;
+  const size_t S = a.Nc8;
+  if (f & 1) { hp[1 * S] = hp[2 * S]; hp[0 * S] = hp[3 * S]; hp[5 * S] = hp[6 * S]; hp[4 * S] = hp[7 * S]; }
+  if (f & 2) { hp[2 * S] = hp[1 * S]; hp[3 * S] = hp[0 * S]; hp[6 * S] = hp[5 * S]; hp[7 * S] = hp[4 * S]; }
+  if (f & 4) { hp[0 * S] = hp[4 * S]; hp[1 * S] = hp[5 * S]; hp[2 * S] = hp[6 * S]; hp[3 * S] = hp[7 * S]; }
+  if (f & 8) { hp[4 * S] = hp[0 * S]; hp[5 * S] = hp[1 * S]; hp[6 * S] = hp[2 * S]; hp[7 * S] = hp[3 * S]; }
+}
+
+// Moments in FP64 from FP32 values: a warp per node, lanes over velocities, partial sums
+// combined with a warp reduction (the FP32 path does not follow the reference's order).
+__global__ void __launch_bounds__(256) k_moments32(const DevState a) {
+  const int node = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  if (node >= a.NF) return;
+  const int lane = threadIdx.x & 31;
+  const int Nc8 = a.Nc8;
+  const float *hp = a.h32 + (size_t)node * 8 * Nc8;
+  double r = 0.0, ux = 0.0, uy = 0.0, uz = 0.0;
+  for (int l = lane; l < Nc8; l += 32) {
+    const double f1 = __ldcs(hp + 0 * Nc8 + l), f2 = __ldcs(hp + 1 * Nc8 + l), f3 = __ldcs(hp + 2 * Nc8 + l),
+                 f4 = __ldcs(hp + 3 * Nc8 + l), f5 = __ldcs(hp + 4 * Nc8 + l), f6 = __ldcs(hp + 5 * Nc8 + l),
+                 f7 = __ldcs(hp + 6 * Nc8 + l), f8 = __ldcs(hp + 7 * Nc8 + l);
+    r += ((f1 + f2) + (f3 + f4)) + ((f5 + f6) + (f7 + f8));
+    ux += __ldg(a.cx + l) * (((f1 - f2) + (f4 - f3)) + ((f5 - f6) + (f8 - f7)));
+    uy += __ldg(a.cy + l) * (((f1 + f2) - (f3 + f4)) + ((f5 + f6) - (f7 + f8)));
+    uz += __ldg(a.cz + l) * (((f1 + f2) + (f3 + f4)) - ((f5 + f6) + (f7 + f8)));
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    r += __shfl_down_sync(0xffffffffu, r, off);
+    ux += __shfl_down_sync(0xffffffffu, ux, off);
+    uy += __shfl_down_sync(0xffffffffu, uy, off);
+    uz += __shfl_down_sync(0xffffffffu, uz, off);
+  }
+  if (lane == 0) {
+    double2 *mp = reinterpret_cast<double2 *>(a.mom) + 2 * (size_t)node;
+    mp[0] = make_double2(r, ux);
+    mp[1] = make_double2(uy, uz);
+  }
+}
+
+__global__ void k_widen(const float *src, double *dst, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    dst[i] = (double)src[i];
+}
+
+__global__ void k_narrow(const double *src, float *dst, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    dst[i] = (float)src[i];
+}
+
+inline unsigned nblocks(size_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+}  // namespace
+
+void upload_tables_fp32() {
+  int8_t prog_of[128];
+  WProg progs[26];
+  int n = 0;
+  for (int lab = 0; lab < 128; ++lab) {
+    prog_of[lab] = -1;
+    const WProg *p = wall_program(lab);
+    if (p) { progs[n] = *p; prog_of[lab] = (int8_t)n; ++n; }
+  }
+  cudaMemcpyToSymbol(c32_prog_of, prog_of, sizeof prog_of);
+  cudaMemcpyToSymbol(c32_prog, progs, sizeof progs);
+  cudaMemcpyToSymbol(c32_incoming, kIncoming, sizeof(int) * 24);
+}
+
+void launch_sweep_hyperplane32(const DevState &s, long t0, long ntask, cudaStream_t st) {
+  if (ntask <= 0) return;
+  if (s.lpt == 32) k_sweep32<32, 2><<<nblocks((size_t)ntask * s.nchunk * 32, 256), 256, 0, st>>>(s, t0, ntask);
+  else k_sweep32<8, 1><<<nblocks((size_t)ntask * s.nchunk * 8, 256), 256, 0, st>>>(s, t0, ntask);
+}
+void launch_commit32(const DevState &s, cudaStream_t st) {
+  if (s.ncommit) k_commit32<<<nblocks((size_t)s.ncommit * s.Nc8, 256), 256, 0, st>>>(s);
+}
+void launch_capture32(const DevState &s, int buf, cudaStream_t st) {
+  k_capture32<<<nblocks((size_t)s.Ny * s.Nz * 4 * s.Nc8, 256), 256, 0, st>>>(s, buf);
+}
+void launch_walls32(const DevState &s, int begin, int end, int gbuf, cudaStream_t st) {
+  if (end <= begin) return;
+  const size_t threads = (size_t)(end - begin) * 32;
+  if (s.Nc8 % 64 == 0) k_walls32<2><<<nblocks(threads, 256), 256, 0, st>>>(s, begin, end, gbuf);
+  else k_walls32<1><<<nblocks(threads, 256), 256, 0, st>>>(s, begin, end, gbuf);
+}
+void launch_inlet_outlet32(const DevState &s, int buf, cudaStream_t st) {
+  k_inlet_outlet32<<<nblocks((size_t)s.Ny * s.Nz * 4 * s.Nc8, 256), 256, 0, st>>>(s, buf);
+}
+void launch_symmetry32(const DevState &s, cudaStream_t st) {
+  if (s.nsym) k_symmetry32<<<nblocks((size_t)s.nsym * s.Nc8, 256), 256, 0, st>>>(s);
+}
+void launch_moments32(const DevState &s, cudaStream_t st) {
+  if (s.NF) k_moments32<<<nblocks((size_t)s.NF * 32, 256), 256, 0, st>>>(s);
+}
+void launch_widen(const float *src, double *dst, size_t n, cudaStream_t st) {
+  if (n) k_widen<<<148 * 16, 256, 0, st>>>(src, dst, n);
+}
+void launch_narrow(const double *src, float *dst, size_t n, cudaStream_t st) {
+  if (n) k_narrow<<<148 * 16, 256, 0, st>>>(src, dst, n);
+}
+
+}  // namespace piks
