@@ -151,6 +151,17 @@ enum { PIKS_PREC_FP64 = 0, PIKS_PREC_FP32 = 1 };
 piks_status piks_set_precision(piks_ctx *ctx, int32_t precision);
 piks_status piks_get_precision(piks_ctx *ctx, int32_t *precision);
 
+/* Sweep schedule. The default cuts the box into 8x8x8 tiles and sweeps, for each octant,
+ * the tiles in diagonal order, each tile's local hyperplanes in shared memory (one launch
+ * per tile diagonal). tx = 0 selects the per-node hyperplane schedule (one launch per
+ * voxel hyperplane u+v+w). Both give identical results; the tile schedule also falls back
+ * to the per-node one when a tile needs more rows than shared memory holds. Takes effect
+ * at the next piks_setup_physical_grid. No counterpart in the reference (its sweep is a
+ * serial raster loop per octant). */
+piks_status piks_set_tiles(piks_ctx *ctx, int32_t tx, int32_t ty, int32_t tz);
+/* [tile schedule in use (0/1), TX, TY, TZ, largest shared-memory slot count of a job] */
+piks_status piks_get_schedule(piks_ctx *ctx, int32_t *out, int32_t n);
+
 /* FP32 solve with FP64 refinement: runs FP32 iterations with chkConverge every
  * chkConvergeStep until error <= switch_eps (or until the error has not reached a new
  * minimum for 5 checks in a row: the FP32 iterate has stopped improving), widens the state

@@ -84,6 +84,8 @@ def load_library(path=LIB_PATH):
         "piks_enable_timing": (i32, [c_void_p, i32]),
         "piks_launches_per_iteration": (i32, [c_void_p, P(i64)]),
         "piks_set_precision": (i32, [c_void_p, i32]),
+        "piks_set_tiles": (i32, [c_void_p, i32, i32, i32]),
+        "piks_get_schedule": (i32, [c_void_p, P(i32), i32]),
         "piks_get_precision": (i32, [c_void_p, P(i32)]),
         "piks_run_refined": (i32, [c_void_p, ctypes.c_char_p, ctypes.c_char_p, i32, dbl, P(i32), P(i32), P(dbl),
                                    P(dbl)]),
@@ -198,6 +200,19 @@ class Solver:
         wall densities and flux); converts a live state on the device."""
         _check(self.lib.piks_set_precision(self._ctx, int(precision)))
 
+    def set_tiles(self, tx, ty=None, tz=None):
+        """Tile shape of the sweep schedule (0 = per-node hyperplanes); applies at the next
+        setup_physical_grid."""
+        ty = tx if ty is None else ty
+        tz = tx if tz is None else tz
+        _check(self.lib.piks_set_tiles(self._ctx, int(tx), int(ty), int(tz)))
+
+    def schedule(self):
+        """{'tiles': bool, 'TX', 'TY', 'TZ', 'max_slots'} of the sweep schedule in use."""
+        a = (ctypes.c_int32 * 5)()
+        _check(self.lib.piks_get_schedule(self._ctx, a, 5))
+        return {"tiles": bool(a[0]), "TX": a[1], "TY": a[2], "TZ": a[3], "max_slots": a[4]}
+
     @property
     def precision(self):
         v = ctypes.c_int32()
@@ -239,7 +254,8 @@ class Solver:
         return f, fw[: inf["nCorner"] * inf["Nc8"] * 8]
 
     _GEO_DTYPES = {"label": np.uint8, "sym_flag": np.uint8, "roles": np.uint16, "wall_e": np.float64,
-                   "hyper_start": np.int64,
+                   "hyper_start": np.int64, "tile_row_begin": np.int64, "tile_task_begin": np.int64,
+                   "tile_steps": np.uint16,
                    "cx": np.float64, "cy": np.float64, "cz": np.float64, "w": np.float64}
 
     def geometry_array(self, name):

@@ -48,6 +48,9 @@ struct piks_ctx {
   std::vector<std::pair<void *, size_t>> allocations;  // device buffers and their bytes
   size_t dev_bytes = 0;
   int prec = PIKS_PREC_FP64;        // storage / sweep precision of the state
+  int tile_dims[3] = {8, 8, 8};     // tile shape of the sweep schedule (0: per-node hyperplanes)
+  TileJobs tiles;
+  bool use_tiles = false;           // tile schedule built and uploaded
   int iStep = 0;
   double mass = 1.0, error = 1.0, permeability = 0.0;
   bool timing = false;
@@ -200,10 +203,16 @@ void enqueue_iteration(piks_ctx *c) {
   const bool f32 = c->prec == PIKS_PREC_FP32;
   {
     Timed t(c, KT_SWEEP);
-    const auto &hs = c->geo.hyper_start;
-    for (size_t h = 0; h + 1 < hs.size(); ++h) {
-      if (f32) launch_sweep_hyperplane32(s, hs[h], hs[h + 1] - hs[h], st);
-      else launch_sweep_hyperplane(s, hs[h], hs[h + 1] - hs[h], st);
+    if (c->use_tiles) {
+      const auto &db = c->tiles.diag_begin;
+      for (size_t d = 0; d + 1 < db.size(); ++d)
+        launch_tile_sweep(s, f32, db[d], db[d + 1] - db[d], c->tiles.diag_rows[d], st);
+    } else {
+      const auto &hs = c->geo.hyper_start;
+      for (size_t h = 0; h + 1 < hs.size(); ++h) {
+        if (f32) launch_sweep_hyperplane32(s, hs[h], hs[h + 1] - hs[h], st);
+        else launch_sweep_hyperplane(s, hs[h], hs[h + 1] - hs[h], st);
+      }
     }
   }
   { Timed t(c, KT_COMMIT); f32 ? launch_commit32(s, st) : launch_commit(s, st); }
@@ -298,6 +307,13 @@ piks_status piks_setup_physical_grid(piks_ctx *c, const uint8_t *raw, int64_t nb
   piks_status st = preprocess(c->setup, raw, nbytes, c->geo, err);
   if (st) return fail(st, err);
   c->have_host_geometry = true;
+  c->use_tiles = false;
+  c->tiles = TileJobs{};
+  if (c->tile_dims[0] > 0) {
+    const int slots = std::min(tile_sweep_max_slots(c->vel.Nc8, false), tile_sweep_max_slots(c->vel.Nc8, true));
+    c->use_tiles = build_tile_jobs(c->geo, c->tile_dims[0], c->tile_dims[1], c->tile_dims[2], slots, c->tiles);
+    if (!c->use_tiles) c->tiles = TileJobs{};
+  }
   if (c->device < 0) return PIKS_OK;
   const Geometry &g = c->geo;
   const Velocity &v = c->vel;
@@ -368,6 +384,18 @@ piks_status piks_setup_physical_grid(piks_ctx *c, const uint8_t *raw, int64_t nb
       s.vtab2 = reinterpret_cast<const double2 *>(pv2);
     }
     UP(g.tasks, tasks, pi);
+  }
+  if (c->use_tiles) {
+    const TileJobs &tj = c->tiles;
+    int64_t *p64 = nullptr;
+    UP(tj.rows, tv.rows, pi);
+    UP(tj.row_begin, tv.row_begin, p64);
+    if ((st = upload(c, tj.tasks, &pi))) return st;
+    s.tv.tasks = reinterpret_cast<const int4 *>(pi);
+    UP(tj.task_begin, tv.task_begin, p64);
+    uint16_t *p16 = nullptr;
+    UP(tj.steps, tv.steps, p16);
+    s.tv.nsteps = tj.nsteps;
   }
 #undef UP
   s.nWall = g.nWall;
@@ -643,6 +671,21 @@ piks_status piks_set_precision(piks_ctx *c, int32_t precision) {
   return PIKS_OK;
 }
 
+piks_status piks_set_tiles(piks_ctx *c, int32_t tx, int32_t ty, int32_t tz) {
+  if (!c) return fail(PIKS_ERR_ARG, "null context");
+  if (tx < 0 || ty < 0 || tz < 0 || (tx > 0 && (ty < 2 || tz < 2 || tx < 2)) || (int64_t)tx * ty * tz > 65535)
+    return fail(PIKS_ERR_ARG, "tile extents must be 0 (per-node schedule) or >= 2 with at most 65535 voxels");
+  c->tile_dims[0] = tx; c->tile_dims[1] = tx ? ty : 0; c->tile_dims[2] = tx ? tz : 0;
+  return PIKS_OK;
+}
+
+piks_status piks_get_schedule(piks_ctx *c, int32_t *out, int32_t n) {
+  if (!c || !out) return fail(PIKS_ERR_ARG, "null argument");
+  const int32_t v[5] = {c->use_tiles ? 1 : 0, c->tiles.TX, c->tiles.TY, c->tiles.TZ, c->tiles.max_rows};
+  for (int i = 0; i < n && i < 5; ++i) out[i] = v[i];
+  return PIKS_OK;
+}
+
 piks_status piks_get_precision(piks_ctx *c, int32_t *precision) {
   if (!c || !precision) return fail(PIKS_ERR_ARG, "null argument");
   *precision = c->prec;
@@ -700,6 +743,10 @@ piks_status piks_geometry_array(piks_ctx *c, const char *name, void *out, int64_
   ARR("bcorner", g.bcorner) ARR("roles", g.roles) ARR("commit", g.commit) ARR("plane_x1", g.plane_x1)
   ARR("plane_xN", g.plane_xN) ARR("sym_node", g.sym_node) ARR("sym_flag", g.sym_flag)
   ARR("flux_list", g.flux_list) ARR("tasks", g.tasks) ARR("hyper_start", g.hyper_start) ARR("cx", c->vel.cx) ARR("cy", c->vel.cy) ARR("cz", c->vel.cz) ARR("w", c->vel.w)
+  const TileJobs &tj = c->tiles;
+  ARR("tile_rows", tj.rows) ARR("tile_row_begin", tj.row_begin) ARR("tile_tasks", tj.tasks)
+  ARR("tile_task_begin", tj.task_begin) ARR("tile_steps", tj.steps) ARR("tile_diag_begin", tj.diag_begin)
+  ARR("tile_diag_rows", tj.diag_rows)
 #undef ARR
   if (nm == "flux_groups") { src = g.flux_groups; n = 10; esz = sizeof(int32_t); }
   if (!esz) return fail(PIKS_ERR_ARG, "unknown geometry array " + nm);
@@ -760,7 +807,12 @@ piks_status piks_launches_per_iteration(piks_ctx *c, int64_t *n) {
   if (!c || !n || !c->have_geometry) return fail(PIKS_ERR_STATE, "no geometry");
   const DevState &s = c->ds;
   int64_t k = 0;
-  for (size_t h = 0; h + 1 < c->geo.hyper_start.size(); ++h) k += c->geo.hyper_start[h + 1] > c->geo.hyper_start[h];
+  if (c->use_tiles) {
+    const auto &db = c->tiles.diag_begin;
+    for (size_t d = 0; d + 1 < db.size(); ++d) k += db[d + 1] > db[d];
+  } else {
+    for (size_t h = 0; h + 1 < c->geo.hyper_start.size(); ++h) k += c->geo.hyper_start[h + 1] > c->geo.hyper_start[h];
+  }
   k += (s.ncommit > 0) + 1 /*capture*/ + (int64_t)(c->geo.level_start.size() - 1) + 1 /*inlet*/ +
        (s.nsym > 0) + (s.NF > 0);
   *n = k;

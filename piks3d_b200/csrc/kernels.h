@@ -5,6 +5,16 @@
 
 namespace piks {
 
+// Device copy of the tile-wavefront schedule (TileJobs in piks_internal.h).
+struct TileView {
+  const int32_t *rows;          // global row codes of every job's shared-memory slots 1..
+  const int64_t *row_begin;     // [njobs + 1]
+  const int4 *tasks;            // node | fx<<27 | fy<<28 | fz<<29, slots x1|x2<<16, y1|y2<<16, z1|z2<<16
+  const int64_t *task_begin;    // [njobs + 1]
+  const uint16_t *steps;        // [njobs][nsteps + 1] task offsets of the local hyperplanes
+  int nsteps;
+};
+
 // Everything the kernels read, as device pointers (one struct passed by value).
 struct DevState {
   int Nx, Ny, Nz, GX, GXY;      // interior extents; ghosted row / plane strides
@@ -46,6 +56,7 @@ struct DevState {
   float *h32, *fw32;
   float *ghostW32[2], *ghostE32[2];
   const float *vtab32;          // [Nc8][kVtab] sweep constants rounded to FP32
+  TileView tv;                  // tile-wavefront sweep schedule (when built)
 };
 
 // Per-velocity sweep constants: cx cy cz w, then c*C products (x: 2/ds, 1/ds, -0.5/ds;
@@ -69,6 +80,11 @@ void launch_walls32(const DevState &s, int begin, int end, int gbuf, cudaStream_
 void launch_inlet_outlet32(const DevState &s, int buf, cudaStream_t st);
 void launch_symmetry32(const DevState &s, cudaStream_t st);
 void launch_moments32(const DevState &s, cudaStream_t st);
+// Tile-wavefront sweep: the jobs [job0, job0 + njobs) of one diagonal, `slots` shared-memory
+// rows per CTA. tile_sweep_velocities() is the chunk width V used for the precision.
+int tile_sweep_velocities(int Nc8, bool fp32);
+int tile_sweep_max_slots(int Nc8, bool fp32);
+void launch_tile_sweep(const DevState &s, bool fp32, int job0, int njobs, int slots, cudaStream_t st);
 void launch_widen(const float *src, double *dst, size_t n, cudaStream_t st);
 void launch_narrow(const double *src, float *dst, size_t n, cudaStream_t st);
 void launch_division_selftest(int64_t samples, uint64_t seed, unsigned long long *mismatches);

@@ -91,6 +91,34 @@ struct Geometry {
   }
 };
 
+// Tile-wavefront form of the sweep tasks. The box is cut into TX x TY x TZ tiles; a job is
+// one (tile, octant): its swept fluid nodes, ordered by the local hyperplane index of the
+// octant's frame inside the tile (the steps), and the unique rows they read or write.
+// Jobs are grouped by the tile hyperplane index of the octant's frame (the diagonals): the
+// jobs of one diagonal are independent, and every row a job reads from another tile was
+// written by a job of an earlier diagonal.
+struct TileJobs {
+  int TX = 0, TY = 0, TZ = 0;
+  int nsteps = 0;                    // TX + TY + TZ - 2 local hyperplanes per tile
+  // rows of each job (global row codes as in Geometry::tasks): the job's own rows first,
+  // in task order, then the other rows it reads; shared-memory slot = 1 + position
+  // (slot 0 is a row of zeros)
+  std::vector<int32_t> rows;
+  std::vector<int64_t> row_begin;    // njobs + 1
+  // per task: node | fx<<27 | fy<<28 | fz<<29, then the slots of x1 | x2<<16, y1 | y2<<16,
+  // z1 | z2<<16; the task's own slot is 1 + its index within the job
+  std::vector<int32_t> tasks;        // 4 int32 per task
+  std::vector<int64_t> task_begin;   // njobs + 1
+  std::vector<uint16_t> steps;       // [njobs][nsteps + 1] task offsets within the job
+  std::vector<int32_t> diag_begin;   // job offset of each diagonal (+1 end entry)
+  std::vector<int32_t> diag_rows;    // largest slot count (rows + zero row) per diagonal
+  int32_t max_rows = 0;
+};
+
+// Builds the tile jobs from g.tasks; returns false when a job needs more than max_slots
+// shared-memory rows (the caller then keeps the hyperplane schedule).
+bool build_tile_jobs(const Geometry &g, int TX, int TY, int TZ, int max_slots, TileJobs &tj);
+
 piks_status make_setup(const piks_params &p, Setup &s, std::string &err);
 piks_status make_velocity(const piks_params &p, Velocity &v, std::string &err);
 piks_status preprocess(const Setup &s, const uint8_t *raw, int64_t nbytes, Geometry &g, std::string &err);

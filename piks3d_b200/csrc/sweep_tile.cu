@@ -1,0 +1,223 @@
+// Tile-wavefront octant sweep (solver.F90:176-526) over the TileJobs schedule.
+//
+// One CTA runs one job (a tile of the box for one octant) for one chunk of V velocities:
+//  1. it copies every row the job touches (its own rows, the upwind rows of neighbouring
+//     tiles, the wall rows seen by its readers) into shared memory with cp.async, V
+//     velocities (one 128-byte segment for V*sizeof(T) = 128) per row;
+//  2. it sweeps the tile's local hyperplanes in order, a group of V/2 lanes per task with
+//     two velocities per lane, reading every upwind value from shared memory and writing
+//     the new value to the task's own slot (one barrier per non-empty hyperplane);
+//  3. it writes the own rows back.
+// Jobs of one diagonal run in one launch; rows a job reads from another tile were written
+// by an earlier launch. Each update applies the same operations to the same operands as
+// the per-node FP64 kernel, so the FP64 result is unchanged by the schedule.
+#include <cuda_runtime.h>
+
+#include "kernels.h"
+
+namespace piks {
+
+namespace {
+
+constexpr int kFwBit = 1 << 30;
+constexpr int kGroups = 16;  // task groups per CTA
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+// RN(num/den) from y = RN(1/den) with Markstein's correction step (see kernels.cu).
+__device__ __forceinline__ double markstein_div(double num, double den, double y) {
+  const double q0 = __dmul_rn(num, y);
+  const double r = __fma_rn(-q0, den, num);
+  return __fma_rn(r, y, q0);
+}
+
+template <typename T> struct Pair;
+template <> struct Pair<double> { using type = double2; };
+template <> struct Pair<float> { using type = float2; };
+
+template <typename T> __device__ __forceinline__ const T *state_h(const DevState &a);
+template <> __device__ __forceinline__ const double *state_h<double>(const DevState &a) { return a.h; }
+template <> __device__ __forceinline__ const float *state_h<float>(const DevState &a) { return a.h32; }
+template <typename T> __device__ __forceinline__ const T *state_fw(const DevState &a);
+template <> __device__ __forceinline__ const double *state_fw<double>(const DevState &a) { return a.fw; }
+template <> __device__ __forceinline__ const float *state_fw<float>(const DevState &a) { return a.fw32; }
+
+template <typename T, int V>
+__global__ void __launch_bounds__(V / 2 * kGroups)
+k_tile_sweep(const DevState a, int job0) {
+  constexpr int LPT = V / 2;                        // lanes per task
+  constexpr int THREADS = LPT * kGroups;
+  constexpr int EPP = 16 / (int)sizeof(T);          // elements per 16-byte piece
+  constexpr int PIECES = V / EPP;                   // pieces per row
+  using T2 = typename Pair<T>::type;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *S = reinterpret_cast<T *>(smem_raw);
+
+  const TileView &tv = a.tv;
+  const int Nc8 = a.Nc8;
+  const int nchunk = Nc8 / V;
+  const int job = job0 + (int)(blockIdx.x / nchunk);
+  const int chunk = (int)(blockIdx.x % nchunk);
+  const int l0 = chunk * V;
+  const int64_t rb = tv.row_begin[job];
+  const int nrows = (int)(tv.row_begin[job + 1] - rb);
+  const int64_t tb = tv.task_begin[job];
+  const int ntask = (int)(tv.task_begin[job + 1] - tb);
+  const T *h = state_h<T>(a);
+  const T *fw = state_fw<T>(a);
+
+  // 1. rows -> shared memory (slot 0 = zeros)
+  for (int i = threadIdx.x; i < nrows * PIECES; i += THREADS) {
+    const int r = i / PIECES, pc = i - r * PIECES;
+    const int code = __ldg(tv.rows + rb + r);
+    const T *src = ((code & kFwBit) ? fw : h) + (size_t)(code & ~kFwBit) * (size_t)Nc8 + l0 + pc * EPP;
+    cp_async16(S + (size_t)(1 + r) * V + pc * EPP, src);
+  }
+  if (threadIdx.x < PIECES) *reinterpret_cast<int4 *>(S + threadIdx.x * EPP) = make_int4(0, 0, 0, 0);
+
+  // per-lane constants of its two velocities
+  const int grp = threadIdx.x / LPT, sub = threadIdx.x % LPT;
+  const int lp = l0 + 2 * sub;
+  const int o = __ldg(tv.rows + rb) & 7;            // own row code = node * 8 + octant
+  const bool nx_ = !(o == 0 || o == 3 || o == 4 || o == 7);
+  const bool ny_ = !(o == 0 || o == 1 || o == 4 || o == 5);
+  const bool nz_ = o >= 4;
+  T K[13][2];
+  if constexpr (sizeof(T) == 8) {
+    const double2 *vt = a.vtab2 + (size_t)(lp >> 1) * kVtab;
+#pragma unroll
+    for (int k = 0; k < 13; ++k) { const double2 t = __ldg(vt + k); K[k][0] = t.x; K[k][1] = t.y; }
+  } else {
+#pragma unroll
+    for (int k = 0; k < 13; ++k) {
+      K[k][0] = __ldg(a.vtab32 + (size_t)lp * kVtab + k);
+      K[k][1] = __ldg(a.vtab32 + (size_t)(lp + 1) * kVtab + k);
+    }
+  }
+  cp_async_wait_all();
+  __syncthreads();
+
+  // 2. local hyperplanes
+  const uint16_t *st = tv.steps + (size_t)job * (tv.nsteps + 1);
+  for (int s = 0; s < tv.nsteps; ++s) {
+    const int t0 = st[s], t1 = st[s + 1];
+    if (t0 == t1) continue;
+    for (int t = t0 + grp; t < t1; t += kGroups) {
+      const int4 rec = __ldg(tv.tasks + tb + t);
+      const int m = rec.x & ((1 << 27) - 1);
+      const bool fx = (rec.x >> 27) & 1, fy = (rec.x >> 28) & 1, fz = (rec.x >> 29) & 1;
+      const int cls = (fx ? 1 : 0) | (fy ? 2 : 0) | (fz ? 4 : 0);
+      auto ld = [&](int slot) { return *reinterpret_cast<const T2 *>(S + (size_t)slot * V + 2 * sub); };
+      const T2 fold = ld(1 + t);
+      const T2 x1 = ld(rec.y & 0xffff), y1 = ld(rec.z & 0xffff), z1 = ld(rec.w & 0xffff);
+      T2 x2{}, y2{}, z2{};
+      if (!fx) x2 = ld((unsigned)rec.y >> 16);
+      if (!fy) y2 = ld((unsigned)rec.z >> 16);
+      if (!fz) z2 = ld((unsigned)rec.w >> 16);
+      const double2 m01 = __ldg(reinterpret_cast<const double2 *>(a.mom) + 2 * (size_t)m);
+      const double2 m23 = __ldg(reinterpret_cast<const double2 *>(a.mom) + 2 * (size_t)m + 1);
+      const T fo[2] = {fold.x, fold.y}, vx1[2] = {x1.x, x1.y}, vx2[2] = {x2.x, x2.y}, vy1[2] = {y1.x, y1.y},
+              vy2[2] = {y2.x, y2.y}, vz1[2] = {z1.x, z1.y}, vz2[2] = {z2.x, z2.y};
+      T out[2];
+      if constexpr (sizeof(T) == 8) {
+        const double rho = m01.x, ux = m01.y, uy = m23.x, uz = m23.y;
+        const double2 dn = __ldg(a.vtab2 + (size_t)(lp >> 1) * kVtab + 13 + cls);
+        const double2 rc = __ldg(a.vtab2 + (size_t)(lp >> 1) * kVtab + 21 + cls);
+        const double den[2] = {dn.x, dn.y}, rcp[2] = {rc.x, rc.y};
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          const double cx = K[0][q], cy = K[1][q], cz = K[2][q], wl = K[3][q];
+          const double ex = dmul(nx_ ? -cx : cx, ux), ey = dmul(ny_ ? -cy : cy, uy), ez = dmul(nz_ ? -cz : cz, uz);
+          const double feq = dmul(wl, dadd(rho, dadd(dadd(ex, ey), ez)));
+          double num = dmul(a.mu, dsub(feq, dmul(0.5, fo[q])));
+          num = dadd(num, dmul(fx ? K[5][q] : K[4][q], vx1[q]));
+          if (!fx) num = dadd(num, dmul(K[6][q], vx2[q]));
+          num = dadd(num, dmul(fy ? K[8][q] : K[7][q], vy1[q]));
+          if (!fy) num = dadd(num, dmul(K[9][q], vy2[q]));
+          num = dadd(num, dmul(fz ? K[11][q] : K[10][q], vz1[q]));
+          if (!fz) num = dadd(num, dmul(K[12][q], vz2[q]));
+          out[q] = markstein_div(num, den[q], rcp[q]);
+        }
+      } else {
+        const float rho = (float)m01.x, ux = (float)m01.y, uy = (float)m23.x, uz = (float)m23.y;
+        const float mu = (float)a.mu;
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          const float cx = K[0][q], cy = K[1][q], cz = K[2][q], wl = K[3][q];
+          const float rcp = __ldg(a.vtab32 + (size_t)(lp + q) * kVtab + 21 + cls);
+          const float feq = wl * (rho + ((nx_ ? -cx : cx) * ux + (ny_ ? -cy : cy) * uy + (nz_ ? -cz : cz) * uz));
+          float num = mu * (feq - 0.5f * fo[q]);
+          num += (fx ? K[5][q] : K[4][q]) * vx1[q];
+          if (!fx) num += K[6][q] * vx2[q];
+          num += (fy ? K[8][q] : K[7][q]) * vy1[q];
+          if (!fy) num += K[9][q] * vy2[q];
+          num += (fz ? K[11][q] : K[10][q]) * vz1[q];
+          if (!fz) num += K[12][q] * vz2[q];
+          out[q] = num * rcp;
+        }
+      }
+      T2 res;
+      res.x = out[0];
+      res.y = out[1];
+      *reinterpret_cast<T2 *>(S + (size_t)(1 + t) * V + 2 * sub) = res;
+    }
+    __syncthreads();
+  }
+
+  // 3. own rows -> global
+  T *hw = const_cast<T *>(h);
+  for (int i = threadIdx.x; i < ntask * PIECES; i += THREADS) {
+    const int r = i / PIECES, pc = i - r * PIECES;
+    const int code = __ldg(tv.rows + rb + r);
+    *reinterpret_cast<int4 *>(hw + (size_t)code * Nc8 + l0 + pc * EPP) =
+        *reinterpret_cast<const int4 *>(S + (size_t)(1 + r) * V + pc * EPP);
+  }
+}
+
+template <typename T, int V>
+void launch_one(const DevState &s, int job0, int njobs, int slots, cudaStream_t st) {
+  static unsigned long long configured = 0;  // one bit per device
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!(configured >> (dev & 63) & 1ull)) {
+    cudaFuncSetAttribute(k_tile_sweep<T, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    configured |= 1ull << (dev & 63);
+  }
+  const size_t smem = (size_t)slots * V * sizeof(T);
+  const unsigned grid = (unsigned)((size_t)njobs * (s.Nc8 / V));
+  k_tile_sweep<T, V><<<grid, V / 2 * kGroups, smem, st>>>(s, job0);
+}
+
+}  // namespace
+
+int tile_sweep_velocities(int Nc8, bool fp32) {
+  if (fp32) return Nc8 % 32 == 0 ? 32 : Nc8 % 16 == 0 ? 16 : 8;
+  return Nc8 % 16 == 0 ? 16 : 8;
+}
+
+int tile_sweep_max_slots(int Nc8, bool fp32) {
+  const int row = tile_sweep_velocities(Nc8, fp32) * (fp32 ? 4 : 8);
+  return (227 * 1024) / row;
+}
+
+void launch_tile_sweep(const DevState &s, bool fp32, int job0, int njobs, int slots, cudaStream_t st) {
+  if (njobs <= 0) return;
+  const int V = tile_sweep_velocities(s.Nc8, fp32);
+  if (fp32) {
+    if (V == 32) launch_one<float, 32>(s, job0, njobs, slots, st);
+    else if (V == 16) launch_one<float, 16>(s, job0, njobs, slots, st);
+    else launch_one<float, 8>(s, job0, njobs, slots, st);
+  } else {
+    if (V == 16) launch_one<double, 16>(s, job0, njobs, slots, st);
+    else launch_one<double, 8>(s, job0, njobs, slots, st);
+  }
+}
+
+}  // namespace piks

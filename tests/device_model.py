@@ -203,6 +203,65 @@ class DeviceModel:
             for m, o, val in new:   # a hyperplane's tasks are independent
                 self.h[m, o] = val
 
+    def sweep_tiles(self, solver):
+        """All eight octant sweeps from the library's tile jobs, diagonal by diagonal: every
+        job of a diagonal first copies its rows (as the CTAs do at their start), then sweeps
+        its local hyperplanes on the copies, then writes its own rows back."""
+        g = solver.geometry_array
+        rows, rbeg = g("tile_rows"), g("tile_row_begin")
+        tasks, tbeg = g("tile_tasks").reshape(-1, 4), g("tile_task_begin")
+        steps, dbeg = g("tile_steps"), g("tile_diag_begin")
+        nst = len(steps) // (len(rbeg) - 1) - 1
+        c15, c10 = 1.5 / self.ds, 1.0 / self.ds
+        P = {"x2": self.cx * (2.0 / self.ds), "x1": self.cx * c10, "xh": self.cx * (-0.5 / self.ds),
+             "y2": self.cy * (2.0 / self.ds), "y1": self.cy * c10, "yh": self.cy * (-0.5 / self.ds),
+             "z2": self.cz * (2.0 / self.ds), "z1": self.cz * c10, "zh": self.cz * (-0.5 / self.ds)}
+        dens = {}
+        for cls in range(8):
+            d = 0.5 * self.mu + self.cx * (c10 if cls & 1 else c15)
+            d = d + self.cy * (c10 if cls & 2 else c15)
+            dens[cls] = d + self.cz * (c10 if cls & 4 else c15)
+        for d in range(len(dbeg) - 1):
+            jobs = range(dbeg[d], dbeg[d + 1])
+            smem = {}
+            for j in jobs:
+                S = [np.zeros(self.Nc8)]
+                for r in rows[rbeg[j]:rbeg[j + 1]]:
+                    S.append(self._row(int(r)).copy())
+                smem[j] = S
+            for j in jobs:
+                S = smem[j]
+                o = int(rows[rbeg[j]]) & 7
+                T = tasks[tbeg[j]:tbeg[j + 1]]
+                st = steps[j * (nst + 1):(j + 1) * (nst + 1)]
+                for s_ in range(nst):
+                    for t in range(st[s_], st[s_ + 1]):
+                        rec = [int(v) & 0xFFFFFFFF for v in T[t]]
+                        m = rec[0] & ((1 << 27) - 1)
+                        fx, fy, fz = bool(rec[0] >> 27 & 1), bool(rec[0] >> 28 & 1), bool(rec[0] >> 29 & 1)
+                        sl = [rec[1] & 0xFFFF, rec[1] >> 16, rec[2] & 0xFFFF, rec[2] >> 16, rec[3] & 0xFFFF, rec[3] >> 16]
+                        ex = (-self.cx if SX[o] < 0 else self.cx) * self.mom[1, m]
+                        ey = (-self.cy if SY[o] < 0 else self.cy) * self.mom[2, m]
+                        ez = (-self.cz if SZ[o] < 0 else self.cz) * self.mom[3, m]
+                        feq = self.w * (self.mom[0, m] + ((ex + ey) + ez))
+                        num = self.mu * (feq - 0.5 * S[1 + t])
+                        num = num + (P["x1"] if fx else P["x2"]) * S[sl[0]]
+                        if not fx:
+                            num = num + P["xh"] * S[sl[1]]
+                        num = num + (P["y1"] if fy else P["y2"]) * S[sl[2]]
+                        if not fy:
+                            num = num + P["yh"] * S[sl[3]]
+                        num = num + (P["z1"] if fz else P["z2"]) * S[sl[4]]
+                        if not fz:
+                            num = num + P["zh"] * S[sl[5]]
+                        cls = (1 if fx else 0) | (2 if fy else 0) | (4 if fz else 0)
+                        S[1 + t] = num / dens[cls]
+            for j in jobs:
+                S = smem[j]
+                for q in range(tbeg[j + 1] - tbeg[j]):
+                    code = int(rows[rbeg[j] + q])
+                    self.h[code // 8, code % 8] = S[1 + q]
+
     # --- the rest of one iteration -------------------------------------------------------
     def _far(self, code, o, gbuf):
         if code >= 0:
@@ -252,12 +311,14 @@ class DeviceModel:
                     else:
                         self.fw[corner, dst_o - 1] = v
 
-    def iterate(self, n=1, schedule="tasks"):
+    def iterate(self, n=1, schedule="tasks", solver=None):
         for _ in range(n):
             it = self.iStep + 1
             cap, prev = it & 1, (it - 1) & 1
             if schedule == "tasks":
                 self.sweep_tasks()
+            elif schedule == "tiles":
+                self.sweep_tiles(solver)
             else:
                 for o in range(8):
                     self.sweep(o)

@@ -130,3 +130,20 @@ def test_fp32_footprint_is_smaller():
         inf = a.info()
         f_bytes = inf["nNodes"] * 8 * inf["Nc8"] * 8
         assert a.info()["device_bytes"] - b.info()["device_bytes"] >= f_bytes // 2
+
+
+def test_fp32_tile_and_hyperplane_schedules_agree():
+    img = images.sphere_pack(16, 0.5, 1.5, 3.5, seed=1)
+    p = base_params(16, Nc_fundamental=4, Kn=0.5, fluidlayer=2)
+    out = []
+    for tiles in ((8, 8, 8), (0, 0, 0)):
+        with pk.Solver(p, device=0) as s:
+            s.set_tiles(*tiles)
+            s.set_precision(pk.PREC_FP32)
+            s.setup_physical_grid(img)
+            s.iterate(20)
+            out.append((s.get_f()[0], s.chk_converge()[0]))
+    (fa, ma), (fb, mb) = out
+    err = np.abs(fa - fb).max() / np.abs(fb).max()
+    print("fp32 tiles vs hyperplanes after 20 iterations: max rel diff %.3e, mass rel diff %.3e" % (err, _rel(ma, mb)))
+    assert err <= 1e-5 and _rel(ma, mb) <= 1e-5

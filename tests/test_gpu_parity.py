@@ -43,14 +43,20 @@ CASES = [
 ]
 
 
+SCHEDULES = {"tiles8": (8, 8, 8), "tiles435": (4, 3, 5), "hyperplanes": (0, 0, 0)}
+
+
+@pytest.mark.parametrize("schedule", list(SCHEDULES))
 @pytest.mark.parametrize("name,make,kw", CASES, ids=[c[0] for c in CASES])
-def test_iterations_bit_exact(name, make, kw):
+def test_iterations_bit_exact(name, make, kw, schedule):
     img = make()
     nz, ny, nx = img.shape
     p = base_params(nx, Ny=ny, Nz=nz, **{k: v for k, v in kw.items() if k not in ("Nx", "Ny", "Nz")})
     o = Oracle(p, img.tobytes(), nthreads=4)
     s = pk.Solver(p, device=0)
+    s.set_tiles(*SCHEDULES[schedule])
     s.setup_physical_grid(img)
+    assert s.schedule()["tiles"] == (SCHEDULES[schedule][0] > 0)
     assert np.array_equal(o.labels(), s.get_labels())
     nodes = s.geometry_array("node_g")
     for it in range(5):

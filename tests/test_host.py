@@ -143,3 +143,48 @@ def test_device_model_bit_exact(n, por, seed, kw):
         fm = m.f_reference_layout().reshape(8, m.Nc8, -1)[:, :, nodes]
         assert np.array_equal(fo, fm)
         assert o.chk_converge()[0] == m.mass_flux()
+
+
+@pytest.mark.parametrize("n,por,seed,tiles,kw", [
+    (12, 0.5, 11, (8, 8, 8), dict(Kn=0.7)),
+    (13, 0.45, 21, (4, 3, 5), dict(wallExtOrder=1)),
+    (11, 0.45, 13, (2, 2, 2), dict(wallExtOrder=3, fluidlayer=1)),
+    (9, 0.6, 14, (5, 4, 3), dict(Nc_fundamental=4, Kn=0.3, pressDrop=0.1)),
+])
+def test_tile_schedule_bit_exact(n, por, seed, tiles, kw):
+    """The tile-wavefront schedule (rows copied per job at the start of its diagonal, local
+    hyperplanes on the copies) gives the oracle's values bit for bit."""
+    img = images.sphere_pack(n, por, 1.2, 3.0, seed=seed)
+    p = base_params(n, **kw)
+    o = Oracle(p, img.tobytes(), nthreads=1)
+    s = pk.Solver(p, device=-1)
+    s.set_tiles(*tiles)
+    s.setup_physical_grid(img)
+    sch = s.schedule()
+    assert sch["tiles"] and (sch["TX"], sch["TY"], sch["TZ"]) == tiles
+    m = DeviceModel(s, p)
+    nodes = m.node_g
+    for _ in range(2):
+        o.iterate(1)
+        m.iterate(1, schedule="tiles", solver=s)
+        fo = o.f().reshape(8, m.Nc8, -1)[:, :, nodes]
+        fm = m.f_reference_layout().reshape(8, m.Nc8, -1)[:, :, nodes]
+        assert np.array_equal(fo, fm)
+        assert o.chk_converge()[0] == m.mass_flux()
+
+
+def test_tile_jobs_cover_every_task_once():
+    img = images.sphere_pack(16, 0.45, 1.5, 3.5, seed=3)
+    p = base_params(16)
+    s = pk.Solver(p, device=-1)
+    s.setup_physical_grid(img)
+    t = s.geometry_array("tasks").reshape(-1, 8)
+    tt = s.geometry_array("tile_tasks").reshape(-1, 4)
+    rows, rbeg, tbeg = s.geometry_array("tile_rows"), s.geometry_array("tile_row_begin"), s.geometry_array("tile_task_begin")
+    own = []
+    for j in range(len(tbeg) - 1):
+        own.extend(rows[rbeg[j]:rbeg[j] + (tbeg[j + 1] - tbeg[j])])
+    assert sorted(own) == sorted((t[:, 0] * 8 + (t[:, 1] & 7)).tolist())
+    assert len(tt) == len(t)
+    rows_per_job = np.diff(rbeg) + 1
+    assert s.schedule()["max_slots"] == rows_per_job.max()
