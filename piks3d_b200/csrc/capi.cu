@@ -48,7 +48,7 @@ struct piks_ctx {
   std::vector<std::pair<void *, size_t>> allocations;  // device buffers and their bytes
   size_t dev_bytes = 0;
   int prec = PIKS_PREC_FP64;        // storage / sweep precision of the state
-  int tile_dims[3] = {8, 8, 8};     // tile shape of the sweep schedule (0: per-node hyperplanes)
+  int tile_dims[3] = {8, 4, 4};     // tile shape of the sweep schedule (0: per-node hyperplanes)
   TileJobs tiles;
   bool use_tiles = false;           // tile schedule built and uploaded
   int iStep = 0;
@@ -204,9 +204,8 @@ void enqueue_iteration(piks_ctx *c) {
   {
     Timed t(c, KT_SWEEP);
     if (c->use_tiles) {
-      const auto &db = c->tiles.diag_begin;
-      for (size_t d = 0; d + 1 < db.size(); ++d)
-        launch_tile_sweep(s, f32, db[d], db[d + 1] - db[d], c->tiles.diag_rows[d], st);
+      const auto &L = c->tiles.launches;
+      for (size_t k = 0; k + 3 < L.size(); k += 4) launch_tile_sweep(s, f32, L[k], L[k + 1], L[k + 2], L[k + 3], st);
     } else {
       const auto &hs = c->geo.hyper_start;
       for (size_t h = 0; h + 1 < hs.size(); ++h) {
@@ -310,7 +309,10 @@ piks_status piks_setup_physical_grid(piks_ctx *c, const uint8_t *raw, int64_t nb
   c->use_tiles = false;
   c->tiles = TileJobs{};
   if (c->tile_dims[0] > 0) {
-    const int slots = std::min(tile_sweep_max_slots(c->vel.Nc8, false), tile_sweep_max_slots(c->vel.Nc8, true));
+    const int vox = c->tile_dims[0] * c->tile_dims[1] * c->tile_dims[2];
+    const int nst = c->tile_dims[0] + c->tile_dims[1] + c->tile_dims[2] - 2;
+    const int slots = std::min(tile_sweep_max_slots(c->vel.Nc8, false, vox, nst),
+                               tile_sweep_max_slots(c->vel.Nc8, true, vox, nst));
     c->use_tiles = build_tile_jobs(c->geo, c->tile_dims[0], c->tile_dims[1], c->tile_dims[2], slots, c->tiles);
     if (!c->use_tiles) c->tiles = TileJobs{};
   }
@@ -390,12 +392,15 @@ piks_status piks_setup_physical_grid(piks_ctx *c, const uint8_t *raw, int64_t nb
     int64_t *p64 = nullptr;
     UP(tj.rows, tv.rows, pi);
     UP(tj.row_begin, tv.row_begin, p64);
+    UP(tj.row_count, tv.row_count, pi);
     if ((st = upload(c, tj.tasks, &pi))) return st;
     s.tv.tasks = reinterpret_cast<const int4 *>(pi);
     UP(tj.task_begin, tv.task_begin, p64);
     uint16_t *p16 = nullptr;
     UP(tj.steps, tv.steps, p16);
+    UP(tj.job_list, tv.job_list, pi);
     s.tv.nsteps = tj.nsteps;
+    s.tv.steps_stride = tj.steps_stride;
   }
 #undef UP
   s.nWall = g.nWall;
@@ -744,9 +749,10 @@ piks_status piks_geometry_array(piks_ctx *c, const char *name, void *out, int64_
   ARR("plane_xN", g.plane_xN) ARR("sym_node", g.sym_node) ARR("sym_flag", g.sym_flag)
   ARR("flux_list", g.flux_list) ARR("tasks", g.tasks) ARR("hyper_start", g.hyper_start) ARR("cx", c->vel.cx) ARR("cy", c->vel.cy) ARR("cz", c->vel.cz) ARR("w", c->vel.w)
   const TileJobs &tj = c->tiles;
-  ARR("tile_rows", tj.rows) ARR("tile_row_begin", tj.row_begin) ARR("tile_tasks", tj.tasks)
+  ARR("tile_rows", tj.rows) ARR("tile_row_begin", tj.row_begin) ARR("tile_row_count", tj.row_count)
+  ARR("tile_tasks", tj.tasks)
   ARR("tile_task_begin", tj.task_begin) ARR("tile_steps", tj.steps) ARR("tile_diag_begin", tj.diag_begin)
-  ARR("tile_diag_rows", tj.diag_rows)
+  ARR("tile_diag_rows", tj.diag_rows) ARR("tile_job_list", tj.job_list) ARR("tile_launches", tj.launches)
 #undef ARR
   if (nm == "flux_groups") { src = g.flux_groups; n = 10; esz = sizeof(int32_t); }
   if (!esz) return fail(PIKS_ERR_ARG, "unknown geometry array " + nm);
@@ -808,8 +814,7 @@ piks_status piks_launches_per_iteration(piks_ctx *c, int64_t *n) {
   const DevState &s = c->ds;
   int64_t k = 0;
   if (c->use_tiles) {
-    const auto &db = c->tiles.diag_begin;
-    for (size_t d = 0; d + 1 < db.size(); ++d) k += db[d + 1] > db[d];
+    k += (int64_t)(c->tiles.launches.size() / 4);
   } else {
     for (size_t h = 0; h + 1 < c->geo.hyper_start.size(); ++h) k += c->geo.hyper_start[h + 1] > c->geo.hyper_start[h];
   }

@@ -8,11 +8,13 @@ namespace piks {
 // Device copy of the tile-wavefront schedule (TileJobs in piks_internal.h).
 struct TileView {
   const int32_t *rows;          // global row codes of every job's shared-memory slots 1..
-  const int64_t *row_begin;     // [njobs + 1]
+  const int64_t *row_begin;     // [njobs + 1], multiples of 4
+  const int32_t *row_count;     // [njobs]
   const int4 *tasks;            // node | fx<<27 | fy<<28 | fz<<29, slots x1|x2<<16, y1|y2<<16, z1|z2<<16
   const int64_t *task_begin;    // [njobs + 1]
-  const uint16_t *steps;        // [njobs][nsteps + 1] task offsets of the local hyperplanes
-  int nsteps;
+  const uint16_t *steps;        // [njobs][steps_stride] task offsets of the local hyperplanes
+  const int32_t *job_list;      // job indices in launch order
+  int nsteps, steps_stride;
 };
 
 // Everything the kernels read, as device pointers (one struct passed by value).
@@ -80,11 +82,11 @@ void launch_walls32(const DevState &s, int begin, int end, int gbuf, cudaStream_
 void launch_inlet_outlet32(const DevState &s, int buf, cudaStream_t st);
 void launch_symmetry32(const DevState &s, cudaStream_t st);
 void launch_moments32(const DevState &s, cudaStream_t st);
-// Tile-wavefront sweep: the jobs [job0, job0 + njobs) of one diagonal, `slots` shared-memory
-// rows per CTA. tile_sweep_velocities() is the chunk width V used for the precision.
+// Tile-wavefront sweep: the jobs job_list[first .. first + njobs) (all of one diagonal),
+// `slots` shared-memory rows and room for `tasks` task records per CTA. tile_sweep_velocities() is the chunk width V used for the precision.
 int tile_sweep_velocities(int Nc8, bool fp32);
-int tile_sweep_max_slots(int Nc8, bool fp32);
-void launch_tile_sweep(const DevState &s, bool fp32, int job0, int njobs, int slots, cudaStream_t st);
+int tile_sweep_max_slots(int Nc8, bool fp32, int tile_voxels, int nsteps);
+void launch_tile_sweep(const DevState &s, bool fp32, int job0, int njobs, int slots, int tasks, cudaStream_t st);
 void launch_widen(const float *src, double *dst, size_t n, cudaStream_t st);
 void launch_narrow(const double *src, float *dst, size_t n, cudaStream_t st);
 void launch_division_selftest(int64_t samples, uint64_t seed, unsigned long long *mismatches);

@@ -103,21 +103,33 @@ struct TileJobs {
   // rows of each job (global row codes as in Geometry::tasks): the job's own rows first,
   // in task order, then the other rows it reads; shared-memory slot = 1 + position
   // (slot 0 is a row of zeros)
+  // (each job's list starts at a multiple of 4 entries, for 16-byte copies)
   std::vector<int32_t> rows;
   std::vector<int64_t> row_begin;    // njobs + 1
+  std::vector<int32_t> row_count;    // njobs
   // per task: node | fx<<27 | fy<<28 | fz<<29, then the slots of x1 | x2<<16, y1 | y2<<16,
   // z1 | z2<<16; the task's own slot is 1 + its index within the job
   std::vector<int32_t> tasks;        // 4 int32 per task
   std::vector<int64_t> task_begin;   // njobs + 1
-  std::vector<uint16_t> steps;       // [njobs][nsteps + 1] task offsets within the job
+  std::vector<uint16_t> steps;       // [njobs][steps_stride] task offsets within the job
+  int steps_stride = 0;              // nsteps + 1 rounded up to a multiple of 8
   std::vector<int32_t> diag_begin;   // job offset of each diagonal (+1 end entry)
   std::vector<int32_t> diag_rows;    // largest slot count (rows + zero row) per diagonal
+  std::vector<int32_t> diag_tasks;   // largest task count of a job per diagonal
+  // launch plan: the jobs of each diagonal sorted by slot count and cut into size classes,
+  // one launch per class, each sized for its largest job
+  std::vector<int32_t> job_list;     // job indices in launch order
+  std::vector<int32_t> launches;     // per launch: first job_list entry, job count, slots, tasks
+  std::vector<int32_t> launch_diag_end;  // launch offset after each diagonal
   int32_t max_rows = 0;
 };
 
 // Builds the tile jobs from g.tasks; returns false when a job needs more than max_slots
 // shared-memory rows (the caller then keeps the hyperplane schedule).
 bool build_tile_jobs(const Geometry &g, int TX, int TY, int TZ, int max_slots, TileJobs &tj);
+// (Re)builds the launch plan with at most max_classes size classes per diagonal; a class
+// holds the jobs whose slot count is above `ratio` times its largest.
+void plan_tile_launches(TileJobs &tj, int max_classes, double ratio);
 
 piks_status make_setup(const piks_params &p, Setup &s, std::string &err);
 piks_status make_velocity(const piks_params &p, Velocity &v, std::string &err);

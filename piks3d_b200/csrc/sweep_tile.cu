@@ -4,10 +4,13 @@
 //  1. it copies every row the job touches (its own rows, the upwind rows of neighbouring
 //     tiles, the wall rows seen by its readers) into shared memory with cp.async, V
 //     velocities (one 128-byte segment for V*sizeof(T) = 128) per row;
-//  2. it sweeps the tile's local hyperplanes in order, a group of V/2 lanes per task with
-//     two velocities per lane, reading every upwind value from shared memory and writing
-//     the new value to the task's own slot (one barrier per non-empty hyperplane);
-//  3. it writes the own rows back.
+//  2. it replaces each own row by the part of its update that depends only on the previous
+//     iteration (mu * (fEq - f_old / 2)), for all tasks at once;
+//  3. it sweeps the tile's local hyperplanes in order, a group of V/2 lanes per task with
+//     two velocities per lane, adding the upwind terms read from shared memory in the
+//     reference's order and writing the new value to the task's own slot (one barrier per
+//     non-empty hyperplane);
+//  4. it writes the own rows back.
 // Jobs of one diagonal run in one launch; rows a job reads from another tile were written
 // by an earlier launch. Each update applies the same operations to the same operands as
 // the per-node FP64 kernel, so the FP64 result is unchanged by the schedule.
@@ -49,9 +52,16 @@ template <typename T> __device__ __forceinline__ const T *state_fw(const DevStat
 template <> __device__ __forceinline__ const double *state_fw<double>(const DevState &a) { return a.fw; }
 template <> __device__ __forceinline__ const float *state_fw<float>(const DevState &a) { return a.fw32; }
 
+// Shared-memory layout of one CTA: [slots][V] rows, the job's task records (int4), the
+// moments of each task's node (two double2), the row codes (int32) and the step offsets.
+__host__ __device__ inline size_t tile_smem_bytes(int slots, int ntask, int steps_stride, int row_bytes) {
+  return (size_t)slots * row_bytes + (size_t)ntask * 48 + ((size_t)slots * 4 + 15) / 16 * 16 +
+         (size_t)steps_stride * 2;
+}
+
 template <typename T, int V>
 __global__ void __launch_bounds__(V / 2 * kGroups)
-k_tile_sweep(const DevState a, int job0) {
+k_tile_sweep(const DevState a, int job0, int slots_cap, int tasks_cap) {
   constexpr int LPT = V / 2;                        // lanes per task
   constexpr int THREADS = LPT * kGroups;
   constexpr int EPP = 16 / (int)sizeof(T);          // elements per 16-byte piece
@@ -63,29 +73,46 @@ k_tile_sweep(const DevState a, int job0) {
   const TileView &tv = a.tv;
   const int Nc8 = a.Nc8;
   const int nchunk = Nc8 / V;
-  const int job = job0 + (int)(blockIdx.x / nchunk);
+  const int job = tv.job_list[job0 + (int)(blockIdx.x / nchunk)];
   const int chunk = (int)(blockIdx.x % nchunk);
   const int l0 = chunk * V;
   const int64_t rb = tv.row_begin[job];
-  const int nrows = (int)(tv.row_begin[job + 1] - rb);
+  const int nrows = tv.row_count[job];
   const int64_t tb = tv.task_begin[job];
   const int ntask = (int)(tv.task_begin[job + 1] - tb);
+  const int nsteps = tv.nsteps;
+  int4 *Trec = reinterpret_cast<int4 *>(smem_raw + (size_t)slots_cap * V * sizeof(T));
+  double2 *Mom = reinterpret_cast<double2 *>(Trec + tasks_cap);
+  int *Codes = reinterpret_cast<int *>(Mom + 2 * (size_t)tasks_cap);
+  uint16_t *Steps = reinterpret_cast<uint16_t *>(Codes + ((size_t)slots_cap + 3) / 4 * 4);
   const T *h = state_h<T>(a);
   const T *fw = state_fw<T>(a);
 
-  // 1. rows -> shared memory (slot 0 = zeros)
+  // 1a. row codes, task records and step offsets -> shared memory
+  for (int i = threadIdx.x; i < (nrows + 3) / 4; i += THREADS)
+    cp_async16(Codes + 4 * i, tv.rows + rb + 4 * i);
+  for (int i = threadIdx.x; i < ntask; i += THREADS) cp_async16(Trec + i, tv.tasks + tb + i);
+  for (int i = threadIdx.x; i < tv.steps_stride / 8; i += THREADS)
+    cp_async16(Steps + 8 * i, tv.steps + (size_t)job * tv.steps_stride + 8 * i);
+  cp_async_wait_all();
+  __syncthreads();
+  // 1b. rows (slot 0 = zeros) and the moments of the tasks' nodes (FP64 Rho, Ux | Uy, Uz)
   for (int i = threadIdx.x; i < nrows * PIECES; i += THREADS) {
     const int r = i / PIECES, pc = i - r * PIECES;
-    const int code = __ldg(tv.rows + rb + r);
+    const int code = Codes[r];
     const T *src = ((code & kFwBit) ? fw : h) + (size_t)(code & ~kFwBit) * (size_t)Nc8 + l0 + pc * EPP;
     cp_async16(S + (size_t)(1 + r) * V + pc * EPP, src);
+  }
+  for (int i = threadIdx.x; i < 2 * ntask; i += THREADS) {
+    const int m = Trec[i >> 1].x & ((1 << 27) - 1);
+    cp_async16(Mom + i, reinterpret_cast<const double2 *>(a.mom) + 2 * (size_t)m + (i & 1));
   }
   if (threadIdx.x < PIECES) *reinterpret_cast<int4 *>(S + threadIdx.x * EPP) = make_int4(0, 0, 0, 0);
 
   // per-lane constants of its two velocities
   const int grp = threadIdx.x / LPT, sub = threadIdx.x % LPT;
   const int lp = l0 + 2 * sub;
-  const int o = __ldg(tv.rows + rb) & 7;            // own row code = node * 8 + octant
+  const int o = Codes[0] & 7;                       // own row code = node * 8 + octant
   const bool nx_ = !(o == 0 || o == 3 || o == 4 || o == 7);
   const bool ny_ = !(o == 0 || o == 1 || o == 4 || o == 5);
   const bool nz_ = o >= 4;
@@ -101,42 +128,69 @@ k_tile_sweep(const DevState a, int job0) {
       K[k][1] = __ldg(a.vtab32 + (size_t)(lp + 1) * kVtab + k);
     }
   }
+
   cp_async_wait_all();
   __syncthreads();
 
-  // 2. local hyperplanes
-  const uint16_t *st = tv.steps + (size_t)job * (tv.nsteps + 1);
-  for (int s = 0; s < tv.nsteps; ++s) {
-    const int t0 = st[s], t1 = st[s + 1];
+  // 2. the part of every update that does not depend on this sweep's values,
+  //    mu * (fEq - f_old / 2) (solver.F90:205-214), replaces f_old in the task's own slot
+  for (int t = grp; t < ntask; t += kGroups) {
+    const double2 m01 = Mom[2 * t], m23 = Mom[2 * t + 1];
+    T2 *own = reinterpret_cast<T2 *>(S + (size_t)(1 + t) * V + 2 * sub);
+    const T2 fold = *own;
+    const T fo[2] = {fold.x, fold.y};
+    T base[2];
+    if constexpr (sizeof(T) == 8) {
+      const double rho = m01.x, ux = m01.y, uy = m23.x, uz = m23.y;
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const double cx = K[0][q], cy = K[1][q], cz = K[2][q], wl = K[3][q];
+        const double ex = dmul(nx_ ? -cx : cx, ux), ey = dmul(ny_ ? -cy : cy, uy), ez = dmul(nz_ ? -cz : cz, uz);
+        const double feq = dmul(wl, dadd(rho, dadd(dadd(ex, ey), ez)));
+        base[q] = dmul(a.mu, dsub(feq, dmul(0.5, fo[q])));
+      }
+    } else {
+      const float rho = (float)m01.x, ux = (float)m01.y, uy = (float)m23.x, uz = (float)m23.y;
+      const float mu = (float)a.mu;
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const float cx = K[0][q], cy = K[1][q], cz = K[2][q], wl = K[3][q];
+        const float feq = wl * (rho + ((nx_ ? -cx : cx) * ux + (ny_ ? -cy : cy) * uy + (nz_ ? -cz : cz) * uz));
+        base[q] = mu * (feq - 0.5f * fo[q]);
+      }
+    }
+    T2 bv;
+    bv.x = base[0];
+    bv.y = base[1];
+    *own = bv;
+  }
+  __syncthreads();
+
+  // 3. local hyperplanes: the upwind terms in the reference's order, then the division
+  for (int s = 0; s < nsteps; ++s) {
+    const int t0 = Steps[s], t1 = Steps[s + 1];
     if (t0 == t1) continue;
     for (int t = t0 + grp; t < t1; t += kGroups) {
-      const int4 rec = __ldg(tv.tasks + tb + t);
-      const int m = rec.x & ((1 << 27) - 1);
+      const int4 rec = Trec[t];
       const bool fx = (rec.x >> 27) & 1, fy = (rec.x >> 28) & 1, fz = (rec.x >> 29) & 1;
       const int cls = (fx ? 1 : 0) | (fy ? 2 : 0) | (fz ? 4 : 0);
       auto ld = [&](int slot) { return *reinterpret_cast<const T2 *>(S + (size_t)slot * V + 2 * sub); };
-      const T2 fold = ld(1 + t);
+      const T2 b2 = ld(1 + t);
       const T2 x1 = ld(rec.y & 0xffff), y1 = ld(rec.z & 0xffff), z1 = ld(rec.w & 0xffff);
       T2 x2{}, y2{}, z2{};
       if (!fx) x2 = ld((unsigned)rec.y >> 16);
       if (!fy) y2 = ld((unsigned)rec.z >> 16);
       if (!fz) z2 = ld((unsigned)rec.w >> 16);
-      const double2 m01 = __ldg(reinterpret_cast<const double2 *>(a.mom) + 2 * (size_t)m);
-      const double2 m23 = __ldg(reinterpret_cast<const double2 *>(a.mom) + 2 * (size_t)m + 1);
-      const T fo[2] = {fold.x, fold.y}, vx1[2] = {x1.x, x1.y}, vx2[2] = {x2.x, x2.y}, vy1[2] = {y1.x, y1.y},
+      const T bs[2] = {b2.x, b2.y}, vx1[2] = {x1.x, x1.y}, vx2[2] = {x2.x, x2.y}, vy1[2] = {y1.x, y1.y},
               vy2[2] = {y2.x, y2.y}, vz1[2] = {z1.x, z1.y}, vz2[2] = {z2.x, z2.y};
       T out[2];
       if constexpr (sizeof(T) == 8) {
-        const double rho = m01.x, ux = m01.y, uy = m23.x, uz = m23.y;
         const double2 dn = __ldg(a.vtab2 + (size_t)(lp >> 1) * kVtab + 13 + cls);
         const double2 rc = __ldg(a.vtab2 + (size_t)(lp >> 1) * kVtab + 21 + cls);
         const double den[2] = {dn.x, dn.y}, rcp[2] = {rc.x, rc.y};
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
-          const double cx = K[0][q], cy = K[1][q], cz = K[2][q], wl = K[3][q];
-          const double ex = dmul(nx_ ? -cx : cx, ux), ey = dmul(ny_ ? -cy : cy, uy), ez = dmul(nz_ ? -cz : cz, uz);
-          const double feq = dmul(wl, dadd(rho, dadd(dadd(ex, ey), ez)));
-          double num = dmul(a.mu, dsub(feq, dmul(0.5, fo[q])));
+          double num = bs[q];
           num = dadd(num, dmul(fx ? K[5][q] : K[4][q], vx1[q]));
           if (!fx) num = dadd(num, dmul(K[6][q], vx2[q]));
           num = dadd(num, dmul(fy ? K[8][q] : K[7][q], vy1[q]));
@@ -146,14 +200,10 @@ k_tile_sweep(const DevState a, int job0) {
           out[q] = markstein_div(num, den[q], rcp[q]);
         }
       } else {
-        const float rho = (float)m01.x, ux = (float)m01.y, uy = (float)m23.x, uz = (float)m23.y;
-        const float mu = (float)a.mu;
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
-          const float cx = K[0][q], cy = K[1][q], cz = K[2][q], wl = K[3][q];
           const float rcp = __ldg(a.vtab32 + (size_t)(lp + q) * kVtab + 21 + cls);
-          const float feq = wl * (rho + ((nx_ ? -cx : cx) * ux + (ny_ ? -cy : cy) * uy + (nz_ ? -cz : cz) * uz));
-          float num = mu * (feq - 0.5f * fo[q]);
+          float num = bs[q];
           num += (fx ? K[5][q] : K[4][q]) * vx1[q];
           if (!fx) num += K[6][q] * vx2[q];
           num += (fy ? K[8][q] : K[7][q]) * vy1[q];
@@ -171,18 +221,18 @@ k_tile_sweep(const DevState a, int job0) {
     __syncthreads();
   }
 
-  // 3. own rows -> global
+  // 4. own rows -> global
   T *hw = const_cast<T *>(h);
   for (int i = threadIdx.x; i < ntask * PIECES; i += THREADS) {
     const int r = i / PIECES, pc = i - r * PIECES;
-    const int code = __ldg(tv.rows + rb + r);
+    const int code = Codes[r];
     *reinterpret_cast<int4 *>(hw + (size_t)code * Nc8 + l0 + pc * EPP) =
         *reinterpret_cast<const int4 *>(S + (size_t)(1 + r) * V + pc * EPP);
   }
 }
 
 template <typename T, int V>
-void launch_one(const DevState &s, int job0, int njobs, int slots, cudaStream_t st) {
+void launch_one(const DevState &s, int job0, int njobs, int slots, int tasks, cudaStream_t st) {
   static unsigned long long configured = 0;  // one bit per device
   int dev = 0;
   cudaGetDevice(&dev);
@@ -190,9 +240,9 @@ void launch_one(const DevState &s, int job0, int njobs, int slots, cudaStream_t 
     cudaFuncSetAttribute(k_tile_sweep<T, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
     configured |= 1ull << (dev & 63);
   }
-  const size_t smem = (size_t)slots * V * sizeof(T);
+  const size_t smem = tile_smem_bytes(slots, tasks, s.tv.steps_stride, V * (int)sizeof(T));
   const unsigned grid = (unsigned)((size_t)njobs * (s.Nc8 / V));
-  k_tile_sweep<T, V><<<grid, V / 2 * kGroups, smem, st>>>(s, job0);
+  k_tile_sweep<T, V><<<grid, V / 2 * kGroups, smem, st>>>(s, job0, slots, tasks);
 }
 
 }  // namespace
@@ -202,21 +252,23 @@ int tile_sweep_velocities(int Nc8, bool fp32) {
   return Nc8 % 16 == 0 ? 16 : 8;
 }
 
-int tile_sweep_max_slots(int Nc8, bool fp32) {
+int tile_sweep_max_slots(int Nc8, bool fp32, int tile_voxels, int nsteps) {
   const int row = tile_sweep_velocities(Nc8, fp32) * (fp32 ? 4 : 8);
-  return (227 * 1024) / row;
+  const size_t fixed = tile_smem_bytes(0, tile_voxels, (nsteps + 1 + 7) / 8 * 8, row) + 16;
+  const size_t cap = 227 * 1024;
+  return fixed >= cap ? 0 : (int)((cap - fixed) / (row + 4));
 }
 
-void launch_tile_sweep(const DevState &s, bool fp32, int job0, int njobs, int slots, cudaStream_t st) {
+void launch_tile_sweep(const DevState &s, bool fp32, int job0, int njobs, int slots, int tasks, cudaStream_t st) {
   if (njobs <= 0) return;
   const int V = tile_sweep_velocities(s.Nc8, fp32);
   if (fp32) {
-    if (V == 32) launch_one<float, 32>(s, job0, njobs, slots, st);
-    else if (V == 16) launch_one<float, 16>(s, job0, njobs, slots, st);
-    else launch_one<float, 8>(s, job0, njobs, slots, st);
+    if (V == 32) launch_one<float, 32>(s, job0, njobs, slots, tasks, st);
+    else if (V == 16) launch_one<float, 16>(s, job0, njobs, slots, tasks, st);
+    else launch_one<float, 8>(s, job0, njobs, slots, tasks, st);
   } else {
-    if (V == 16) launch_one<double, 16>(s, job0, njobs, slots, st);
-    else launch_one<double, 8>(s, job0, njobs, slots, st);
+    if (V == 16) launch_one<double, 16>(s, job0, njobs, slots, tasks, st);
+    else launch_one<double, 8>(s, job0, njobs, slots, tasks, st);
   }
 }
 

@@ -10,6 +10,7 @@ bool build_tile_jobs(const Geometry &g, int TX, int TY, int TZ, int max_slots, T
   tj = TileJobs{};
   tj.TX = TX; tj.TY = TY; tj.TZ = TZ;
   tj.nsteps = TX + TY + TZ - 2;
+  tj.steps_stride = (tj.nsteps + 1 + 7) / 8 * 8;
   if (max_slots > 65535) max_slots = 65535;  // slots are stored in 16 bits
   const int Nx = g.Nx, Ny = g.Ny, Nz = g.Nz;
   const int nTx = (Nx + TX - 1) / TX, nTy = (Ny + TY - 1) / TY, nTz = (Nz + TZ - 1) / TZ;
@@ -64,6 +65,7 @@ bool build_tile_jobs(const Geometry &g, int TX, int TY, int TZ, int max_slots, T
   tj.rows.reserve(ntask * 2);
   tj.diag_begin.assign((size_t)ndiag + 1, 0);
   tj.diag_rows.assign((size_t)ndiag, 0);
+  tj.diag_tasks.assign((size_t)ndiag, 0);
   int32_t njobs = 0;
   size_t q = 0;
   while (q < ntask) {
@@ -102,11 +104,14 @@ bool build_tile_jobs(const Geometry &g, int TX, int TY, int TZ, int max_slots, T
     }
     const int32_t nslots = (int32_t)(1 + ((int64_t)tj.rows.size() - rb));
     if (nslots > max_slots) return false;
+    tj.row_count.push_back(nslots - 1);
+    while (tj.rows.size() % 4) tj.rows.push_back(0);
     tj.diag_rows[(size_t)diag] = std::max(tj.diag_rows[(size_t)diag], nslots);
+    tj.diag_tasks[(size_t)diag] = std::max(tj.diag_tasks[(size_t)diag], (int32_t)(e - q));
     tj.max_rows = std::max(tj.max_rows, nslots);
     // step offsets
     const size_t sb = tj.steps.size();
-    tj.steps.resize(sb + (size_t)tj.nsteps + 1, 0);
+    tj.steps.resize(sb + (size_t)tj.steps_stride, 0);
     for (size_t p = q; p < e; ++p) tj.steps[sb + step[order[p]] + 1]++;
     for (int s = 0; s < tj.nsteps; ++s) tj.steps[sb + s + 1] = (uint16_t)(tj.steps[sb + s + 1] + tj.steps[sb + s]);
     tj.diag_begin[(size_t)diag + 1] = njobs + 1;
@@ -116,7 +121,41 @@ bool build_tile_jobs(const Geometry &g, int TX, int TY, int TZ, int max_slots, T
   tj.row_begin.push_back((int64_t)tj.rows.size());
   tj.task_begin.push_back((int64_t)(tj.tasks.size() / 4));
   for (int d = 0; d < ndiag; ++d) tj.diag_begin[(size_t)d + 1] = std::max(tj.diag_begin[(size_t)d + 1], tj.diag_begin[(size_t)d]);
+  plan_tile_launches(tj, 1, 0.0);
   return true;
+}
+
+void plan_tile_launches(TileJobs &tj, int max_classes, double ratio) {
+  tj.job_list.clear();
+  tj.launches.clear();
+  tj.launch_diag_end.clear();
+  const size_t ndiag = tj.diag_begin.empty() ? 0 : tj.diag_begin.size() - 1;
+  std::vector<int32_t> jobs;
+  for (size_t d = 0; d < ndiag; ++d) {
+    jobs.clear();
+    for (int32_t j = tj.diag_begin[d]; j < tj.diag_begin[d + 1]; ++j) jobs.push_back(j);
+    std::stable_sort(jobs.begin(), jobs.end(),
+                     [&](int32_t a, int32_t b) { return tj.row_count[(size_t)a] > tj.row_count[(size_t)b]; });
+    size_t q = 0;
+    int classes = 0;
+    while (q < jobs.size()) {
+      const int32_t top = tj.row_count[(size_t)jobs[q]];
+      size_t e = q;
+      int32_t tmax = 0;
+      while (e < jobs.size() && (classes + 1 == max_classes || tj.row_count[(size_t)jobs[e]] > ratio * top)) {
+        tmax = std::max(tmax, (int32_t)(tj.task_begin[(size_t)jobs[e] + 1] - tj.task_begin[(size_t)jobs[e]]));
+        ++e;
+      }
+      tj.launches.push_back((int32_t)tj.job_list.size());
+      tj.launches.push_back((int32_t)(e - q));
+      tj.launches.push_back(top + 1);
+      tj.launches.push_back(tmax);
+      for (size_t k = q; k < e; ++k) tj.job_list.push_back(jobs[k]);
+      ++classes;
+      q = e;
+    }
+    tj.launch_diag_end.push_back((int32_t)(tj.launches.size() / 4));
+  }
 }
 
 }  // namespace piks

@@ -208,10 +208,11 @@ class DeviceModel:
         job of a diagonal first copies its rows (as the CTAs do at their start), then sweeps
         its local hyperplanes on the copies, then writes its own rows back."""
         g = solver.geometry_array
-        rows, rbeg = g("tile_rows"), g("tile_row_begin")
+        rows, rbeg, rcnt = g("tile_rows"), g("tile_row_begin"), g("tile_row_count")
         tasks, tbeg = g("tile_tasks").reshape(-1, 4), g("tile_task_begin")
         steps, dbeg = g("tile_steps"), g("tile_diag_begin")
-        nst = len(steps) // (len(rbeg) - 1) - 1
+        stride = len(steps) // (len(rbeg) - 1)
+        nst = int(solver.schedule()["TX"] + solver.schedule()["TY"] + solver.schedule()["TZ"] - 2)
         c15, c10 = 1.5 / self.ds, 1.0 / self.ds
         P = {"x2": self.cx * (2.0 / self.ds), "x1": self.cx * c10, "xh": self.cx * (-0.5 / self.ds),
              "y2": self.cy * (2.0 / self.ds), "y1": self.cy * c10, "yh": self.cy * (-0.5 / self.ds),
@@ -226,14 +227,15 @@ class DeviceModel:
             smem = {}
             for j in jobs:
                 S = [np.zeros(self.Nc8)]
-                for r in rows[rbeg[j]:rbeg[j + 1]]:
+                assert rbeg[j] % 4 == 0
+                for r in rows[rbeg[j]:rbeg[j] + rcnt[j]]:
                     S.append(self._row(int(r)).copy())
                 smem[j] = S
             for j in jobs:
                 S = smem[j]
                 o = int(rows[rbeg[j]]) & 7
                 T = tasks[tbeg[j]:tbeg[j + 1]]
-                st = steps[j * (nst + 1):(j + 1) * (nst + 1)]
+                st = steps[j * stride:(j + 1) * stride]
                 for s_ in range(nst):
                     for t in range(st[s_], st[s_ + 1]):
                         rec = [int(v) & 0xFFFFFFFF for v in T[t]]

@@ -186,5 +186,17 @@ def test_tile_jobs_cover_every_task_once():
         own.extend(rows[rbeg[j]:rbeg[j] + (tbeg[j + 1] - tbeg[j])])
     assert sorted(own) == sorted((t[:, 0] * 8 + (t[:, 1] & 7)).tolist())
     assert len(tt) == len(t)
-    rows_per_job = np.diff(rbeg) + 1
+    rows_per_job = s.geometry_array("tile_row_count") + 1
+    assert np.all(rbeg % 4 == 0) and np.all(np.diff(rbeg) >= rows_per_job - 1)
+    # launch plan: every job once, one diagonal per launch, launch sized for its jobs
+    jl = s.geometry_array("tile_job_list")
+    L = s.geometry_array("tile_launches").reshape(-1, 4)
+    dbeg = s.geometry_array("tile_diag_begin")
+    assert sorted(jl.tolist()) == list(range(len(rbeg) - 1))
+    ntask = np.diff(tbeg)
+    for first, count, slots, tmax in L:
+        jobs = jl[first:first + count]
+        diag = np.searchsorted(dbeg, jobs, side="right") - 1
+        assert count > 0 and np.all(diag == diag[0])
+        assert slots >= rows_per_job[jobs].max() and tmax >= ntask[jobs].max()
     assert s.schedule()["max_slots"] == rows_per_job.max()
