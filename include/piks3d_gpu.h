@@ -159,7 +159,15 @@ piks_status piks_get_precision(piks_ctx *ctx, int32_t *precision);
  * at the next piks_setup_physical_grid. No counterpart in the reference (its sweep is a
  * serial raster loop per octant). */
 piks_status piks_set_tiles(piks_ctx *ctx, int32_t tx, int32_t ty, int32_t tz);
-/* [tile schedule in use (0/1), TX, TY, TZ, largest shared-memory slot count of a job] */
+/* How the tile jobs are launched: PIKS_SCHED_TILE_DIAGONALS (default) launches each tile
+ * diagonal separately; PIKS_SCHED_TILE_DATAFLOW runs all jobs of an iteration in one
+ * launch, each job waiting for its upwind neighbour tiles through device flags (waits give
+ * up after about a second: piks_synchronize / piks_chk_converge then return
+ * PIKS_ERR_CUDA). */
+enum { PIKS_SCHED_TILE_DATAFLOW = 0, PIKS_SCHED_TILE_DIAGONALS = 1 };
+piks_status piks_set_schedule(piks_ctx *ctx, int32_t schedule);
+/* [tile schedule in use (0/1), TX, TY, TZ, largest shared-memory slot count of a job,
+ *  launch schedule, number of jobs] */
 piks_status piks_get_schedule(piks_ctx *ctx, int32_t *out, int32_t n);
 
 /* FP32 solve with FP64 refinement: runs FP32 iterations with chkConverge every

@@ -86,6 +86,7 @@ def load_library(path=LIB_PATH):
         "piks_set_precision": (i32, [c_void_p, i32]),
         "piks_set_tiles": (i32, [c_void_p, i32, i32, i32]),
         "piks_get_schedule": (i32, [c_void_p, P(i32), i32]),
+        "piks_set_schedule": (i32, [c_void_p, i32]),
         "piks_get_precision": (i32, [c_void_p, P(i32)]),
         "piks_run_refined": (i32, [c_void_p, ctypes.c_char_p, ctypes.c_char_p, i32, dbl, P(i32), P(i32), P(dbl),
                                    P(dbl)]),
@@ -130,6 +131,7 @@ def _dptr(a):
 
 
 PREC_FP64, PREC_FP32 = 0, 1
+SCHED_TILE_DATAFLOW, SCHED_TILE_DIAGONALS = 0, 1
 
 KERNEL_NAMES = ("sweep", "commit", "capture", "walls", "inlet_outlet", "symmetry", "moments", "flux")
 
@@ -207,11 +209,16 @@ class Solver:
         tz = tx if tz is None else tz
         _check(self.lib.piks_set_tiles(self._ctx, int(tx), int(ty), int(tz)))
 
+    def set_schedule(self, schedule):
+        """SCHED_TILE_DATAFLOW (one launch per sweep) or SCHED_TILE_DIAGONALS."""
+        _check(self.lib.piks_set_schedule(self._ctx, int(schedule)))
+
     def schedule(self):
-        """{'tiles': bool, 'TX', 'TY', 'TZ', 'max_slots'} of the sweep schedule in use."""
-        a = (ctypes.c_int32 * 5)()
-        _check(self.lib.piks_get_schedule(self._ctx, a, 5))
-        return {"tiles": bool(a[0]), "TX": a[1], "TY": a[2], "TZ": a[3], "max_slots": a[4]}
+        """{'tiles': bool, 'TX', 'TY', 'TZ', 'max_slots', 'launch', 'jobs'} of the sweep schedule."""
+        a = (ctypes.c_int32 * 7)()
+        _check(self.lib.piks_get_schedule(self._ctx, a, 7))
+        return {"tiles": bool(a[0]), "TX": a[1], "TY": a[2], "TZ": a[3], "max_slots": a[4], "launch": a[5],
+                "jobs": a[6]}
 
     @property
     def precision(self):

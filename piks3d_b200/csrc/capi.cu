@@ -51,6 +51,7 @@ struct piks_ctx {
   int tile_dims[3] = {8, 4, 4};     // tile shape of the sweep schedule (0: per-node hyperplanes)
   TileJobs tiles;
   bool use_tiles = false;           // tile schedule built and uploaded
+  int schedule = PIKS_SCHED_TILE_DIAGONALS;
   int iStep = 0;
   double mass = 1.0, error = 1.0, permeability = 0.0;
   bool timing = false;
@@ -194,6 +195,18 @@ void drain_timing(piks_ctx *c) {
   c->ev_next = 0;
 }
 
+// The dataflow sweep's error flag: set when a dependency wait gave up (the values of that
+// sweep are then not the solver's).
+piks_status check_sweep_error(piks_ctx *c) {
+  if (!c->use_tiles || !c->ds.tv.err) return PIKS_OK;
+  int e = 0;
+  piks_status st = cuda_check(cudaMemcpyAsync(&e, c->ds.tv.err, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "err D2H");
+  if (!st) st = cuda_check(cudaStreamSynchronize(c->stream), "err sync");
+  if (st) return st;
+  if (e) return fail(PIKS_ERR_CUDA, "tile sweep: a dependency wait timed out");
+  return PIKS_OK;
+}
+
 // One source iteration (solver.F90:111-1940) as a launch sequence on the context stream.
 void enqueue_iteration(piks_ctx *c) {
   DevState &s = c->ds;
@@ -203,7 +216,9 @@ void enqueue_iteration(piks_ctx *c) {
   const bool f32 = c->prec == PIKS_PREC_FP32;
   {
     Timed t(c, KT_SWEEP);
-    if (c->use_tiles) {
+    if (c->use_tiles && c->schedule == PIKS_SCHED_TILE_DATAFLOW) {
+      launch_tile_sweep_dataflow(s, f32, n, c->tiles.max_rows, c->tiles.max_tasks, st);
+    } else if (c->use_tiles) {
       const auto &L = c->tiles.launches;
       for (size_t k = 0; k + 3 < L.size(); k += 4) launch_tile_sweep(s, f32, L[k], L[k + 1], L[k + 2], L[k + 3], st);
     } else {
@@ -399,6 +414,14 @@ piks_status piks_setup_physical_grid(piks_ctx *c, const uint8_t *raw, int64_t nb
     uint16_t *p16 = nullptr;
     UP(tj.steps, tv.steps, p16);
     UP(tj.job_list, tv.job_list, pi);
+    UP(tj.up, tv.up, pi);
+    s.tv.njobs = (int)(tj.row_count.size());
+    int *pw = nullptr;
+    if ((st = zeros(c, (size_t)s.tv.njobs * (size_t)(v.Nc8 / 8 > 0 ? v.Nc8 / 8 : 1), &pw))) return st;
+    s.tv.flags = pw;
+    if ((st = zeros(c, (size_t)2, &pw))) return st;
+    s.tv.counter = pw;
+    s.tv.err = pw + 1;
     s.tv.nsteps = tj.nsteps;
     s.tv.steps_stride = tj.steps_stride;
   }
@@ -443,6 +466,7 @@ piks_status piks_chk_converge(piks_ctx *c, double *mass, double *perm, double *e
   double m2 = 0.0;
   piks_status st = cuda_check(cudaMemcpyAsync(&m2, c->ds.flux_out, sizeof(double), cudaMemcpyDeviceToHost, c->stream), "flux D2H");
   if (!st) st = cuda_check(cudaStreamSynchronize(c->stream), "flux sync");
+  if (!st) st = check_sweep_error(c);
   if (st) return st;
   // output.F90:151-155
   const double kPi = std::atan(1.0) * 4.0;
@@ -684,10 +708,19 @@ piks_status piks_set_tiles(piks_ctx *c, int32_t tx, int32_t ty, int32_t tz) {
   return PIKS_OK;
 }
 
+piks_status piks_set_schedule(piks_ctx *c, int32_t schedule) {
+  if (!c) return fail(PIKS_ERR_ARG, "null context");
+  if (schedule != PIKS_SCHED_TILE_DATAFLOW && schedule != PIKS_SCHED_TILE_DIAGONALS)
+    return fail(PIKS_ERR_ARG, "unknown schedule");
+  c->schedule = schedule;
+  return PIKS_OK;
+}
+
 piks_status piks_get_schedule(piks_ctx *c, int32_t *out, int32_t n) {
   if (!c || !out) return fail(PIKS_ERR_ARG, "null argument");
-  const int32_t v[5] = {c->use_tiles ? 1 : 0, c->tiles.TX, c->tiles.TY, c->tiles.TZ, c->tiles.max_rows};
-  for (int i = 0; i < n && i < 5; ++i) out[i] = v[i];
+  const int32_t v[7] = {c->use_tiles ? 1 : 0, c->tiles.TX, c->tiles.TY, c->tiles.TZ, c->tiles.max_rows,
+                        c->schedule, (int32_t)c->tiles.row_count.size()};
+  for (int i = 0; i < n && i < 7; ++i) out[i] = v[i];
   return PIKS_OK;
 }
 
@@ -814,7 +847,7 @@ piks_status piks_launches_per_iteration(piks_ctx *c, int64_t *n) {
   const DevState &s = c->ds;
   int64_t k = 0;
   if (c->use_tiles) {
-    k += (int64_t)(c->tiles.launches.size() / 4);
+    k += c->schedule == PIKS_SCHED_TILE_DATAFLOW ? 1 : (int64_t)(c->tiles.launches.size() / 4);
   } else {
     for (size_t h = 0; h + 1 < c->geo.hyper_start.size(); ++h) k += c->geo.hyper_start[h + 1] > c->geo.hyper_start[h];
   }
@@ -827,7 +860,9 @@ piks_status piks_launches_per_iteration(piks_ctx *c, int64_t *n) {
 piks_status piks_synchronize(piks_ctx *c) {
   if (!c) return fail(PIKS_ERR_ARG, "null context");
   cudaSetDevice(c->device);
-  return cuda_check(cudaStreamSynchronize(c->stream), "synchronize");
+  piks_status st = cuda_check(cudaStreamSynchronize(c->stream), "synchronize");
+  if (!st && c->have_geometry) st = check_sweep_error(c);
+  return st;
 }
 
 piks_status piks_destroy(piks_ctx *c) {

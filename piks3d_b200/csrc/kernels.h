@@ -14,6 +14,11 @@ struct TileView {
   const int64_t *task_begin;    // [njobs + 1]
   const uint16_t *steps;        // [njobs][steps_stride] task offsets of the local hyperplanes
   const int32_t *job_list;      // job indices in launch order
+  const int32_t *up;            // [njobs][4] upstream jobs (tile neighbours upwind, same octant) or -1
+  int *flags;                   // [njobs][chunks] epoch of the last sweep that finished the item
+  int *counter;                 // work-item counter of the dataflow launch
+  int *err;                     // set when a dependency wait gave up
+  int njobs;
   int nsteps, steps_stride;
 };
 
@@ -87,6 +92,9 @@ void launch_moments32(const DevState &s, cudaStream_t st);
 int tile_sweep_velocities(int Nc8, bool fp32);
 int tile_sweep_max_slots(int Nc8, bool fp32, int tile_voxels, int nsteps);
 void launch_tile_sweep(const DevState &s, bool fp32, int job0, int njobs, int slots, int tasks, cudaStream_t st);
+// Dataflow form: all jobs in one launch, ordered by the flags of `epoch` (> 0, one value per
+// sweep); slots / tasks are the largest of any job.
+void launch_tile_sweep_dataflow(const DevState &s, bool fp32, int epoch, int slots, int tasks, cudaStream_t st);
 void launch_widen(const float *src, double *dst, size_t n, cudaStream_t st);
 void launch_narrow(const double *src, float *dst, size_t n, cudaStream_t st);
 void launch_division_selftest(int64_t samples, uint64_t seed, unsigned long long *mismatches);

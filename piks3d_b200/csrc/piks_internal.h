@@ -121,7 +121,9 @@ struct TileJobs {
   std::vector<int32_t> job_list;     // job indices in launch order
   std::vector<int32_t> launches;     // per launch: first job_list entry, job count, slots, tasks
   std::vector<int32_t> launch_diag_end;  // launch offset after each diagonal
-  int32_t max_rows = 0;
+  std::vector<int32_t> up;           // [njobs][4]: jobs of the upwind x, y, z neighbour tiles (same octant) or -1
+  int32_t max_rows = 0;              // largest slot count of a job
+  int32_t max_tasks = 0;             // largest task count of a job
 };
 
 // Builds the tile jobs from g.tasks; returns false when a job needs more than max_slots

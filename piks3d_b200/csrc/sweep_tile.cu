@@ -59,22 +59,20 @@ __host__ __device__ inline size_t tile_smem_bytes(int slots, int ntask, int step
          (size_t)steps_stride * 2;
 }
 
+// One job (tile, octant) for the velocity chunk `chunk`, by the whole CTA.
 template <typename T, int V>
-__global__ void __launch_bounds__(V / 2 * kGroups)
-k_tile_sweep(const DevState a, int job0, int slots_cap, int tasks_cap) {
+__device__ __forceinline__ void tile_job(const DevState &a, int job, int chunk, int slots_cap, int tasks_cap,
+                                         unsigned char *smem_raw) {
   constexpr int LPT = V / 2;                        // lanes per task
   constexpr int THREADS = LPT * kGroups;
+  constexpr int GROUPS = kGroups;                   // tasks in flight per pass
   constexpr int EPP = 16 / (int)sizeof(T);          // elements per 16-byte piece
   constexpr int PIECES = V / EPP;                   // pieces per row
   using T2 = typename Pair<T>::type;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
   T *S = reinterpret_cast<T *>(smem_raw);
 
   const TileView &tv = a.tv;
   const int Nc8 = a.Nc8;
-  const int nchunk = Nc8 / V;
-  const int job = tv.job_list[job0 + (int)(blockIdx.x / nchunk)];
-  const int chunk = (int)(blockIdx.x % nchunk);
   const int l0 = chunk * V;
   const int64_t rb = tv.row_begin[job];
   const int nrows = tv.row_count[job];
@@ -134,7 +132,7 @@ k_tile_sweep(const DevState a, int job0, int slots_cap, int tasks_cap) {
 
   // 2. the part of every update that does not depend on this sweep's values,
   //    mu * (fEq - f_old / 2) (solver.F90:205-214), replaces f_old in the task's own slot
-  for (int t = grp; t < ntask; t += kGroups) {
+  for (int t = grp; t < ntask; t += GROUPS) {
     const double2 m01 = Mom[2 * t], m23 = Mom[2 * t + 1];
     T2 *own = reinterpret_cast<T2 *>(S + (size_t)(1 + t) * V + 2 * sub);
     const T2 fold = *own;
@@ -170,7 +168,7 @@ k_tile_sweep(const DevState a, int job0, int slots_cap, int tasks_cap) {
   for (int s = 0; s < nsteps; ++s) {
     const int t0 = Steps[s], t1 = Steps[s + 1];
     if (t0 == t1) continue;
-    for (int t = t0 + grp; t < t1; t += kGroups) {
+    for (int t = t0 + grp; t < t1; t += GROUPS) {
       const int4 rec = Trec[t];
       const bool fx = (rec.x >> 27) & 1, fy = (rec.x >> 28) & 1, fz = (rec.x >> 29) & 1;
       const int cls = (fx ? 1 : 0) | (fy ? 2 : 0) | (fz ? 4 : 0);
@@ -232,12 +230,119 @@ k_tile_sweep(const DevState a, int job0, int slots_cap, int tasks_cap) {
 }
 
 template <typename T, int V>
+__global__ void __launch_bounds__(V / 2 * kGroups)
+k_tile_sweep(const DevState a, int job0, int slots_cap, int tasks_cap) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int nchunk = a.Nc8 / V;
+  tile_job<T, V>(a, a.tv.job_list[job0 + (int)(blockIdx.x / nchunk)], (int)(blockIdx.x % nchunk), slots_cap,
+                 tasks_cap, smem_raw);
+}
+
+// Lets `fn` use all the shared memory a block may opt into, less its static shared memory.
+void allow_dynamic_smem(const void *fn, int dev) {
+  cudaFuncAttributes fa{};
+  int optin = 0;
+  if (cudaFuncGetAttributes(&fa, fn) != cudaSuccess ||
+      cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+}
+
+__device__ __forceinline__ int ld_acquire(const int *p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(int *p, int v) {
+  asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Waits until *flag == epoch. Gives up after about a second (kMaxPolls polls) or as soon
+// as another CTA has given up, and then returns false with *err set.
+constexpr int kMaxPolls = 1 << 21;
+__device__ bool wait_flag(const int *flag, int epoch, int *err) {
+  for (int it = 0; it < kMaxPolls; ++it) {
+    if (ld_acquire(flag) == epoch) return true;
+    if ((it & 63) == 63 && ld_acquire(err) != 0) return false;
+    __nanosleep(256);
+  }
+  atomicExch(err, 1);
+  return false;
+}
+
+// Dataflow form of the sweep: one launch per iteration. Work items (job, chunk) are taken
+// in the launch plan's order (diagonal by diagonal) from a global counter; an item first
+// waits until the items of its upstream tiles (same octant, same chunk) carry this
+// iteration's epoch, and publishes its own epoch after its rows are written. Items are
+// claimed in an order in which every upstream item comes first, by CTAs that are running,
+// so the earliest unfinished claimed item can always proceed.
+template <typename T, int V>
+__global__ void __launch_bounds__(V / 2 * kGroups)
+k_tile_sweep_dataflow(const DevState a, int epoch, int slots_cap, int tasks_cap) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ int item_s, skip_s;
+  const TileView &tv = a.tv;
+  const int nchunk = a.Nc8 / V;
+  const int nitems = tv.njobs * nchunk;
+  for (;;) {
+    if (threadIdx.x == 0) { item_s = atomicAdd(tv.counter, 1); skip_s = 0; }
+    __syncthreads();
+    const int item = item_s;
+    if (item >= nitems) break;
+    const int job = tv.job_list[item / nchunk], chunk = item % nchunk;
+    if (threadIdx.x < 3) {
+      const int u = tv.up[4 * job + threadIdx.x];
+      if (u >= 0 && !wait_flag(tv.flags + (size_t)u * nchunk + chunk, epoch, tv.err)) skip_s = 1;
+    }
+    __syncthreads();
+    if (!skip_s) tile_job<T, V>(a, job, chunk, slots_cap, tasks_cap, smem_raw);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      st_release(tv.flags + (size_t)job * nchunk + chunk, epoch);
+    }
+  }
+}
+
+template <typename T, int V>
+void launch_dataflow(const DevState &s, int epoch, int slots, int tasks, cudaStream_t st) {
+  static unsigned long long configured = 0;  // one bit per device
+  static int per_sm[64][2];                  // resident CTAs per SM for the last smem size
+  static size_t per_sm_smem[64];
+  int dev = 0;
+  cudaGetDevice(&dev);
+  dev &= 63;
+  if (!(configured >> dev & 1ull)) {
+    allow_dynamic_smem(reinterpret_cast<const void *>(k_tile_sweep_dataflow<T, V>), dev);
+    configured |= 1ull << dev;
+    per_sm_smem[dev] = 0;
+  }
+  const size_t smem = tile_smem_bytes(slots, tasks, s.tv.steps_stride, V * (int)sizeof(T));
+  if (per_sm_smem[dev] != smem) {
+    int nb = 1, nsm = 148;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_tile_sweep_dataflow<T, V>, V / 2 * kGroups, smem);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    per_sm[dev][0] = nb < 1 ? 1 : nb;
+    per_sm[dev][1] = nsm;
+    per_sm_smem[dev] = smem;
+  }
+  const long items = (long)s.tv.njobs * (s.Nc8 / V);
+  long grid = (long)per_sm[dev][0] * per_sm[dev][1];
+  if (grid > items) grid = items;
+  if (grid < 1) return;
+  cudaMemsetAsync(s.tv.counter, 0, sizeof(int), st);
+  k_tile_sweep_dataflow<T, V><<<(unsigned)grid, V / 2 * kGroups, smem, st>>>(s, epoch, slots, tasks);
+}
+
+template <typename T, int V>
 void launch_one(const DevState &s, int job0, int njobs, int slots, int tasks, cudaStream_t st) {
   static unsigned long long configured = 0;  // one bit per device
   int dev = 0;
   cudaGetDevice(&dev);
   if (!(configured >> (dev & 63) & 1ull)) {
-    cudaFuncSetAttribute(k_tile_sweep<T, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    allow_dynamic_smem(reinterpret_cast<const void *>(k_tile_sweep<T, V>), dev);
     configured |= 1ull << (dev & 63);
   }
   const size_t smem = tile_smem_bytes(slots, tasks, s.tv.steps_stride, V * (int)sizeof(T));
@@ -247,6 +352,7 @@ void launch_one(const DevState &s, int job0, int njobs, int slots, int tasks, cu
 
 }  // namespace
 
+// Velocities per CTA: 128-byte rows where the octant has enough velocities.
 int tile_sweep_velocities(int Nc8, bool fp32) {
   if (fp32) return Nc8 % 32 == 0 ? 32 : Nc8 % 16 == 0 ? 16 : 8;
   return Nc8 % 16 == 0 ? 16 : 8;
@@ -255,7 +361,7 @@ int tile_sweep_velocities(int Nc8, bool fp32) {
 int tile_sweep_max_slots(int Nc8, bool fp32, int tile_voxels, int nsteps) {
   const int row = tile_sweep_velocities(Nc8, fp32) * (fp32 ? 4 : 8);
   const size_t fixed = tile_smem_bytes(0, tile_voxels, (nsteps + 1 + 7) / 8 * 8, row) + 16;
-  const size_t cap = 227 * 1024;
+  const size_t cap = 227 * 1024 - 256;  // less the kernels' static shared memory
   return fixed >= cap ? 0 : (int)((cap - fixed) / (row + 4));
 }
 
@@ -269,6 +375,23 @@ void launch_tile_sweep(const DevState &s, bool fp32, int job0, int njobs, int sl
   } else {
     if (V == 16) launch_one<double, 16>(s, job0, njobs, slots, tasks, st);
     else launch_one<double, 8>(s, job0, njobs, slots, tasks, st);
+  }
+}
+
+}  // namespace piks
+
+namespace piks {
+
+void launch_tile_sweep_dataflow(const DevState &s, bool fp32, int epoch, int slots, int tasks, cudaStream_t st) {
+  if (s.tv.njobs <= 0) return;
+  const int V = tile_sweep_velocities(s.Nc8, fp32);
+  if (fp32) {
+    if (V == 32) launch_dataflow<float, 32>(s, epoch, slots, tasks, st);
+    else if (V == 16) launch_dataflow<float, 16>(s, epoch, slots, tasks, st);
+    else launch_dataflow<float, 8>(s, epoch, slots, tasks, st);
+  } else {
+    if (V == 16) launch_dataflow<double, 16>(s, epoch, slots, tasks, st);
+    else launch_dataflow<double, 8>(s, epoch, slots, tasks, st);
   }
 }
 

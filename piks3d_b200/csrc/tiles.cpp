@@ -67,11 +67,15 @@ bool build_tile_jobs(const Geometry &g, int TX, int TY, int TZ, int max_slots, T
   tj.diag_rows.assign((size_t)ndiag, 0);
   tj.diag_tasks.assign((size_t)ndiag, 0);
   int32_t njobs = 0;
+  std::vector<int64_t> job_tile;
+  std::vector<int8_t> job_oct;
   size_t q = 0;
   while (q < ntask) {
     size_t e = q;
     while (e < ntask && same_job(order[e], order[q])) ++e;
     const int diag = dio[(size_t)order[q]] / 8;
+    job_tile.push_back(tile[(size_t)order[q]]);
+    job_oct.push_back((int8_t)(dio[(size_t)order[q]] % 8));
     const int64_t rb = (int64_t)tj.rows.size();
     tj.row_begin.push_back(rb);
     tj.task_begin.push_back((int64_t)(tj.tasks.size() / 4));
@@ -109,6 +113,7 @@ bool build_tile_jobs(const Geometry &g, int TX, int TY, int TZ, int max_slots, T
     tj.diag_rows[(size_t)diag] = std::max(tj.diag_rows[(size_t)diag], nslots);
     tj.diag_tasks[(size_t)diag] = std::max(tj.diag_tasks[(size_t)diag], (int32_t)(e - q));
     tj.max_rows = std::max(tj.max_rows, nslots);
+    tj.max_tasks = std::max(tj.max_tasks, (int32_t)(e - q));
     // step offsets
     const size_t sb = tj.steps.size();
     tj.steps.resize(sb + (size_t)tj.steps_stride, 0);
@@ -121,6 +126,19 @@ bool build_tile_jobs(const Geometry &g, int TX, int TY, int TZ, int max_slots, T
   tj.row_begin.push_back((int64_t)tj.rows.size());
   tj.task_begin.push_back((int64_t)(tj.tasks.size() / 4));
   for (int d = 0; d < ndiag; ++d) tj.diag_begin[(size_t)d + 1] = std::max(tj.diag_begin[(size_t)d + 1], tj.diag_begin[(size_t)d]);
+  // upstream jobs: the neighbour tiles on the upwind side of each axis, same octant
+  std::vector<int32_t> job_of((size_t)ntiles * 8, -1);
+  for (int32_t j = 0; j < njobs; ++j) job_of[(size_t)job_tile[(size_t)j] * 8 + job_oct[(size_t)j]] = j;
+  tj.up.assign((size_t)njobs * 4, -1);
+  for (int32_t j = 0; j < njobs; ++j) {
+    const int64_t t = job_tile[(size_t)j];
+    const int o = job_oct[(size_t)j];
+    const int a = (int)(t % nTx), b = (int)((t / nTx) % nTy), c = (int)(t / ((int64_t)nTx * nTy));
+    const int na = a - oct_sx(o), nb = b - oct_sy(o), nc = c - oct_sz(o);
+    if (na >= 0 && na < nTx) tj.up[(size_t)j * 4 + 0] = job_of[(size_t)(na + (int64_t)nTx * (b + (int64_t)nTy * c)) * 8 + o];
+    if (nb >= 0 && nb < nTy) tj.up[(size_t)j * 4 + 1] = job_of[(size_t)(a + (int64_t)nTx * (nb + (int64_t)nTy * c)) * 8 + o];
+    if (nc >= 0 && nc < nTz) tj.up[(size_t)j * 4 + 2] = job_of[(size_t)(a + (int64_t)nTx * (b + (int64_t)nTy * nc)) * 8 + o];
+  }
   plan_tile_launches(tj, 1, 0.0);
   return true;
 }

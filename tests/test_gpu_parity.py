@@ -43,7 +43,10 @@ CASES = [
 ]
 
 
-SCHEDULES = {"tiles8": (8, 8, 8), "tiles435": (4, 3, 5), "hyperplanes": (0, 0, 0)}
+SCHEDULES = {"tiles844_dataflow": ((8, 4, 4), pk.SCHED_TILE_DATAFLOW),
+             "tiles435_dataflow": ((4, 3, 5), pk.SCHED_TILE_DATAFLOW),
+             "tiles8_diagonals": ((8, 8, 8), pk.SCHED_TILE_DIAGONALS),
+             "hyperplanes": ((0, 0, 0), pk.SCHED_TILE_DATAFLOW)}
 
 
 @pytest.mark.parametrize("schedule", list(SCHEDULES))
@@ -54,9 +57,11 @@ def test_iterations_bit_exact(name, make, kw, schedule):
     p = base_params(nx, Ny=ny, Nz=nz, **{k: v for k, v in kw.items() if k not in ("Nx", "Ny", "Nz")})
     o = Oracle(p, img.tobytes(), nthreads=4)
     s = pk.Solver(p, device=0)
-    s.set_tiles(*SCHEDULES[schedule])
+    tiles, launch = SCHEDULES[schedule]
+    s.set_tiles(*tiles)
+    s.set_schedule(launch)
     s.setup_physical_grid(img)
-    assert s.schedule()["tiles"] == (SCHEDULES[schedule][0] > 0)
+    assert s.schedule()["tiles"] == (tiles[0] > 0)
     assert np.array_equal(o.labels(), s.get_labels())
     nodes = s.geometry_array("node_g")
     for it in range(5):
