@@ -180,6 +180,27 @@ piks_status piks_run_refined(piks_ctx *ctx, const char *results_path, const char
                              double switch_eps, int32_t *steps32, int32_t *steps, double *permeability,
                              double *seconds);
 
+/* Batches: several solves (contexts with the tile schedule, on one device, of any size,
+ * velocity set, Knudsen number and precision) iterated together. One batch iteration runs,
+ * per (precision, velocity-chunk) class, a single dataflow launch over the tile jobs of all
+ * members, then every member's boundary kernels; after two plain iterations the sequence is
+ * captured as a CUDA graph per iteration parity and replayed until the membership changes.
+ * Each member's values are those of the same solve run alone. While a context is in a
+ * batch, iterate and check it only through the batch. Members may be added and removed
+ * between iterations (continuous batching); piks_set_precision on a member is picked up
+ * at the next batch iteration. No counterpart in the reference (one image per run). */
+typedef struct piks_batch piks_batch;
+piks_status piks_batch_create(int32_t device, piks_batch **out);
+piks_status piks_batch_add(piks_batch *b, piks_ctx *ctx);
+piks_status piks_batch_remove(piks_batch *b, piks_ctx *ctx);
+piks_status piks_batch_size(piks_batch *b, int32_t *n);
+/* nsteps iterations of every member (asynchronous on the batch's stream). */
+piks_status piks_batch_iterate(piks_batch *b, int32_t nsteps);
+/* chkConverge of every member (arrays in membership order, any may be NULL). */
+piks_status piks_batch_chk_converge(piks_batch *b, double *mass, double *permeability, double *error);
+piks_status piks_batch_synchronize(piks_batch *b);
+piks_status piks_batch_destroy(piks_batch *b);
+
 piks_status piks_synchronize(piks_ctx *ctx);
 piks_status piks_destroy(piks_ctx *ctx);
 const char *piks_last_error(void);

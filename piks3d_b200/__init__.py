@@ -90,6 +90,14 @@ def load_library(path=LIB_PATH):
         "piks_get_precision": (i32, [c_void_p, P(i32)]),
         "piks_run_refined": (i32, [c_void_p, ctypes.c_char_p, ctypes.c_char_p, i32, dbl, P(i32), P(i32), P(dbl),
                                    P(dbl)]),
+        "piks_batch_create": (i32, [i32, P(c_void_p)]),
+        "piks_batch_add": (i32, [c_void_p, c_void_p]),
+        "piks_batch_remove": (i32, [c_void_p, c_void_p]),
+        "piks_batch_size": (i32, [c_void_p, P(i32)]),
+        "piks_batch_iterate": (i32, [c_void_p, i32]),
+        "piks_batch_chk_converge": (i32, [c_void_p, P(dbl), P(dbl), P(dbl)]),
+        "piks_batch_synchronize": (i32, [c_void_p]),
+        "piks_batch_destroy": (i32, [c_void_p]),
         "piks_synchronize": (i32, [c_void_p]),
         "piks_destroy": (i32, [c_void_p]),
         "piks_last_error": (ctypes.c_char_p, []),
@@ -295,3 +303,58 @@ class Solver:
         n = ctypes.c_int64()
         _check(self.lib.piks_launches_per_iteration(self._ctx, ctypes.byref(n)))
         return n.value
+
+
+class Batch:
+    """Several solves iterated together on one GPU (piks_batch_*): one dataflow sweep launch
+    per precision class over all members' tile jobs, then each member's boundary kernels,
+    replayed from a captured CUDA graph while the membership is unchanged."""
+
+    def __init__(self, device=0):
+        self.lib = load_library()
+        self._b = ctypes.c_void_p()
+        self.members = []
+        _check(self.lib.piks_batch_create(int(device), ctypes.byref(self._b)))
+
+    def add(self, solver):
+        _check(self.lib.piks_batch_add(self._b, solver._ctx))
+        if solver not in self.members:
+            self.members.append(solver)
+
+    def remove(self, solver):
+        _check(self.lib.piks_batch_remove(self._b, solver._ctx))
+        self.members.remove(solver)
+
+    def __len__(self):
+        return len(self.members)
+
+    def iterate(self, nsteps=1):
+        _check(self.lib.piks_batch_iterate(self._b, int(nsteps)))
+
+    def chk_converge(self):
+        """-> (mass, permeability, error) arrays in membership order."""
+        n = len(self.members)
+        m, k, e = (np.zeros(max(1, n)) for _ in range(3))
+        _check(self.lib.piks_batch_chk_converge(self._b, _dptr(m), _dptr(k), _dptr(e)))
+        return m[:n], k[:n], e[:n]
+
+    def synchronize(self):
+        _check(self.lib.piks_batch_synchronize(self._b))
+
+    def close(self):
+        if self._b:
+            self.lib.piks_batch_destroy(self._b)
+            self._b = ctypes.c_void_p()
+            self.members = []
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -11,9 +11,7 @@
 #include <string>
 #include <vector>
 
-#include "kernels.h"
-#include "piks3d_gpu.h"
-#include "piks_internal.h"
+#include "context.h"
 
 namespace piks {
 void write_fields(const Setup &s, const Geometry &g, const double *rho, const double *ux,
@@ -23,52 +21,27 @@ void write_fields(const Setup &s, const Geometry &g, const double *rho, const do
 using namespace piks;
 
 namespace {
-
 thread_local std::string g_last_error;
+const char kKernelNames[] = "sweep,commit,capture,walls,inlet_outlet,symmetry,moments,flux";
+}  // namespace
+
+namespace piks {
 
 piks_status fail(piks_status st, const std::string &msg) {
   g_last_error = msg;
   return st;
 }
 
-const char kKernelNames[] = "sweep,commit,capture,walls,inlet_outlet,symmetry,moments,flux";
-enum { KT_SWEEP, KT_COMMIT, KT_CAPTURE, KT_WALLS, KT_INLET, KT_SYM, KT_MOM, KT_FLUX, KT_N };
-
-}  // namespace
-
-struct piks_ctx {
-  Setup setup;
-  Velocity vel;
-  Geometry geo;
-  int device = 0;
-  cudaStream_t own_stream = nullptr, stream = nullptr;
-  bool have_geometry = false;       // device state ready
-  bool have_host_geometry = false;  // preprocessing done
-  DevState ds{};
-  std::vector<std::pair<void *, size_t>> allocations;  // device buffers and their bytes
-  size_t dev_bytes = 0;
-  int prec = PIKS_PREC_FP64;        // storage / sweep precision of the state
-  int tile_dims[3] = {8, 4, 4};     // tile shape of the sweep schedule (0: per-node hyperplanes)
-  TileJobs tiles;
-  bool use_tiles = false;           // tile schedule built and uploaded
-  int schedule = PIKS_SCHED_TILE_DIAGONALS;
-  int iStep = 0;
-  double mass = 1.0, error = 1.0, permeability = 0.0;
-  bool timing = false;
-  double kt_ms[KT_N] = {0};
-  int64_t kt_n[KT_N] = {0};
-  std::vector<cudaEvent_t> ev_pool;
-  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
-  size_t ev_next = 0;
-};
-
-namespace {
-
 piks_status cuda_check(cudaError_t e, const char *what) {
   if (e == cudaSuccess) return PIKS_OK;
   if (e == cudaErrorMemoryAllocation) return fail(PIKS_ERR_OOM, std::string(what) + ": " + cudaGetErrorString(e));
   return fail(PIKS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
+
+}  // namespace piks
+
+
+namespace {
 
 template <typename T>
 piks_status upload(piks_ctx *c, const std::vector<T> &v, T **out, size_t min_count = 1) {
@@ -207,12 +180,32 @@ piks_status check_sweep_error(piks_ctx *c) {
   return PIKS_OK;
 }
 
+// The boundary part of iteration n (solver.F90:535-1938): switch commits, halo capture,
+// walls, inlet/outlet, symmetry, moments, on stream st.
+void enqueue_boundaries_timed(piks_ctx *c, cudaStream_t st, int n) {
+  DevState &s = c->ds;
+  const int cap = n & 1, prev = (n - 1) & 1;
+  const bool f32 = c->prec == PIKS_PREC_FP32;
+  { Timed t(c, KT_COMMIT); f32 ? launch_commit32(s, st) : launch_commit(s, st); }
+  { Timed t(c, KT_CAPTURE); f32 ? launch_capture32(s, cap, st) : launch_capture(s, cap, st); }
+  {
+    Timed t(c, KT_WALLS);
+    const auto &ls = c->geo.level_start;
+    for (size_t L = 0; L + 1 < ls.size(); ++L) {
+      if (f32) launch_walls32(s, ls[L], ls[L + 1], prev, st);
+      else launch_walls(s, ls[L], ls[L + 1], prev, st);
+    }
+  }
+  { Timed t(c, KT_INLET); f32 ? launch_inlet_outlet32(s, prev, st) : launch_inlet_outlet(s, prev, st); }
+  { Timed t(c, KT_SYM); f32 ? launch_symmetry32(s, st) : launch_symmetry(s, st); }
+  { Timed t(c, KT_MOM); f32 ? launch_moments32(s, st) : launch_moments(s, st); }
+}
+
 // One source iteration (solver.F90:111-1940) as a launch sequence on the context stream.
 void enqueue_iteration(piks_ctx *c) {
   DevState &s = c->ds;
   cudaStream_t st = c->stream;
   const int n = c->iStep + 1;          // the iteration being run (1-based)
-  const int cap = n & 1, prev = (n - 1) & 1;
   const bool f32 = c->prec == PIKS_PREC_FP32;
   {
     Timed t(c, KT_SWEEP);
@@ -229,24 +222,36 @@ void enqueue_iteration(piks_ctx *c) {
       }
     }
   }
-  { Timed t(c, KT_COMMIT); f32 ? launch_commit32(s, st) : launch_commit(s, st); }
-  { Timed t(c, KT_CAPTURE); f32 ? launch_capture32(s, cap, st) : launch_capture(s, cap, st); }
-  {
-    Timed t(c, KT_WALLS);
-    const auto &ls = c->geo.level_start;
-    for (size_t L = 0; L + 1 < ls.size(); ++L) {
-      if (f32) launch_walls32(s, ls[L], ls[L + 1], prev, st);
-      else launch_walls(s, ls[L], ls[L + 1], prev, st);
-    }
-  }
-  { Timed t(c, KT_INLET); f32 ? launch_inlet_outlet32(s, prev, st) : launch_inlet_outlet(s, prev, st); }
-  { Timed t(c, KT_SYM); f32 ? launch_symmetry32(s, st) : launch_symmetry(s, st); }
-  { Timed t(c, KT_MOM); f32 ? launch_moments32(s, st) : launch_moments(s, st); }
+  enqueue_boundaries_timed(c, st, n);
   c->iStep = n;
   if (c->timing && c->pending.size() > 4096) drain_timing(c);
 }
 
 }  // namespace
+
+namespace piks {
+
+void enqueue_boundaries(piks_ctx *c, cudaStream_t st, int n) {
+  const bool timing = c->timing;
+  c->timing = false;
+  enqueue_boundaries_timed(c, st, n);
+  c->timing = timing;
+}
+
+void launch_check(piks_ctx *c, cudaStream_t st) {
+  const double inv = 1.0 / c->setup.p.Ref_L;
+  launch_flux(c->ds, c->setup.ds, std::sqrt(1.0 / 2.0), inv * inv, st);
+}
+
+// output.F90:151-155
+void finish_check(piks_ctx *c, double m2) {
+  const double kPi = std::atan(1.0) * 4.0;
+  c->error = std::fabs(1.0 - m2 / c->mass) / (double)c->setup.p.chkConvergeStep;
+  c->mass = m2;
+  c->permeability = c->mass * c->setup.p.Kn * std::sqrt(4.0 / kPi);
+}
+
+}  // namespace piks
 
 extern "C" {
 
@@ -437,6 +442,7 @@ piks_status piks_setup_physical_grid(piks_ctx *c, const uint8_t *raw, int64_t nb
   st = cuda_check(cudaStreamSynchronize(c->stream), "setup");
   if (st) return st;
   c->have_geometry = true;
+  c->version += 1;
   c->iStep = 0;
   c->mass = 1.0;  // flow.F90:97
   c->error = 1.0;
@@ -458,21 +464,16 @@ piks_status piks_chk_converge(piks_ctx *c, double *mass, double *perm, double *e
   if (!c) return fail(PIKS_ERR_ARG, "null context");
   if (!c->have_geometry) return fail(PIKS_ERR_STATE, "piks_setup_physical_grid has not been called");
   cudaSetDevice(c->device);
-  const double inv = 1.0 / c->setup.p.Ref_L;
   {
     Timed t(c, KT_FLUX);
-    launch_flux(c->ds, c->setup.ds, std::sqrt(1.0 / 2.0), inv * inv, c->stream);
+    launch_check(c, c->stream);
   }
   double m2 = 0.0;
   piks_status st = cuda_check(cudaMemcpyAsync(&m2, c->ds.flux_out, sizeof(double), cudaMemcpyDeviceToHost, c->stream), "flux D2H");
   if (!st) st = cuda_check(cudaStreamSynchronize(c->stream), "flux sync");
   if (!st) st = check_sweep_error(c);
   if (st) return st;
-  // output.F90:151-155
-  const double kPi = std::atan(1.0) * 4.0;
-  c->error = std::fabs(1.0 - m2 / c->mass) / (double)c->setup.p.chkConvergeStep;
-  c->mass = m2;
-  c->permeability = c->mass * c->setup.p.Kn * std::sqrt(4.0 / kPi);
+  finish_check(c, m2);
   if (mass) *mass = c->mass;
   if (perm) *perm = c->permeability;
   if (err) *err = c->error;
@@ -697,6 +698,7 @@ piks_status piks_set_precision(piks_ctx *c, int32_t precision) {
   if (st) return st;
   free_state(c, c->prec);
   c->prec = precision;
+  c->version += 1;
   return PIKS_OK;
 }
 

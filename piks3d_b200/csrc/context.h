@@ -1,0 +1,52 @@
+// The solver context behind the C ABI's piks_ctx, shared by capi.cu and batch.cu.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "kernels.h"
+#include "piks3d_gpu.h"
+#include "piks_internal.h"
+
+namespace piks {
+enum { KT_SWEEP, KT_COMMIT, KT_CAPTURE, KT_WALLS, KT_INLET, KT_SYM, KT_MOM, KT_FLUX, KT_N };
+piks_status fail(piks_status st, const std::string &msg);   // records the message for piks_last_error
+piks_status cuda_check(cudaError_t e, const char *what);
+}  // namespace piks
+
+struct piks_ctx {
+  piks::Setup setup;
+  piks::Velocity vel;
+  piks::Geometry geo;
+  int device = 0;
+  cudaStream_t own_stream = nullptr, stream = nullptr;
+  bool have_geometry = false;       // device state ready
+  bool have_host_geometry = false;  // preprocessing done
+  piks::DevState ds{};
+  std::vector<std::pair<void *, size_t>> allocations;  // device buffers and their bytes
+  size_t dev_bytes = 0;
+  int prec = PIKS_PREC_FP64;        // storage / sweep precision of the state
+  int tile_dims[3] = {8, 4, 4};     // tile shape of the sweep schedule (0: per-node hyperplanes)
+  piks::TileJobs tiles;
+  bool use_tiles = false;           // tile schedule built and uploaded
+  int schedule = PIKS_SCHED_TILE_DIAGONALS;
+  int iStep = 0;
+  int version = 0;                  // bumped whenever the device state is reallocated
+  double mass = 1.0, error = 1.0, permeability = 0.0;
+  bool timing = false;
+  double kt_ms[piks::KT_N] = {0};
+  int64_t kt_n[piks::KT_N] = {0};
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
+  size_t ev_next = 0;
+};
+
+namespace piks {
+// The boundary part of iteration n (commit ... moments) on stream st, untimed.
+void enqueue_boundaries(piks_ctx *c, cudaStream_t st, int n);
+// chkConverge's flux kernel on stream st, and the host update from its result m2.
+void launch_check(piks_ctx *c, cudaStream_t st);
+void finish_check(piks_ctx *c, double m2);
+}  // namespace piks

@@ -95,6 +95,11 @@ void launch_tile_sweep(const DevState &s, bool fp32, int job0, int njobs, int sl
 // Dataflow form: all jobs in one launch, ordered by the flags of `epoch` (> 0, one value per
 // sweep); slots / tasks are the largest of any job.
 void launch_tile_sweep_dataflow(const DevState &s, bool fp32, int epoch, int slots, int tasks, cudaStream_t st);
+// Batched dataflow sweep over several solves of one precision / chunk width V: states is a
+// device array of DevState, items (member | chunk << 12, job) in dependency order; the
+// members' flags must be zero.
+void launch_tile_sweep_batch(const DevState *states, const int2 *items, int nitems, bool fp32, int V, int slots,
+                             int tasks, int stride, int *counter, int *err, cudaStream_t st);
 void launch_widen(const float *src, double *dst, size_t n, cudaStream_t st);
 void launch_narrow(const double *src, float *dst, size_t n, cudaStream_t st);
 void launch_division_selftest(int64_t samples, uint64_t seed, unsigned long long *mismatches);

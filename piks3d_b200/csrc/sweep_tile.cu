@@ -306,6 +306,62 @@ k_tile_sweep_dataflow(const DevState a, int epoch, int slots_cap, int tasks_cap)
   }
 }
 
+// Batched dataflow sweep: the work items of several solves (one DevState each, in device
+// memory) in one launch. items[i] = (member | chunk << 12, job), ordered so that every
+// item's upstream items (same member, same chunk) come first. A member's flags are cleared
+// before the launch and hold 1 once an item is done.
+template <typename T, int V>
+__global__ void __launch_bounds__(V / 2 * kGroups)
+k_tile_sweep_batch(const DevState *states, const int2 *items, int nitems, int slots_cap, int tasks_cap, int *counter,
+                   int *err) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ int item_s, skip_s;
+  for (;;) {
+    if (threadIdx.x == 0) { item_s = atomicAdd(counter, 1); skip_s = 0; }
+    __syncthreads();
+    const int item = item_s;
+    if (item >= nitems) break;
+    const int2 it = items[item];
+    const int member = it.x & 4095, chunk = it.x >> 12, job = it.y;
+    const DevState &a = states[member];
+    const int nchunk = a.Nc8 / V;
+    if (threadIdx.x < 3) {
+      const int u = a.tv.up[4 * job + threadIdx.x];
+      if (u >= 0 && !wait_flag(a.tv.flags + (size_t)u * nchunk + chunk, 1, err)) skip_s = 1;
+    }
+    __syncthreads();
+    if (!skip_s) tile_job<T, V>(a, job, chunk, slots_cap, tasks_cap, smem_raw);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      st_release(a.tv.flags + (size_t)job * nchunk + chunk, 1);
+    }
+  }
+}
+
+template <typename T, int V>
+void launch_batch(const DevState *states, const int2 *items, int nitems, int slots, int tasks, int stride,
+                  int *counter, int *err, cudaStream_t st) {
+  static unsigned long long configured = 0;  // one bit per device
+  int dev = 0;
+  cudaGetDevice(&dev);
+  dev &= 63;
+  if (!(configured >> dev & 1ull)) {
+    allow_dynamic_smem(reinterpret_cast<const void *>(k_tile_sweep_batch<T, V>), dev);
+    configured |= 1ull << dev;
+  }
+  const size_t smem = tile_smem_bytes(slots, tasks, stride, V * (int)sizeof(T));
+  int nb = 1, nsm = 148;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_tile_sweep_batch<T, V>, V / 2 * kGroups, smem);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  long grid = (long)(nb < 1 ? 1 : nb) * nsm;
+  if (grid > nitems) grid = nitems;
+  if (grid < 1) return;
+  cudaMemsetAsync(counter, 0, sizeof(int), st);
+  k_tile_sweep_batch<T, V><<<(unsigned)grid, V / 2 * kGroups, smem, st>>>(states, items, nitems, slots, tasks, counter,
+                                                                         err);
+}
+
 template <typename T, int V>
 void launch_dataflow(const DevState &s, int epoch, int slots, int tasks, cudaStream_t st) {
   static unsigned long long configured = 0;  // one bit per device
@@ -392,6 +448,23 @@ void launch_tile_sweep_dataflow(const DevState &s, bool fp32, int epoch, int slo
   } else {
     if (V == 16) launch_dataflow<double, 16>(s, epoch, slots, tasks, st);
     else launch_dataflow<double, 8>(s, epoch, slots, tasks, st);
+  }
+}
+
+}  // namespace piks
+
+namespace piks {
+
+void launch_tile_sweep_batch(const DevState *states, const int2 *items, int nitems, bool fp32, int V, int slots,
+                             int tasks, int stride, int *counter, int *err, cudaStream_t st) {
+  if (nitems <= 0) return;
+  if (fp32) {
+    if (V == 32) launch_batch<float, 32>(states, items, nitems, slots, tasks, stride, counter, err, st);
+    else if (V == 16) launch_batch<float, 16>(states, items, nitems, slots, tasks, stride, counter, err, st);
+    else launch_batch<float, 8>(states, items, nitems, slots, tasks, stride, counter, err, st);
+  } else {
+    if (V == 16) launch_batch<double, 16>(states, items, nitems, slots, tasks, stride, counter, err, st);
+    else launch_batch<double, 8>(states, items, nitems, slots, tasks, stride, counter, err, st);
   }
 }
 
