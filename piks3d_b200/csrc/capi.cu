@@ -310,10 +310,19 @@ piks_status piks_create(const piks_params *p, int32_t device, piks_ctx **out) {
   if (!st) st = cuda_check(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking), "cudaStreamCreate");
   if (st) { delete c; return st; }
   c->stream = c->own_stream;
-  upload_tables();
-  upload_tables_fp32();
-  st = cuda_check(cudaGetLastError(), "upload_tables");
-  if (st) { cudaStreamDestroy(c->own_stream); delete c; return st; }
+  {
+    // the wall programs in constant memory are the same for every context: once per device
+    static std::mutex mu;
+    static unsigned long long uploaded = 0;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!(uploaded >> (device & 63) & 1ull)) {
+      upload_tables();
+      upload_tables_fp32();
+      st = cuda_check(cudaGetLastError(), "upload_tables");
+      if (st) { cudaStreamDestroy(c->own_stream); delete c; return st; }
+      uploaded |= 1ull << (device & 63);
+    }
+  }
   *out = c;
   return PIKS_OK;
 }

@@ -1,0 +1,264 @@
+"""Host-side drivers above the C ABI: convergence control for one solve, batched solves of
+many images, and a continuous-batching request server.
+
+Convergence (main.F90:98-121 keeps iterating until chkConverge's error <= eps). Besides
+that rule, a solve can stop at a permeability tolerance: chkConverge runs every
+chkConvergeStep iterations; with d_k the relative change of the mass flux between two
+checks and r = d_k / d_(k-1) the observed contraction per check, the distance of the
+current permeability to the limit of the iteration is estimated as d_k * r / (1 - r)
+(geometric tail, Aitken's estimate); the solve stops once that estimate is below `tol`
+for two checks in a row.
+
+Precision: a "refined" solve runs the FP32 sweep (FP64 moments, wall densities, flux and
+convergence test) until it meets the stopping rule or stops improving, then widens its
+state to FP64 on the device and continues in FP64 until the rule holds in FP64.
+"""
+import concurrent.futures as cf
+import math
+import time
+
+import numpy as np
+
+from . import Batch, PREC_FP32, PREC_FP64, Solver
+
+
+class Convergence:
+    """Per-solve stopping rule over the sequence of chkConverge results."""
+
+    def __init__(self, eps=1e-8, tol=None, stall_checks=5, min_checks=3):
+        self.eps, self.tol, self.stall_checks, self.min_checks = eps, tol, stall_checks, min_checks
+        self.masses = []
+        self.best = math.inf
+        self.since_best = 0
+        self.estimate = math.inf     # estimated relative distance of the permeability to its limit
+        self._prev_ok = False
+
+    def update(self, mass, error):
+        """Records one check; returns True when the solve has converged."""
+        self.masses.append(mass)
+        if error < self.best:
+            self.best, self.since_best = error, 0
+        else:
+            self.since_best += 1
+        if self.tol is None:
+            return error <= self.eps
+        if len(self.masses) < max(3, self.min_checks):
+            return False
+        m2, m1, m0 = self.masses[-1], self.masses[-2], self.masses[-3]
+        d1 = abs(m2 - m1) / max(abs(m2), 1e-300)
+        d0 = abs(m1 - m0) / max(abs(m1), 1e-300)
+        if d1 == 0.0:
+            self.estimate = 0.0
+        elif d0 > 0.0 and d1 < d0:
+            r = d1 / d0
+            self.estimate = d1 * r / (1.0 - r)
+        else:
+            self.estimate = math.inf
+        ok = self.estimate <= self.tol
+        converged = ok and self._prev_ok
+        self._prev_ok = ok
+        return converged
+
+    def stalled(self):
+        return self.since_best >= self.stall_checks
+
+
+class Job:
+    """One solve request: an image (uint8, z-y-x) and its piks_params."""
+
+    def __init__(self, image, params, name=None, arrival=0.0):
+        self.image, self.params, self.name, self.arrival = image, params, name, arrival
+        self.solver = None
+        self.conv = None
+        self.phase = None             # "fp32" / "fp64"
+        self.steps32 = 0
+        self.steps = 0
+        self.result = None
+        self.admitted = None
+        self.finished = None
+        self.footprint = None
+
+
+def footprint_bytes(image, params, precision="refined"):
+    """HBM needed by a solve, estimated from the image before preprocessing: per fluid voxel
+    the distribution function (8 octants x Nc8 velocities, FP32 or FP64) and its FP64 moments,
+    plus the solid voxels next to fluid (walls) and a fixed overhead for tables. A refined
+    solve holds FP32 and FP64 copies of f for the instant of the switch."""
+    nc8 = params.Nc_fundamental ** 3
+    fluid = int(np.count_nonzero(np.asarray(image) == 0))
+    nodes = int(fluid * 1.7) + 2 * params.fluidlayer * image.shape[0] * image.shape[1]
+    f32 = nodes * 8 * nc8 * 4
+    f64 = nodes * 8 * nc8 * 8
+    moments = fluid * 32
+    tables = nodes * 8 * 48 + (64 << 20)
+    if precision == "fp64":
+        return f64 + moments + tables
+    if precision == "fp32":
+        return f32 + moments + tables
+    return f32 + f64 + moments + tables
+
+
+def _prepare(job, device, precision):
+    s = Solver(job.params, device=device)
+    if precision in ("fp32", "refined"):
+        s.set_precision(PREC_FP32)
+    s.setup_physical_grid(job.image)
+    return s
+
+
+class BatchRunner:
+    """Solves many jobs on one GPU as a continuously refilled batch: jobs are admitted while
+    their estimated footprint fits the HBM budget and the batch has a free slot, preprocessed
+    on host threads while the GPU iterates, iterated together (piks_batch_*), checked every
+    chkConvergeStep iterations, switched from FP32 to FP64 when their FP32 phase ends, and
+    retired (state freed) as soon as they converge."""
+
+    def __init__(self, device=0, precision="refined", tol=1e-4, eps=None, switch_eps=1e-6, max_members=64,
+                 hbm_budget=None, prep_threads=4, keep_fields=False):
+        import torch  # noqa: F401  (device memory query only)
+        self.device, self.precision, self.tol, self.eps = device, precision, tol, eps
+        self.switch_eps, self.max_members, self.keep_fields = switch_eps, max_members, keep_fields
+        if hbm_budget is None:
+            import torch
+            free, _total = torch.cuda.mem_get_info(device)
+            hbm_budget = int(free * 0.85)
+        self.hbm_budget = hbm_budget
+        self.pool = cf.ThreadPoolExecutor(max_workers=prep_threads)
+        self.batch = Batch(device=device)
+        self.active = []
+        self.preparing = []           # (job, future)
+        self.reserved = 0
+
+    def close(self):
+        for j in self.active:
+            j.solver.close()
+        self.active = []
+        for j, fut in self.preparing:
+            try:
+                fut.result().close()
+            except Exception:
+                pass
+        self.preparing = []
+        self.batch.close()
+        self.pool.shutdown(wait=True)
+
+    def _chk_step(self):
+        return self.active[0].params.chkConvergeStep if self.active else 10
+
+    def try_admit(self, job, now):
+        """Starts preprocessing `job` if its footprint fits; returns False when it must wait."""
+        fp = footprint_bytes(job.image, job.params, self.precision)
+        slots = len(self.active) + len(self.preparing)
+        if slots >= self.max_members or (self.reserved + fp > self.hbm_budget and slots > 0):
+            return False
+        job.footprint = fp
+        job.admitted = now
+        self.reserved += fp
+        self.preparing.append((job, self.pool.submit(_prepare, job, self.device, self.precision)))
+        return True
+
+    def _join_ready(self, block=False):
+        still = []
+        for job, fut in self.preparing:
+            if block or fut.done():
+                job.solver = fut.result()
+                job.phase = "fp64" if self.precision == "fp64" else "fp32"
+                job.conv = self._new_conv(job)
+                self.batch.add(job.solver)
+                self.active.append(job)
+            else:
+                still.append((job, fut))
+        self.preparing = still
+
+    def _new_conv(self, job):
+        eps = self.eps if self.eps is not None else job.params.eps
+        if job.phase == "fp32" and self.precision == "refined":
+            return Convergence(eps=max(eps, self.switch_eps), tol=self.tol)
+        return Convergence(eps=eps, tol=self.tol)
+
+    def step(self):
+        """Admitted jobs that finished preprocessing join; one chkConvergeStep of iterations;
+        one check; finished jobs leave. Returns the jobs that finished."""
+        self._join_ready(block=not self.active and bool(self.preparing))
+        if not self.active:
+            return []
+        chk = self._chk_step()
+        self.batch.iterate(chk)
+        mass, perm, err = self.batch.chk_converge()
+        done = []
+        for i, job in enumerate(list(self.active)):
+            job.steps += chk
+            if job.phase == "fp32":
+                job.steps32 += chk
+            conv = job.conv.update(mass[i], err[i])
+            if job.phase == "fp32" and self.precision == "refined" and (conv or job.conv.stalled()):
+                # the FP64 phase continues from the widened FP32 iterate
+                job.solver.set_precision(PREC_FP64)
+                job.phase = "fp64"
+                job.conv = self._new_conv(job)
+                job.conv.masses = [mass[i]]
+                continue
+            if conv or job.steps >= job.params.maxStep:
+                job.result = {"steps": job.steps, "steps32": job.steps32, "mass": float(mass[i]),
+                              "permeability": float(perm[i]), "error": float(err[i]),
+                              "converged": bool(conv), "estimate": job.conv.estimate}
+                if self.keep_fields:
+                    job.result["macro"] = job.solver.get_macro()
+                done.append(job)
+        for job in done:
+            self.batch.remove(job.solver)
+            self.active.remove(job)
+            job.solver.close()
+            job.solver = None
+            self.reserved -= job.footprint
+            job.finished = time.perf_counter()
+        return done
+
+    def run(self, jobs):
+        """Solves `jobs` (all available at once) and returns them with results."""
+        t0 = time.perf_counter()
+        pending = list(jobs)
+        finished = []
+        while pending or self.active or self.preparing:
+            now = time.perf_counter() - t0
+            while pending and self.try_admit(pending[0], now):
+                pending.pop(0)
+            finished.extend(self.step())
+        return finished
+
+
+def solve_one(image, params, device=0, precision="fp64", tol=None, eps=None, switch_eps=1e-6, tiles=None,
+              keep_fields=False):
+    """One solve through a context of its own (no batch): the reference's loop with the same
+    stopping rule as the batch runner. Returns a result dict."""
+    s = Solver(params, device=device)
+    if tiles is not None:
+        s.set_tiles(*tiles)
+    if precision in ("fp32", "refined"):
+        s.set_precision(PREC_FP32)
+    s.setup_physical_grid(image)
+    chk = params.chkConvergeStep
+    phase = "fp64" if precision == "fp64" else "fp32"
+    base_eps = eps if eps is not None else params.eps
+    conv = Convergence(eps=max(base_eps, switch_eps) if precision == "refined" else base_eps, tol=tol)
+    steps = steps32 = 0
+    while True:
+        s.iterate(chk)
+        steps += chk
+        if phase == "fp32":
+            steps32 += chk
+        m, k, e = s.chk_converge()
+        ok = conv.update(m, e)
+        if phase == "fp32" and precision == "refined" and (ok or conv.stalled()):
+            s.set_precision(PREC_FP64)
+            phase = "fp64"
+            conv = Convergence(eps=base_eps, tol=tol)
+            conv.masses = [m]
+            continue
+        if ok or steps >= params.maxStep:
+            res = {"steps": steps, "steps32": steps32, "mass": m, "permeability": k, "error": e,
+                   "converged": bool(ok), "estimate": conv.estimate}
+            if keep_fields:
+                res["macro"] = s.get_macro()
+            s.close()
+            return res

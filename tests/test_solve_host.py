@@ -1,0 +1,121 @@
+"""Host logic of the drivers (no GPU): the permeability-tolerance stopping rule, the HBM
+footprint estimate, and the request server's queueing, admission and latency accounting
+(driven by a stand-in runner and a simulated clock)."""
+import math
+
+import numpy as np
+
+import piks3d_b200 as pk
+from piks3d_b200.solve import Convergence, Job, footprint_bytes
+from piks3d_b200.serve import Server, percentile, poisson_arrivals
+
+
+def test_tolerance_rule_on_geometric_sequence():
+    for r in (0.3, 0.7, 0.95):
+        c = Convergence(tol=1e-4)
+        for k in range(1, 2000):
+            m = 2.0 * (1.0 - 0.5 * r ** k)
+            if c.update(m, 0.1):
+                break
+        limit = 2.0
+        assert abs(m - limit) / limit <= 1e-4, (r, k)
+        assert abs(m - limit) / limit >= 1e-7, "stopped far later than needed"
+
+
+def test_tolerance_rule_waits_on_non_contracting_changes():
+    c = Convergence(tol=1e-4)
+    out = [c.update(1.0 + 0.01 * ((-1) ** k), 0.1) for k in range(20)]
+    assert not any(out) and math.isinf(c.estimate)
+
+
+def test_eps_rule_and_stall():
+    c = Convergence(eps=1e-8)
+    assert not c.update(1.0, 1e-7) and c.update(1.0, 1e-9)
+    c = Convergence(eps=1e-12, stall_checks=3)
+    for e in (1e-6, 2e-6, 3e-6, 4e-6):
+        c.update(1.0, e)
+    assert c.stalled()
+
+
+def test_footprint_orders():
+    p = pk.default_params(Nx=32, Ny=32, Nz=32, Nc_fundamental=4)
+    img = np.zeros((32, 32, 32), np.uint8)
+    f32 = footprint_bytes(img, p, "fp32")
+    f64 = footprint_bytes(img, p, "fp64")
+    ref = footprint_bytes(img, p, "refined")
+    assert f32 < f64 < ref
+    assert f64 - f32 >= 32 ** 3 * 8 * 64 * 4
+
+
+def test_poisson_arrivals_rate():
+    t = poisson_arrivals(20.0, 60.0, seed=1)
+    assert 1000 < len(t) < 1400 and all(0 <= a < 60 for a in t) and t == sorted(t)
+
+
+class FakeClock:
+    def __init__(self):
+        self.t = 0.0
+
+    def __call__(self):
+        return self.t
+
+    def sleep(self, dt):
+        self.t += max(dt, 1e-3)
+
+
+class FakeRunner:
+    """Stand-in for BatchRunner: each job needs `work` checks; a check takes 0.1 s; at most
+    `slots` jobs at once."""
+
+    def __init__(self, clock, slots=2):
+        self.clock, self.slots = clock, slots
+        self.active, self.preparing = [], []
+
+    def try_admit(self, job, now):
+        if len(self.active) >= self.slots:
+            return False
+        job.left = job.work
+        self.active.append(job)
+        return True
+
+    def step(self):
+        self.clock.t += 0.1
+        done = []
+        for j in list(self.active):
+            j.left -= 1
+            if j.left == 0:
+                j.finished = self.clock.t
+                self.active.remove(j)
+                done.append(j)
+        return done
+
+
+def test_server_fifo_admission_and_latency():
+    clock = FakeClock()
+    runner = FakeRunner(clock, slots=2)
+    jobs = []
+    for i, (arr, work) in enumerate([(0.0, 3), (0.05, 1), (0.06, 2), (1.0, 1)]):
+        j = Job(None, None, name=str(i), arrival=arr)
+        j.work = work
+        jobs.append(j)
+    rep = Server(runner, clock=clock, sleep=clock.sleep).run(jobs)
+    assert rep["completed"] == 4 and rep["unfinished"] == 0
+    lat = {j.name: round(j.latency, 6) for j in rep["jobs"]}
+    # job 0 and 1 start at t=0 (job 1 only arrives at 0.05: admitted at the next check), job 2 waits for a slot
+    assert lat["0"] == 0.3
+    assert lat["1"] == round(0.2 - 0.05, 6)
+    assert lat["2"] == round(0.4 - 0.06, 6)
+    assert lat["3"] < 0.2
+    assert abs(rep["latency_p50_s"] - percentile(list(lat.values()), 50)) < 1e-9
+
+
+def test_server_horizon_stops_with_unfinished():
+    clock = FakeClock()
+    runner = FakeRunner(clock, slots=1)
+    jobs = []
+    for i in range(5):
+        j = Job(None, None, name=str(i), arrival=0.0)
+        j.work = 10
+        jobs.append(j)
+    rep = Server(runner, horizon=1.5, clock=clock, sleep=clock.sleep).run(jobs)
+    assert rep["completed"] == 1 and rep["unfinished"] == 4
