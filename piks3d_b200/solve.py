@@ -4,10 +4,9 @@ many images, and a continuous-batching request server.
 Convergence (main.F90:98-121 keeps iterating until chkConverge's error <= eps). Besides
 that rule, a solve can stop at a permeability tolerance: chkConverge runs every
 chkConvergeStep iterations; with d_k the relative change of the mass flux between two
-checks and r = d_k / d_(k-1) the observed contraction per check, the distance of the
-current permeability to the limit of the iteration is estimated as d_k * r / (1 - r)
-(geometric tail, Aitken's estimate); the solve stops once that estimate is below `tol`
-for two checks in a row.
+checks and r the observed contraction per check, the distance of the current
+permeability to the limit of the iteration is estimated as d_k * r / (1 - r) (geometric
+tail, as in Aitken's extrapolation); see Convergence for the exact rule.
 
 Precision: a "refined" solve runs the FP32 sweep (FP64 moments, wall densities, flux and
 convergence test) until it meets the stopping rule or stops improving, then widens its
@@ -23,15 +22,24 @@ from . import Batch, PREC_FP32, PREC_FP64, Solver
 
 
 class Convergence:
-    """Per-solve stopping rule over the sequence of chkConverge results."""
+    """Per-solve stopping rule over the sequence of chkConverge results.
 
-    def __init__(self, eps=1e-8, tol=None, stall_checks=5, min_checks=3):
-        self.eps, self.tol, self.stall_checks, self.min_checks = eps, tol, stall_checks, min_checks
+    With `tol` set: after at least `min_checks` checks, r is the largest of the last three
+    ratios d_k / d_(k-1) of successive relative mass-flux changes; when all three are below
+    1 the remaining relative distance to the limit is estimated as d_k * r / (1 - r), and
+    the solve stops once the estimate is below safety * tol at `consec` checks in a row.
+    (Early transients of the source iteration can show a few shrinking changes before the
+    slow mode takes over; requiring three contracting ratios and three passing checks is
+    what keeps the rule from stopping there.)"""
+
+    def __init__(self, eps=1e-8, tol=None, stall_checks=5, min_checks=5, consec=3, safety=0.5):
+        self.eps, self.tol, self.stall_checks = eps, tol, stall_checks
+        self.min_checks, self.consec, self.safety = min_checks, consec, safety
         self.masses = []
         self.best = math.inf
         self.since_best = 0
         self.estimate = math.inf     # estimated relative distance of the permeability to its limit
-        self._prev_ok = False
+        self._ok_run = 0
 
     def update(self, mass, error):
         """Records one check; returns True when the solve has converged."""
@@ -42,22 +50,18 @@ class Convergence:
             self.since_best += 1
         if self.tol is None:
             return error <= self.eps
-        if len(self.masses) < max(3, self.min_checks):
+        if len(self.masses) < max(5, self.min_checks):
             return False
-        m2, m1, m0 = self.masses[-1], self.masses[-2], self.masses[-3]
-        d1 = abs(m2 - m1) / max(abs(m2), 1e-300)
-        d0 = abs(m1 - m0) / max(abs(m1), 1e-300)
-        if d1 == 0.0:
+        m = self.masses
+        d = [abs(m[-1 - i] - m[-2 - i]) / max(abs(m[-1 - i]), 1e-300) for i in range(4)]
+        if d[0] == 0.0:
             self.estimate = 0.0
-        elif d0 > 0.0 and d1 < d0:
-            r = d1 / d0
-            self.estimate = d1 * r / (1.0 - r)
         else:
-            self.estimate = math.inf
-        ok = self.estimate <= self.tol
-        converged = ok and self._prev_ok
-        self._prev_ok = ok
-        return converged
+            rs = [d[i] / d[i + 1] if d[i + 1] > 0.0 else math.inf for i in range(3)]
+            r = max(rs)
+            self.estimate = d[0] * r / (1.0 - r) if r < 1.0 else math.inf
+        self._ok_run = self._ok_run + 1 if self.estimate <= self.safety * self.tol else 0
+        return self._ok_run >= self.consec
 
     def stalled(self):
         return self.since_best >= self.stall_checks

@@ -119,3 +119,26 @@ def test_server_horizon_stops_with_unfinished():
         jobs.append(j)
     rep = Server(runner, horizon=1.5, clock=clock, sleep=clock.sleep).run(jobs)
     assert rep["completed"] == 1 and rep["unfinished"] == 4
+
+
+def test_tolerance_rule_on_oracle_traces():
+    """The rule applied to the oracle's own mass-flux trace stops within the tolerance of
+    the converged value (pack with an early transient, and a single sphere)."""
+    from piks3d_b200 import images
+    from conftest import base_params
+    from oracle import Oracle
+    cases = [(images.sphere_pack(18, 0.45, 2.0, 4.0, seed=3), base_params(18, Nc_fundamental=2, Kn=2.0, fluidlayer=2)),
+             (images.centred_sphere(20, 7.0), base_params(20, Nc_fundamental=2, Kn=1.0))]
+    for img, p in cases:
+        o = Oracle(p, img.tobytes(), nthreads=4)
+        ms = []
+        for _ in range(100):
+            o.iterate(10)
+            m, _, e = o.chk_converge()
+            ms.append(m)
+            if e < 1e-12:
+                break
+        o.close()
+        c = Convergence(tol=1e-4)
+        stop = next(k for k, m in enumerate(ms) if c.update(m, 1.0))
+        assert abs(ms[stop] - ms[-1]) / abs(ms[-1]) <= 1e-4
