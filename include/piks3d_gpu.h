@@ -166,6 +166,13 @@ piks_status piks_set_tiles(piks_ctx *ctx, int32_t tx, int32_t ty, int32_t tz);
  * PIKS_ERR_CUDA). */
 enum { PIKS_SCHED_TILE_DATAFLOW = 0, PIKS_SCHED_TILE_DIAGONALS = 1 };
 piks_status piks_set_schedule(piks_ctx *ctx, int32_t schedule);
+/* Autotuner of the sweep schedule: right after piks_setup_physical_grid (before the first
+ * iteration) times `sweeps` sweeps of each candidate (4 int32 each: TX, TY, TZ, launch
+ * schedule; NULL / ncand 0 = a built-in list) on this image, keeps the fastest, and resets
+ * the state to setupFlow's zeros. chosen (4 int32) receives the winner, ms_out (ncand) the
+ * milliseconds per sweep of each candidate (-1 where a candidate does not apply). */
+piks_status piks_autotune(piks_ctx *ctx, const int32_t *candidates, int32_t ncand, int32_t sweeps,
+                          int32_t *chosen, double *ms_out);
 /* [tile schedule in use (0/1), TX, TY, TZ, largest shared-memory slot count of a job,
  *  launch schedule, number of jobs] */
 piks_status piks_get_schedule(piks_ctx *ctx, int32_t *out, int32_t n);

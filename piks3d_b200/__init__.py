@@ -87,6 +87,7 @@ def load_library(path=LIB_PATH):
         "piks_set_tiles": (i32, [c_void_p, i32, i32, i32]),
         "piks_get_schedule": (i32, [c_void_p, P(i32), i32]),
         "piks_set_schedule": (i32, [c_void_p, i32]),
+        "piks_autotune": (i32, [c_void_p, P(i32), i32, i32, P(i32), P(dbl)]),
         "piks_get_precision": (i32, [c_void_p, P(i32)]),
         "piks_run_refined": (i32, [c_void_p, ctypes.c_char_p, ctypes.c_char_p, i32, dbl, P(i32), P(i32), P(dbl),
                                    P(dbl)]),
@@ -220,6 +221,19 @@ class Solver:
     def set_schedule(self, schedule):
         """SCHED_TILE_DATAFLOW (one launch per sweep) or SCHED_TILE_DIAGONALS."""
         _check(self.lib.piks_set_schedule(self._ctx, int(schedule)))
+
+    def autotune(self, candidates=None, sweeps=2):
+        """Times each (TX, TY, TZ, schedule) candidate on this image right after setup, keeps
+        the fastest and resets the state; -> (chosen, {candidate: ms per sweep})."""
+        if candidates:
+            flat = (ctypes.c_int32 * (4 * len(candidates)))(*[int(v) for c in candidates for v in c])
+            n = len(candidates)
+        else:
+            flat, n = None, 5
+        chosen = (ctypes.c_int32 * 4)()
+        ms = (ctypes.c_double * max(n, 5))()
+        _check(self.lib.piks_autotune(self._ctx, flat, len(candidates) if candidates else 0, int(sweeps), chosen, ms))
+        return tuple(chosen), ms[:n]
 
     def schedule(self):
         """{'tiles': bool, 'TX', 'TY', 'TZ', 'max_slots', 'launch', 'jobs'} of the sweep schedule."""

@@ -201,11 +201,9 @@ void enqueue_boundaries_timed(piks_ctx *c, cudaStream_t st, int n) {
   { Timed t(c, KT_MOM); f32 ? launch_moments32(s, st) : launch_moments(s, st); }
 }
 
-// One source iteration (solver.F90:111-1940) as a launch sequence on the context stream.
-void enqueue_iteration(piks_ctx *c) {
+// The eight octant sweeps (solver.F90:176-526) of iteration n on stream st.
+void enqueue_sweep(piks_ctx *c, cudaStream_t st, int n) {
   DevState &s = c->ds;
-  cudaStream_t st = c->stream;
-  const int n = c->iStep + 1;          // the iteration being run (1-based)
   const bool f32 = c->prec == PIKS_PREC_FP32;
   {
     Timed t(c, KT_SWEEP);
@@ -222,9 +220,69 @@ void enqueue_iteration(piks_ctx *c) {
       }
     }
   }
-  enqueue_boundaries_timed(c, st, n);
+}
+
+// One source iteration (solver.F90:111-1940) as a launch sequence on the context stream.
+void enqueue_iteration(piks_ctx *c) {
+  const int n = c->iStep + 1;          // the iteration being run (1-based)
+  enqueue_sweep(c, c->stream, n);
+  enqueue_boundaries_timed(c, c->stream, n);
   c->iStep = n;
   if (c->timing && c->pending.size() > 4096) drain_timing(c);
+}
+
+// Tile schedule of the context's tile_dims on the host (false: not usable, e.g. a job needs
+// more shared memory than a block has).
+bool build_tiles(piks_ctx *c) {
+  c->use_tiles = false;
+  c->tiles = TileJobs{};
+  if (c->tile_dims[0] <= 0) return false;
+  const int vox = c->tile_dims[0] * c->tile_dims[1] * c->tile_dims[2];
+  const int nst = c->tile_dims[0] + c->tile_dims[1] + c->tile_dims[2] - 2;
+  const int slots = std::min(tile_sweep_max_slots(c->vel.Nc8, false, vox, nst),
+                             tile_sweep_max_slots(c->vel.Nc8, true, vox, nst));
+  c->use_tiles = build_tile_jobs(c->geo, c->tile_dims[0], c->tile_dims[1], c->tile_dims[2], slots, c->tiles);
+  if (!c->use_tiles) c->tiles = TileJobs{};
+  return c->use_tiles;
+}
+
+// Device copy of the tile schedule (replacing an earlier one), with zeroed dataflow flags.
+piks_status upload_tiles(piks_ctx *c) {
+  DevState &s = c->ds;
+  TileView &tv = s.tv;
+  for (const void *p : {(const void *)tv.rows, (const void *)tv.row_begin, (const void *)tv.row_count,
+                        (const void *)tv.tasks, (const void *)tv.task_begin, (const void *)tv.steps,
+                        (const void *)tv.job_list, (const void *)tv.up, (const void *)tv.flags,
+                        (const void *)tv.counter})
+    if (p) release(c, const_cast<void *>(p));
+  tv = TileView{};
+  if (!c->use_tiles) return PIKS_OK;
+  const TileJobs &tj = c->tiles;
+  piks_status st;
+  int32_t *pi = nullptr;
+  int64_t *p64 = nullptr;
+  uint16_t *p16 = nullptr;
+#define UPT(vec, field, ptr) do { if ((st = upload(c, vec, &ptr))) return st; tv.field = ptr; } while (0)
+  UPT(tj.rows, rows, pi);
+  UPT(tj.row_begin, row_begin, p64);
+  UPT(tj.row_count, row_count, pi);
+  if ((st = upload(c, tj.tasks, &pi))) return st;
+  tv.tasks = reinterpret_cast<const int4 *>(pi);
+  UPT(tj.task_begin, task_begin, p64);
+  UPT(tj.steps, steps, p16);
+  UPT(tj.job_list, job_list, pi);
+  UPT(tj.up, up, pi);
+#undef UPT
+  tv.njobs = (int)(tj.row_count.size());
+  int *pw = nullptr;
+  if ((st = zeros(c, (size_t)tv.njobs * (size_t)(c->vel.Nc8 / 8 > 0 ? c->vel.Nc8 / 8 : 1), &pw))) return st;
+  tv.flags = pw;
+  if ((st = zeros(c, (size_t)2, &pw))) return st;
+  tv.counter = pw;
+  tv.err = pw + 1;
+  tv.nsteps = tj.nsteps;
+  tv.steps_stride = tj.steps_stride;
+  return PIKS_OK;
 }
 
 }  // namespace
@@ -335,16 +393,7 @@ piks_status piks_setup_physical_grid(piks_ctx *c, const uint8_t *raw, int64_t nb
   piks_status st = preprocess(c->setup, raw, nbytes, c->geo, err);
   if (st) return fail(st, err);
   c->have_host_geometry = true;
-  c->use_tiles = false;
-  c->tiles = TileJobs{};
-  if (c->tile_dims[0] > 0) {
-    const int vox = c->tile_dims[0] * c->tile_dims[1] * c->tile_dims[2];
-    const int nst = c->tile_dims[0] + c->tile_dims[1] + c->tile_dims[2] - 2;
-    const int slots = std::min(tile_sweep_max_slots(c->vel.Nc8, false, vox, nst),
-                               tile_sweep_max_slots(c->vel.Nc8, true, vox, nst));
-    c->use_tiles = build_tile_jobs(c->geo, c->tile_dims[0], c->tile_dims[1], c->tile_dims[2], slots, c->tiles);
-    if (!c->use_tiles) c->tiles = TileJobs{};
-  }
+  build_tiles(c);
   if (c->device < 0) return PIKS_OK;
   const Geometry &g = c->geo;
   const Velocity &v = c->vel;
@@ -416,30 +465,8 @@ piks_status piks_setup_physical_grid(piks_ctx *c, const uint8_t *raw, int64_t nb
     }
     UP(g.tasks, tasks, pi);
   }
-  if (c->use_tiles) {
-    const TileJobs &tj = c->tiles;
-    int64_t *p64 = nullptr;
-    UP(tj.rows, tv.rows, pi);
-    UP(tj.row_begin, tv.row_begin, p64);
-    UP(tj.row_count, tv.row_count, pi);
-    if ((st = upload(c, tj.tasks, &pi))) return st;
-    s.tv.tasks = reinterpret_cast<const int4 *>(pi);
-    UP(tj.task_begin, tv.task_begin, p64);
-    uint16_t *p16 = nullptr;
-    UP(tj.steps, tv.steps, p16);
-    UP(tj.job_list, tv.job_list, pi);
-    UP(tj.up, tv.up, pi);
-    s.tv.njobs = (int)(tj.row_count.size());
-    int *pw = nullptr;
-    if ((st = zeros(c, (size_t)s.tv.njobs * (size_t)(v.Nc8 / 8 > 0 ? v.Nc8 / 8 : 1), &pw))) return st;
-    s.tv.flags = pw;
-    if ((st = zeros(c, (size_t)2, &pw))) return st;
-    s.tv.counter = pw;
-    s.tv.err = pw + 1;
-    s.tv.nsteps = tj.nsteps;
-    s.tv.steps_stride = tj.steps_stride;
-  }
 #undef UP
+  if ((st = upload_tiles(c))) return st;
   s.nWall = g.nWall;
   s.ncommit = (int)(g.commit.size() / 3);
   s.nsym = (int)g.sym_node.size();
@@ -733,6 +760,74 @@ piks_status piks_get_schedule(piks_ctx *c, int32_t *out, int32_t n) {
                         c->schedule, (int32_t)c->tiles.row_count.size()};
   for (int i = 0; i < n && i < 7; ++i) out[i] = v[i];
   return PIKS_OK;
+}
+
+piks_status piks_autotune(piks_ctx *c, const int32_t *cand, int32_t ncand, int32_t sweeps, int32_t *chosen,
+                          double *ms_out) {
+  if (!c) return fail(PIKS_ERR_ARG, "null context");
+  if (c->device < 0 || !c->have_geometry) return fail(PIKS_ERR_STATE, "piks_autotune needs a device state");
+  if (c->iStep != 0) return fail(PIKS_ERR_STATE, "piks_autotune must run before the first iteration");
+  static const int32_t kDefault[] = {8, 4, 4, PIKS_SCHED_TILE_DIAGONALS, 8, 4, 4, PIKS_SCHED_TILE_DATAFLOW,
+                                     4, 4, 4, PIKS_SCHED_TILE_DIAGONALS, 4, 4, 4, PIKS_SCHED_TILE_DATAFLOW,
+                                     8, 8, 4, PIKS_SCHED_TILE_DIAGONALS};
+  if (!cand || ncand <= 0) { cand = kDefault; ncand = 5; }
+  if (sweeps < 1) sweeps = 1;
+  cudaSetDevice(c->device);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const bool timing = c->timing;
+  c->timing = false;
+  double best = 1e300;
+  int bi = -1;
+  piks_status st = PIKS_OK;
+  int epoch = 1;
+  for (int i = 0; i < ncand && !st; ++i) {
+    const int32_t *k = cand + 4 * i;
+    if (ms_out) ms_out[i] = -1.0;
+    if (k[0] < 2 || k[1] < 2 || k[2] < 2 || (int64_t)k[0] * k[1] * k[2] > 65535) continue;
+    if (k[3] != PIKS_SCHED_TILE_DIAGONALS && k[3] != PIKS_SCHED_TILE_DATAFLOW) continue;
+    c->tile_dims[0] = k[0]; c->tile_dims[1] = k[1]; c->tile_dims[2] = k[2];
+    if (!build_tiles(c)) continue;
+    if ((st = upload_tiles(c))) break;
+    c->schedule = k[3];
+    enqueue_sweep(c, c->stream, epoch++);  // warm-up
+    cudaEventRecord(e0, c->stream);
+    for (int r = 0; r < sweeps; ++r) enqueue_sweep(c, c->stream, epoch++);
+    cudaEventRecord(e1, c->stream);
+    if ((st = cuda_check(cudaEventSynchronize(e1), "autotune"))) break;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    const double per = ms / sweeps;
+    if (ms_out) ms_out[i] = per;
+    if (per < best) { best = per; bi = i; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->timing = timing;
+  if (st) return st;
+  if (bi < 0) return fail(PIKS_ERR_ARG, "no usable tile candidate");
+  const int32_t *k = cand + 4 * bi;
+  c->tile_dims[0] = k[0]; c->tile_dims[1] = k[1]; c->tile_dims[2] = k[2];
+  build_tiles(c);
+  if ((st = upload_tiles(c))) return st;
+  c->schedule = k[3];
+  // the trial sweeps changed f: back to the state of setupFlow (all zero)
+  const StateSizes z = state_sizes(c);
+  DevState &s = c->ds;
+  const size_t e = c->prec == PIKS_PREC_FP32 ? sizeof(float) : sizeof(double);
+  void *hs = c->prec == PIKS_PREC_FP32 ? (void *)s.h32 : (void *)s.h;
+  void *fws = c->prec == PIKS_PREC_FP32 ? (void *)s.fw32 : (void *)s.fw;
+  cudaMemsetAsync(hs, 0, z.h * e, c->stream);
+  if (z.fw) cudaMemsetAsync(fws, 0, z.fw * e, c->stream);
+  for (int b = 0; b < 2; ++b) {
+    cudaMemsetAsync(c->prec == PIKS_PREC_FP32 ? (void *)s.ghostW32[b] : (void *)s.ghostW[b], 0, z.plane * e, c->stream);
+    cudaMemsetAsync(c->prec == PIKS_PREC_FP32 ? (void *)s.ghostE32[b] : (void *)s.ghostE[b], 0, z.plane * e, c->stream);
+  }
+  cudaMemsetAsync(s.mom, 0, (size_t)c->geo.NF * 4 * sizeof(double), c->stream);
+  c->version += 1;
+  if (chosen) for (int j = 0; j < 4; ++j) chosen[j] = k[j];
+  return cuda_check(cudaStreamSynchronize(c->stream), "autotune reset");
 }
 
 piks_status piks_get_precision(piks_ctx *c, int32_t *precision) {

@@ -138,3 +138,24 @@ def test_tutorial_case_trace_matches_golden():
         m, k, e = s.chk_converge()
         assert (repr(m), repr(k), repr(e)) == (mass, perm, err), step
     s.close()
+
+
+def test_autotune_then_bit_exact():
+    """The autotuner's trial sweeps leave no trace: after it, iterations equal the oracle's."""
+    img = images.sphere_pack(10, 0.55, 1.2, 2.5, seed=4)
+    p = base_params(10, Nc_fundamental=4, Kn=0.3, pressDrop=0.1)
+    o = Oracle(p, img.tobytes(), nthreads=4)
+    s = pk.Solver(p, device=0)
+    s.setup_physical_grid(img)
+    cands = [(8, 4, 4, pk.SCHED_TILE_DIAGONALS), (4, 4, 4, pk.SCHED_TILE_DATAFLOW), (2, 3, 2, pk.SCHED_TILE_DIAGONALS)]
+    chosen, ms = s.autotune(cands, sweeps=2)
+    assert chosen in cands and all(m > 0 for m in ms)
+    sch = s.schedule()
+    assert (sch["TX"], sch["TY"], sch["TZ"], sch["launch"]) == chosen
+    nodes = s.geometry_array("node_g")
+    for _ in range(3):
+        o.iterate(1)
+        s.iterate(1)
+    _compare_state(o, s, nodes)
+    assert o.chk_converge() == s.chk_converge()
+    s.close()
