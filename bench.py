@@ -1,17 +1,22 @@
 #!/usr/bin/env python
 """Benchmark of the B200 source-iteration solver (one JSON line on rank 0).
 
-Workload (N = 1, per rank): the 128^3 Boolean sphere pack (porosity 0.40, radii uniform
-in 4-8 voxels, seed 12345) with two fluid layers at inlet and outlet (fluidlayer = 2: with
-walls next to the periodic inlet/outlet planes the scheme's second-order wall
-extrapolation diverges), 512 discrete velocities (Nc_fundamental = 4, half-range
-Gauss-Hermite), Kn = 0.5, plain FP64 solve (--precision fp32: FP32 sweep). A step is one source iteration (8 octant
-sweeps, halo, wall, inlet/outlet and symmetry boundary conditions, moments). The metric
-is fluid voxel-velocity updates per second (N_fluid * Nv per iteration), whole job.
+Workload (per rank): the 128^3 Boolean sphere pack (porosity 0.40, radii uniform in 4-8
+voxels, seed 12345), 512 discrete velocities (Nc_fundamental = 4, half-range Gauss-Hermite),
+Kn = 0.5, first-order wall extrapolation (wallExtOrder = 1, as in the reference's shipped
+tutorials: with second-order extrapolation the scheme diverges on packs with one-voxel
+channels). A step is one source iteration (8 octant sweeps, halo, walls, inlet/outlet,
+symmetry, moments).
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+value: fluid voxel-velocity updates per second of the refined solver's iteration (FP32
+sweep, FP64 moments / wall densities / flux), whole job; the same for the plain FP64
+iteration is in "fp64". "solve": both solvers run to convergence at a 1e-4 permeability
+tolerance (solves/s, iterations, permeability difference, velocity-field difference);
+"e2e" is the refined solve through the public API, image upload to field download.
 
---impl reference times the CPU restatement of PIKS3D's own OpenMP solver (oracle/,
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--no-solve]
+
+--impl reference times the CPU restatement of PIKS3D's own OpenMP solver (oracle/;
 the reference itself is Fortran + MPI and cannot be built here) on the same workload
 with all host threads, on rank 0 only. Under torchrun with N > 1 every rank solves its
 own copy of the workload (independent solves, no collective on the data path) and the
@@ -28,9 +33,10 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-WORKLOAD = dict(n=128, porosity=0.40, rmin=4.0, rmax=8.0, seed=12345, Nc_fundamental=4, Kn=0.5, fluidlayer=2)
-METRIC = "fluid voxel-velocity updates/s (plain FP64 source iteration)"
+WORKLOAD = dict(n=128, porosity=0.40, rmin=4.0, rmax=8.0, seed=12345, Nc_fundamental=4, Kn=0.5, wallExtOrder=1)
+METRIC = "solves/s + p99 latency vs plain FP64 GPU at 1e-4 perm error; Gvoxel-vel upd/s"
 UNIT = "Gupd/s"
+TOL = 1e-4
 
 
 def workload_image():
@@ -42,14 +48,14 @@ def workload_image():
 def workload_params(pk):
     w = WORKLOAD
     return pk.default_params(Nx=w["n"], Ny=w["n"], Nz=w["n"], Nc_fundamental=w["Nc_fundamental"],
-                             Kn=w["Kn"], pressDrop=1.0, eps=1e-8, chkConvergeStep=10, maxStep=100000,
-                             fluidlayer=w["fluidlayer"])
+                             Kn=w["Kn"], pressDrop=1.0, eps=1e-8, chkConvergeStep=10, maxStep=20000,
+                             wallExtOrder=w["wallExtOrder"])
 
 
 def config_dict(extra=None):
     w = WORKLOAD
-    d = {"workload": "sphere-pack %d^3 porosity %.2f radii %g-%g seed %d, fluidlayer %d, Nv=%d, Kn=%g" % (
-        w["n"], w["porosity"], w["rmin"], w["rmax"], w["seed"], w["fluidlayer"], 8 * w["Nc_fundamental"] ** 3, w["Kn"]),
+    d = {"workload": "sphere-pack %d^3 porosity %.2f radii %g-%g seed %d, Nv=%d, Kn=%g, wallExtOrder %d" % (
+        w["n"], w["porosity"], w["rmin"], w["rmax"], w["seed"], 8 * w["Nc_fundamental"] ** 3, w["Kn"], w["wallExtOrder"]),
          "image": "%dx%dx%d uint8" % (w["n"], w["n"], w["n"]), "velocities": 8 * w["Nc_fundamental"] ** 3,
          "Kn": w["Kn"], "l2": "inputs larger than L2 (distribution function > 4 GB per rank)"}
     if extra:
@@ -74,7 +80,7 @@ class ClockSampler:
             os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.QUERY,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=self.fh, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -177,30 +183,9 @@ def run_reference(args, world, rank):
     return 0
 
 
-def run_ours(args, world, rank, local):
-    import torch
-    import piks3d_b200 as pk
-
-    torch.cuda.set_device(local)
-    device = torch.device("cuda", local)
-    img = workload_image()
-    p = workload_params(pk)
-
-    # --- device-resident run: value, roofline ---------------------------------------------
-    prec = pk.PREC_FP32 if args.precision == "fp32" else pk.PREC_FP64
-    esz = 4 if prec == pk.PREC_FP32 else 8
-    s = pk.Solver(p, device=local)
-    s.set_precision(prec)
-    s.setup_physical_grid(img)
-    info = s.info()
-    stream = torch.cuda.Stream(device=device)
-    s.set_stream(stream.cuda_stream)
-    nf, nc8 = info["Nfluid"], info["Nc8"]
-    nv = 8 * nc8
-    sw = s.geometry_array("node_g")  # noqa: F841 (keeps the call path warm)
-    # swept updates per iteration: fluid nodes outside each octant's inflow planes
-    lab = s.get_labels()
-    fluid = lab == 0
+def swept_updates(s):
+    """Swept (node, octant) pairs per iteration: fluid nodes outside each octant's inflow planes."""
+    fluid = s.get_labels() == 0
     swept = 0
     for sx in (1, -1):
         for sy in (1, -1):
@@ -209,82 +194,143 @@ def run_ours(args, world, rank, local):
                 f = f[:, 1:, :] if sy > 0 else f[:, :-1, :]
                 f = f[:, :, 1:] if sx > 0 else f[:, :, :-1]
                 swept += int(f.sum())
-    sweep_bytes = 2 * esz * nc8 * swept + 32 * nf     # h read + write per swept update, moments read once
-    iter_bytes = 2 * esz * nv * (nf + info["nWall"]) + 2 * 32 * nf
+    return swept
 
+
+def measure_iterations(pk, p, img, prec, args, world, local, device, clocks=None):
+    """K timed iterations (after W warm-up) of one precision with CUDA events on the
+    launching stream; per-kernel times from the library's own events."""
+    import torch
+    s = pk.Solver(p, device=local)
+    s.set_precision(prec)
+    s.setup_physical_grid(img)
+    info = s.info()
+    stream = torch.cuda.Stream(device=device)
+    s.set_stream(stream.cuda_stream)
+    esz = 4 if prec == pk.PREC_FP32 else 8
+    nf, nc8 = info["Nfluid"], info["Nc8"]
+    swept = swept_updates(s)
+    sweep_bytes = 2 * esz * nc8 * swept + 32 * nf     # f read + write per swept update, moments read once
     s.iterate(args.warmup)
     s.synchronize()
     s.enable_timing(True)
     s.kernel_times(reset=True)
-    clocks = ClockSampler(local)
     barrier(world, device)
     torch.cuda.synchronize()
-    clocks.start()
+    if clocks:
+        clocks.start()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     s.iterate(args.steps)
     ev1.record(stream)
     torch.cuda.synchronize()
-    clk = clocks.stop()
+    clk = clocks.stop() if clocks else None
     ms_local = ev0.elapsed_time(ev1)
     kt = s.kernel_times(reset=True)
     s.enable_timing(False)
     launches = s.launches_per_iteration() * args.steps
+    sched = s.schedule()
     s.close()
     ms = reduce_max(ms_local, world, device)
-    barrier(world, device)
+    sweep_ms = kt["sweep"][0] / max(1, kt["sweep"][1])
+    return {"info": info, "ms": ms, "kt": kt, "launches": launches, "clocks": clk, "swept": swept,
+            "sweep_bytes": sweep_bytes, "sweep_ms": sweep_ms, "schedule": sched,
+            "gupd": nf * 8 * nc8 * args.steps * world / (ms * 1e-3) / 1e9}
 
-    # --- end to end through the C ABI with host buffers ---------------------------------------
-    box = info["Nx"] * info["Ny"] * info["Nz"]
-    torch.cuda.synchronize()
-    barrier(world, device)
-    t0 = time.perf_counter()
-    s2 = pk.Solver(p, device=local)
-    s2.set_precision(prec)
-    s2.setup_physical_grid(img)                 # H2D: image -> geometry tables + zeroed state
-    s2.iterate(args.steps)
-    mass, perm, err = s2.chk_converge()          # D2H: mass flux
-    rho, ux, uy, uz = s2.get_macro()             # D2H: fields
-    s2.close()
-    e2e_local = time.perf_counter() - t0
-    e2e_s = reduce_max(e2e_local, world, device)
+
+def traffic_per_update(precision):
+    """DRAM bytes per swept voxel-velocity update of the sweep kernel, from the committed
+    summary of an ncu capture (profiles/), or None."""
+    try:
+        d = json.load(open(os.path.join(ROOT, "profiles", "tile_sweep_traffic.json")))
+        return d[precision]["dram_bytes_per_swept_update"]
+    except Exception:
+        return None
+
+
+def run_ours(args, world, rank, local):
+    import numpy as np
+    import torch
+    import piks3d_b200 as pk
+    from piks3d_b200.solve import solve_one
+
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    img = workload_image()
+    p = workload_params(pk)
+
+    # --- device-resident iterations: value (refined solver's FP32 iteration), fp64, roofline
+    clocks = ClockSampler(local)
+    m32 = measure_iterations(pk, p, img, pk.PREC_FP32, args, world, local, device, clocks)
+    m64 = measure_iterations(pk, p, img, pk.PREC_FP64, args, world, local, device)
+    info = m32["info"]
+    nf, nc8 = info["Nfluid"], info["Nc8"]
+    nv = 8 * nc8
+
+    # --- full solves through the public API (image upload to field download) ------------------
+    solve = None
+    e2e = None
+    if not args.no_solve:
+        torch.cuda.synchronize()
+        barrier(world, device)
+        t0 = time.perf_counter()
+        r64 = solve_one(img, p, device=local, precision="fp64", tol=TOL, keep_fields=True)
+        t64 = reduce_max(time.perf_counter() - t0, world, device)
+        barrier(world, device)
+        t0 = time.perf_counter()
+        rrf = solve_one(img, p, device=local, precision="refined", tol=TOL, keep_fields=True)
+        trf = reduce_max(time.perf_counter() - t0, world, device)
+        u64, urf = r64.pop("macro"), rrf.pop("macro")
+        num = sum(float(np.sum((a - b) ** 2)) for a, b in zip(urf[1:], u64[1:]))
+        den = sum(float(np.sum(b ** 2)) for b in u64[1:])
+        solve = {
+            "tolerance": TOL, "rule": "estimated distance of k to the iteration's limit <= tol/2, two checks in a row",
+            "fp64": {**r64, "seconds": t64, "solves_per_s": world / t64},
+            "refined": {**rrf, "seconds": trf, "solves_per_s": world / trf},
+            "speedup_solves_per_s": t64 / trf,
+            "perm_rel_diff_refined_vs_fp64": abs(rrf["permeability"] - r64["permeability"]) / abs(r64["permeability"]),
+            "velocity_rel_l2_diff_refined_vs_fp64": (num / den) ** 0.5,
+        }
+        box = info["Nx"] * info["Ny"] * info["Nz"]
+        steps = rrf["steps"]
+        e2e = {"value": nf * nv * steps * world / trf / 1e9, "unit": UNIT,
+               "h2d_bytes_per_step": img.nbytes / steps,
+               "d2h_bytes_per_step": (8 * steps / p.chkConvergeStep + 4 * box * 8) / steps, "seconds": trf,
+               "what": "refined solve through the public API: create + setup_physical_grid(host image) + "
+                       "%d iterations with a check every %d + get_macro, wall clock" % (steps, p.chkConvergeStep)}
 
     if rank != 0:
         return 0
-    upd = nf * nv * args.steps * world
-    value = upd / (ms * 1e-3) / 1e9
-    sweep_ms, sweep_groups = kt["sweep"]
-    per_iter_sweep_ms = sweep_ms / max(1, sweep_groups)
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except Exception:
         pass
     hbm = peaks.get("hbm_gbs", 6650.0)
-    achieved = sweep_bytes / (per_iter_sweep_ms * 1e-3) / 1e9
-    h2d = img.nbytes
-    d2h = 4 * box * 8 + 8
+    achieved = m32["sweep_bytes"] / (m32["sweep_ms"] * 1e-3) / 1e9
+    tpu = traffic_per_update("fp32")
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64" if esz == 8 else "f32 (moments, wall densities, flux f64)",
+        "metric": METRIC, "value": m32["gupd"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": m32["ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 sweep; f64 moments, wall densities, flux, convergence test",
         "data": "synthetic",
         "config": config_dict({"Nfluid": nf, "nWall": info["nWall"], "parallelism": "replicas x%d" % world,
-                               "precision": args.precision}),
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": None,
-                     "kernel": "k_sweep (all tile-diagonal launches of one iteration)",
-                     "alg_bytes_per_iteration": sweep_bytes,
-                     "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650"},
-        "iteration_bandwidth_gbs": iter_bytes / (ms / args.steps * 1e-3) / 1e9,
-        "kernel_ms_per_iteration": {k: v[0] / max(1, args.steps) for k, v in kt.items()},
-        "e2e": {"value": upd / e2e_s / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,
-                "d2h_bytes_per_step": d2h / args.steps, "seconds": e2e_s,
-                "what": "create + setup_physical_grid(host image) + %d iterations + chk_converge + get_macro, wall clock" % args.steps},
-        "gpu_launches": launches,
-        "clocks": clk,
-        "permeability_after_steps": perm,
+                               "schedule": m32["schedule"]}),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": (tpu * m32["swept"] * nc8) if tpu else None,
+                     "kernel": "k_tile_sweep<float> (all launches of one iteration's sweep)",
+                     "alg_bytes_per_iteration": m32["sweep_bytes"],
+                     "peak_source": ("MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks
+                                     else "fallback 6650 (of fallback)")},
+        "kernel_ms_per_iteration": {k: v[0] / max(1, args.steps) for k, v in m32["kt"].items()},
+        "fp64": {"value": m64["gupd"], "unit": UNIT, "ms_per_step": m64["ms"] / args.steps,
+                 "kernel_ms_per_iteration": {k: v[0] / max(1, args.steps) for k, v in m64["kt"].items()},
+                 "sweep_frac_of_hbm": m64["sweep_bytes"] / (m64["sweep_ms"] * 1e-3) / 1e9 / hbm},
+        "solve": solve,
+        "e2e": e2e,
+        "gpu_launches": m32["launches"],
+        "clocks": m32["clocks"],
     }
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(p, img, args.cpu_iters)
@@ -295,13 +341,12 @@ def run_ours(args, world, rank, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-iters", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],
-                    help="fp32: FP32 f and sweep, FP64 moments / wall densities / flux")
+    ap.add_argument("--no-solve", action="store_true", help="skip the full solves (solve / e2e blocks)")
     ap.add_argument("--n", type=int, default=None,
                     help="image edge (default 128); smaller edges are for profiling captures, not bench lines")
     args = ap.parse_args()

@@ -9,8 +9,9 @@ permeability to the limit of the iteration is estimated as d_k * r / (1 - r) (ge
 tail, as in Aitken's extrapolation); see Convergence for the exact rule.
 
 Precision: a "refined" solve runs the FP32 sweep (FP64 moments, wall densities, flux and
-convergence test) until it meets the stopping rule or stops improving, then widens its
-state to FP64 on the device and continues in FP64 until the rule holds in FP64.
+convergence test) until it meets the stopping rule, or its mass flux changes by less than
+`switch_change` (relative) per check twice in a row, or its error stops improving; it then
+widens its state to FP64 on the device and continues in FP64 until the rule holds there.
 """
 import concurrent.futures as cf
 import math
@@ -24,22 +25,32 @@ from . import Batch, PREC_FP32, PREC_FP64, Solver
 class Convergence:
     """Per-solve stopping rule over the sequence of chkConverge results.
 
-    With `tol` set: after at least `min_checks` checks, r is the largest of the last three
-    ratios d_k / d_(k-1) of successive relative mass-flux changes; when all three are below
-    1 the remaining relative distance to the limit is estimated as d_k * r / (1 - r), and
-    the solve stops once the estimate is below safety * tol at `consec` checks in a row.
-    (Early transients of the source iteration can show a few shrinking changes before the
-    slow mode takes over; requiring three contracting ratios and three passing checks is
-    what keeps the rule from stopping there.)"""
+    With `tol` set: d_i is the relative change of the mass flux between consecutive checks.
+    Over the last `window` values a straight line is fitted to log d_i; its slope gives the
+    contraction per check r, and the remaining relative distance of the permeability to the
+    limit of the iteration is estimated as d * r / (1 - r), with d the fitted last change.
+    The solve stops once that estimate is below safety * tol at `consec` checks in a row,
+    provided r < 1 and the points lie close to the line (residual below `maxres` in log).
+    Fitting over several checks, rather than taking one ratio of two changes, keeps the rule
+    from being fooled by the early transient of the source iteration or by rounding noise
+    in the FP32 phase of a refined solve."""
 
-    def __init__(self, eps=1e-8, tol=None, stall_checks=5, min_checks=5, consec=3, safety=0.5):
+    def __init__(self, eps=1e-8, tol=None, stall_checks=5, window=6, min_checks=8, consec=2, safety=0.5,
+                 maxres=0.35):
         self.eps, self.tol, self.stall_checks = eps, tol, stall_checks
-        self.min_checks, self.consec, self.safety = min_checks, consec, safety
+        self.window, self.min_checks, self.consec, self.safety, self.maxres = window, min_checks, consec, safety, maxres
         self.masses = []
         self.best = math.inf
         self.since_best = 0
         self.estimate = math.inf     # estimated relative distance of the permeability to its limit
         self._ok_run = 0
+        self._small_run = 0
+
+    def last_change(self):
+        """Relative change of the mass flux between the last two checks."""
+        if len(self.masses) < 2:
+            return math.inf
+        return abs(self.masses[-1] - self.masses[-2]) / max(abs(self.masses[-1]), 1e-300)
 
     def update(self, mass, error):
         """Records one check; returns True when the solve has converged."""
@@ -50,18 +61,29 @@ class Convergence:
             self.since_best += 1
         if self.tol is None:
             return error <= self.eps
-        if len(self.masses) < max(5, self.min_checks):
+        w = self.window
+        if len(self.masses) < max(w + 1, self.min_checks):
             return False
         m = self.masses
-        d = [abs(m[-1 - i] - m[-2 - i]) / max(abs(m[-1 - i]), 1e-300) for i in range(4)]
-        if d[0] == 0.0:
+        d = np.array([abs(m[-w + i] - m[-w + i - 1]) / max(abs(m[-w + i]), 1e-300) for i in range(w)])
+        if d[-1] == 0.0:
             self.estimate = 0.0
+        elif np.any(d <= 0.0):
+            self.estimate = math.inf
         else:
-            rs = [d[i] / d[i + 1] if d[i + 1] > 0.0 else math.inf for i in range(3)]
-            r = max(rs)
-            self.estimate = d[0] * r / (1.0 - r) if r < 1.0 else math.inf
+            x = np.arange(w, dtype=np.float64)
+            y = np.log(d)
+            b, a = np.polyfit(x, y, 1)
+            res = float(np.std(y - (a + b * x)))
+            r = math.exp(b)
+            self.estimate = math.exp(a + b * (w - 1)) * r / (1.0 - r) if (r < 1.0 and res <= self.maxres) else math.inf
         self._ok_run = self._ok_run + 1 if self.estimate <= self.safety * self.tol else 0
         return self._ok_run >= self.consec
+
+    def small_changes(self, threshold, checks=2):
+        """True once the last `checks` relative changes were all at most `threshold`."""
+        self._small_run = self._small_run + 1 if self.last_change() <= threshold else 0
+        return self._small_run >= checks
 
     def stalled(self):
         return self.since_best >= self.stall_checks
@@ -117,11 +139,12 @@ class BatchRunner:
     chkConvergeStep iterations, switched from FP32 to FP64 when their FP32 phase ends, and
     retired (state freed) as soon as they converge."""
 
-    def __init__(self, device=0, precision="refined", tol=1e-4, eps=None, switch_eps=1e-6, max_members=64,
-                 hbm_budget=None, prep_threads=4, keep_fields=False):
+    def __init__(self, device=0, precision="refined", tol=1e-4, eps=None, switch_eps=1e-6, switch_change=1e-6,
+                 max_members=64, hbm_budget=None, prep_threads=4, keep_fields=False):
         import torch  # noqa: F401  (device memory query only)
         self.device, self.precision, self.tol, self.eps = device, precision, tol, eps
         self.switch_eps, self.max_members, self.keep_fields = switch_eps, max_members, keep_fields
+        self.switch_change = switch_change
         if hbm_budget is None:
             import torch
             free, _total = torch.cuda.mem_get_info(device)
@@ -195,7 +218,8 @@ class BatchRunner:
             if job.phase == "fp32":
                 job.steps32 += chk
             conv = job.conv.update(mass[i], err[i])
-            if job.phase == "fp32" and self.precision == "refined" and (conv or job.conv.stalled()):
+            small = job.conv.small_changes(self.switch_change)
+            if job.phase == "fp32" and self.precision == "refined" and (conv or small or job.conv.stalled()):
                 # the FP64 phase continues from the widened FP32 iterate
                 job.solver.set_precision(PREC_FP64)
                 job.phase = "fp64"
@@ -231,8 +255,8 @@ class BatchRunner:
         return finished
 
 
-def solve_one(image, params, device=0, precision="fp64", tol=None, eps=None, switch_eps=1e-6, tiles=None,
-              keep_fields=False):
+def solve_one(image, params, device=0, precision="fp64", tol=None, eps=None, switch_eps=1e-6, switch_change=1e-6,
+              tiles=None, keep_fields=False):
     """One solve through a context of its own (no batch): the reference's loop with the same
     stopping rule as the batch runner. Returns a result dict."""
     s = Solver(params, device=device)
@@ -253,7 +277,8 @@ def solve_one(image, params, device=0, precision="fp64", tol=None, eps=None, swi
             steps32 += chk
         m, k, e = s.chk_converge()
         ok = conv.update(m, e)
-        if phase == "fp32" and precision == "refined" and (ok or conv.stalled()):
+        small = conv.small_changes(switch_change)
+        if phase == "fp32" and precision == "refined" and (ok or small or conv.stalled()):
             s.set_precision(PREC_FP64)
             phase = "fp64"
             conv = Convergence(eps=base_eps, tol=tol)

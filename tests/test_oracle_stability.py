@@ -3,10 +3,11 @@
 With second-order wall extrapolation (wallExtOrder = 2, the default), a wall one voxel
 away from the inlet or outlet plane (x = 2 with fluid at x = 1, or x = Nx - 1 with fluid at
 x = Nx) extrapolates its incoming distribution through the periodic ghost plane, and the
-source iteration diverges (mass flux and permeability grow without bound). The reference
-avoids it in its own tutorials with wallExtOrder = 1; two fluid layers at inlet and outlet
-(fluidlayer = 2) keep every such wall away from the ghost planes. The benchmark workloads
-use fluidlayer = 2 for that reason.
+source iteration diverges (mass flux and permeability grow without bound). Two fluid layers
+at inlet and outlet (fluidlayer = 2) keep every such wall away from the ghost planes, but on
+larger packs walls facing each other across one-voxel channels extrapolate from each
+other's re-emitted values with gain 2 and diverge as well. The reference's shipped
+tutorials use wallExtOrder = 1, and so do the benchmark workloads.
 """
 import numpy as np
 import pytest
