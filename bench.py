@@ -338,6 +338,101 @@ def run_ours(args, world, rank, local):
     return 0
 
 
+def batch_jobs(pk, count, seed, max_step):
+    """The batching workload: seeded sphere packs, edges from {32, 48, 64, 80, 96}, porosity
+    U[0.3, 0.6], Kn log-uniform in [0.01, 10], 64 or 512 velocities per sample."""
+    import numpy as np
+    from piks3d_b200 import images
+    from piks3d_b200.solve import Job
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for i in range(count):
+        n = int(rng.choice([32, 48, 64, 80, 96]))
+        por = float(rng.uniform(0.3, 0.6))
+        kn = float(np.exp(rng.uniform(np.log(0.01), np.log(10.0))))
+        ncf = int(rng.choice([2, 4]))
+        img = images.sphere_pack(n, por, 4.0, 8.0, seed=seed * 1000 + i)
+        p = pk.default_params(Nx=n, Ny=n, Nz=n, Nc_fundamental=ncf, Kn=kn, pressDrop=1.0, wallExtOrder=1,
+                              maxStep=max_step, chkConvergeStep=10, eps=1e-8)
+        jobs.append(Job(img, p, name="img%d" % i))
+    return jobs
+
+
+def run_batch_workload(args, world, rank, local):
+    """Many images: plain FP64 solves one after another vs the refined solver's batch runner,
+    both to the 1e-4 permeability tolerance; solves/s of each and the permeability
+    differences per image."""
+    import numpy as np
+    import torch
+    import piks3d_b200 as pk
+    from piks3d_b200.solve import BatchRunner, solve_one
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    jobs = batch_jobs(pk, args.images, args.seed + rank, args.max_step)
+    barrier(world, device)
+    t0 = time.perf_counter()
+    plain = [solve_one(j.image, j.params, device=local, precision="fp64", tol=TOL) for j in jobs]
+    t_plain = reduce_max(time.perf_counter() - t0, world, device)
+    runner = BatchRunner(device=local, precision="refined", tol=TOL, max_members=args.images)
+    barrier(world, device)
+    t0 = time.perf_counter()
+    done = runner.run(batch_jobs(pk, args.images, args.seed + rank, args.max_step))
+    t_batch = reduce_max(time.perf_counter() - t0, world, device)
+    runner.close()
+    if rank != 0:
+        return 0
+    by = {j.name: j.result for j in done}
+    diffs = [abs(by[j.name]["permeability"] - p["permeability"]) / abs(p["permeability"]) for j, p in zip(jobs, plain)]
+    steps_plain = sum(p["steps"] for p in plain)
+    line = {
+        "metric": METRIC, "workload": "batch", "value": args.images * world / t_batch, "unit": "solves/s",
+        "n_gpus": world, "higher_is_better": True, "scaling": "weak", "data": "synthetic",
+        "config": {"workload": "%d seeded sphere packs, edges {32..96}, porosity U[0.3,0.6], Kn log-U[0.01,10], "
+                               "64 or 512 velocities, wallExtOrder 1, tolerance %g on k" % (args.images, TOL)},
+        "plain_fp64_sequential": {"seconds": t_plain, "solves_per_s": args.images * world / t_plain,
+                                  "iterations": steps_plain,
+                                  "converged": sum(1 for p in plain if p["converged"])},
+        "refined_batched": {"seconds": t_batch, "solves_per_s": args.images * world / t_batch,
+                            "iterations": sum(r["steps"] for r in by.values()),
+                            "fp32_iterations": sum(r["steps32"] for r in by.values()),
+                            "converged": sum(1 for r in by.values() if r["converged"])},
+        "speedup_solves_per_s": t_plain / t_batch,
+        "perm_rel_diff_refined_vs_fp64": {"max": max(diffs), "median": float(np.median(diffs))},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def run_serve_workload(args, world, rank, local):
+    """The serving workload: a seeded Poisson request stream through the server."""
+    import torch
+    import piks3d_b200 as pk
+    from piks3d_b200.serve import Server, make_stream
+    from piks3d_b200.solve import BatchRunner
+    torch.cuda.set_device(local)
+
+    def params(n, kn):
+        return pk.default_params(Nx=n, Ny=n, Nz=n, Nc_fundamental=4, Kn=kn, pressDrop=1.0, wallExtOrder=1,
+                                 maxStep=args.max_step, chkConvergeStep=10, eps=1e-8)
+
+    jobs = make_stream(args.rate, args.duration, args.seed + rank, params,
+                       edge_range=(args.edge_min, args.edge_max))
+    runner = BatchRunner(device=local, precision="refined", tol=TOL, max_members=64)
+    rep = Server(runner, horizon=args.horizon).run(jobs)
+    runner.close()
+    if rank != 0:
+        return 0
+    rep.pop("jobs")
+    line = {"metric": METRIC, "workload": "serve", "value": rep["solves_per_s"], "unit": "solves/s",
+            "n_gpus": world, "higher_is_better": True, "data": "synthetic",
+            "config": {"workload": "Poisson %g req/s for %g s, sphere packs edges %d-%d, porosity U[0.25,0.6], "
+                                   "Kn log-U[0.01,10], 512 velocities, tolerance %g on k, horizon %g s" % (
+                                       args.rate, args.duration, args.edge_min, args.edge_max, TOL, args.horizon)},
+            **rep}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -347,6 +442,16 @@ def main():
     ap.add_argument("--cpu-iters", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-solve", action="store_true", help="skip the full solves (solve / e2e blocks)")
+    ap.add_argument("--workload", default="precision", choices=["precision", "batch", "serve"],
+                    help="precision: the 128^3 pack (default); batch: many images; serve: request stream")
+    ap.add_argument("--images", type=int, default=64)
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--max-step", type=int, default=20000)
+    ap.add_argument("--rate", type=float, default=20.0)
+    ap.add_argument("--duration", type=float, default=60.0)
+    ap.add_argument("--horizon", type=float, default=300.0)
+    ap.add_argument("--edge-min", type=int, default=48)
+    ap.add_argument("--edge-max", type=int, default=160)
     ap.add_argument("--n", type=int, default=None,
                     help="image edge (default 128); smaller edges are for profiling captures, not bench lines")
     args = ap.parse_args()
@@ -356,6 +461,10 @@ def main():
     try:
         if args.impl == "reference":
             rc = run_reference(args, world, rank)
+        elif args.workload == "batch":
+            rc = run_batch_workload(args, world, rank, local)
+        elif args.workload == "serve":
+            rc = run_serve_workload(args, world, rank, local)
         else:
             rc = run_ours(args, world, rank, local)
     finally:
