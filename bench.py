@@ -398,6 +398,11 @@ def run_batch_workload(args, world, rank, local):
                             "converged": sum(1 for r in by.values() if r["converged"])},
         "speedup_solves_per_s": t_plain / t_batch,
         "perm_rel_diff_refined_vs_fp64": {"max": max(diffs), "median": float(np.median(diffs))},
+        "images": [{"name": j.name, "n": int(j.image.shape[0]), "velocities": 8 * j.params.Nc_fundamental ** 3,
+                    "Kn": j.params.Kn, "porosity": float((j.image == 0).mean()),
+                    "fp64_steps": p["steps"], "fp64_k": p["permeability"],
+                    "refined_steps": by[j.name]["steps"], "refined_fp32_steps": by[j.name]["steps32"],
+                    "refined_k": by[j.name]["permeability"]} for j, p in zip(jobs, plain)],
     }
     print(json.dumps(line))
     return 0

@@ -9,9 +9,10 @@ permeability to the limit of the iteration is estimated as d_k * r / (1 - r) (ge
 tail, as in Aitken's extrapolation); see Convergence for the exact rule.
 
 Precision: a "refined" solve runs the FP32 sweep (FP64 moments, wall densities, flux and
-convergence test) until it meets the stopping rule, or its mass flux changes by less than
-`switch_change` (relative) per check twice in a row, or its error stops improving; it then
-widens its state to FP64 on the device and continues in FP64 until the rule holds there.
+convergence test) until it meets the stopping rule or its mass flux changes by less than
+`switch_change` (relative) per check twice in a row (the FP32 iterate then sits near its
+rounding floor); it then widens its state to FP64 on the device and continues in FP64
+until the rule holds there.
 """
 import concurrent.futures as cf
 import math
@@ -219,7 +220,7 @@ class BatchRunner:
                 job.steps32 += chk
             conv = job.conv.update(mass[i], err[i])
             small = job.conv.small_changes(self.switch_change)
-            if job.phase == "fp32" and self.precision == "refined" and (conv or small or job.conv.stalled()):
+            if job.phase == "fp32" and self.precision == "refined" and (conv or small):
                 # the FP64 phase continues from the widened FP32 iterate
                 job.solver.set_precision(PREC_FP64)
                 job.phase = "fp64"
@@ -278,7 +279,7 @@ def solve_one(image, params, device=0, precision="fp64", tol=None, eps=None, swi
         m, k, e = s.chk_converge()
         ok = conv.update(m, e)
         small = conv.small_changes(switch_change)
-        if phase == "fp32" and precision == "refined" and (ok or small or conv.stalled()):
+        if phase == "fp32" and precision == "refined" and (ok or small):
             s.set_precision(PREC_FP64)
             phase = "fp64"
             conv = Convergence(eps=base_eps, tol=tol)
