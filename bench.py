@@ -457,7 +457,7 @@ def main():
     ap.add_argument("--horizon", type=float, default=300.0)
     ap.add_argument("--edge-min", type=int, default=48)
     ap.add_argument("--edge-max", type=int, default=160)
-    ap.add_argument("--n", type=int, default=None,
+    ap.add_argument("--edge", "--n", dest="n", type=int, default=None,
                     help="image edge (default 128); smaller edges are for profiling captures, not bench lines")
     args = ap.parse_args()
     if args.n:
