@@ -112,8 +112,8 @@ __global__ void k_capture32(const DevState a, int buf) {
   a.ghostE32[buf][idx] = nE >= 0 ? a.h32[hidx(nE, oE, a.Nc8, l)] : 0.f;
 }
 
-// Walls: extrapolation and re-emission in FP32, the wall densities summed in FP64 (in the
-// reference's order over l) and the re-emitted value formed in FP64 before rounding.
+// Walls: extrapolation and re-emission in FP32, the wall densities summed in FP64 (a warp
+// reduction) and the re-emitted value formed in FP64 before rounding.
 template <int VPL>
 __global__ void __launch_bounds__(256) k_walls32(const DevState a, int begin, int end, int gbuf) {
   const int widx = begin + (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -169,12 +169,11 @@ __global__ void __launch_bounds__(256) k_walls32(const DevState a, int begin, in
         const double ca = !lv ? 0.0 : dir < 2 ? __ldg(a.cx + l) : dir < 4 ? __ldg(a.cy + l) : __ldg(a.cz + l);
         tface[v] = ca * (((double)ext[0][v] + (double)ext[1][v]) + (double)ext[2][v] + (double)ext[3][v]);
       }
-      const int nl = min(chunkw, Nc8 - l0);
-      for (int sidx = 0; sidx < nl; ++sidx) {
-        const int srcl = sidx / VPL, v = sidx % VPL;
-        racc += __shfl_sync(0xffffffffu, (VPL == 2 && v == 1) ? tface[VPL - 1] : tface[0], srcl);
-      }
+#pragma unroll
+      for (int v = 0; v < VPL; ++v) racc += tface[v];
     }
+    // warp sum in FP64 (the FP32 path does not keep the reference's summation order)
+    for (int off = 16; off > 0; off >>= 1) racc += __shfl_xor_sync(0xffffffffu, racc, off);
     if (fi == 0) rho0 = racc; else if (fi == 1) rho1 = racc; else rho2 = racc;
   }
   rho0 /= a.DiffFlux; rho1 /= a.DiffFlux; rho2 /= a.DiffFlux;

@@ -31,15 +31,20 @@ class Convergence:
     contraction per check r, and the remaining relative distance of the permeability to the
     limit of the iteration is estimated as d * r / (1 - r), with d the fitted last change.
     The solve stops once that estimate is below safety * tol at `consec` checks in a row,
-    provided r < 1 and the points lie close to the line (residual below `maxres` in log).
-    Fitting over several checks, rather than taking one ratio of two changes, keeps the rule
-    from being fooled by the early transient of the source iteration or by rounding noise
-    in the FP32 phase of a refined solve."""
+    provided r < 1 and the points lie close to the line (residual below `maxres` in log),
+    and the last `gate_run` changes were each at most gate * tol. Fitting over several
+    checks, rather than taking one ratio of two changes, keeps the rule from being fooled by
+    the early transient of the source iteration or by rounding noise in the FP32 phase of a
+    refined solve; the gate on the size of the changes keeps it from stopping where a fast
+    mode and a slow mode of opposite sign cancel for a few checks (the mass flux passing
+    through a turning point looks converged there)."""
 
     def __init__(self, eps=1e-8, tol=None, stall_checks=5, window=6, min_checks=8, consec=2, safety=0.5,
-                 maxres=0.35):
+                 maxres=0.35, gate=0.02, gate_run=3):
         self.eps, self.tol, self.stall_checks = eps, tol, stall_checks
         self.window, self.min_checks, self.consec, self.safety, self.maxres = window, min_checks, consec, safety, maxres
+        self.gate, self.gate_run = gate, gate_run
+        self._gate_ok = 0
         self.masses = []
         self.best = math.inf
         self.since_best = 0
@@ -79,7 +84,8 @@ class Convergence:
             r = math.exp(b)
             self.estimate = math.exp(a + b * (w - 1)) * r / (1.0 - r) if (r < 1.0 and res <= self.maxres) else math.inf
         self._ok_run = self._ok_run + 1 if self.estimate <= self.safety * self.tol else 0
-        return self._ok_run >= self.consec
+        self._gate_ok = self._gate_ok + 1 if self.last_change() <= self.gate * self.tol else 0
+        return self._ok_run >= self.consec and self._gate_ok >= self.gate_run
 
     def small_changes(self, threshold, checks=2):
         """True once the last `checks` relative changes were all at most `threshold`."""
