@@ -23,7 +23,10 @@ namespace piks {
 namespace {
 
 constexpr int kFwBit = 1 << 30;
-constexpr int kGroups = 16;  // task groups per CTA
+// Task groups per CTA (tasks of one local hyperplane in flight): 16 for FP64, 8 for FP32,
+// whose groups have twice the lanes (V = 32 velocities); both measured fastest on B200.
+template <typename T> constexpr int groups_of() { return sizeof(T) == 8 ? 16 : 8; }
+template <typename T, int V> constexpr int threads_of() { return V / 2 * groups_of<T>(); }
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
@@ -64,8 +67,8 @@ template <typename T, int V>
 __device__ __forceinline__ void tile_job(const DevState &a, int job, int chunk, int slots_cap, int tasks_cap,
                                          unsigned char *smem_raw) {
   constexpr int LPT = V / 2;                        // lanes per task
-  constexpr int THREADS = LPT * kGroups;
-  constexpr int GROUPS = kGroups;                   // tasks in flight per pass
+  constexpr int THREADS = LPT * groups_of<T>();
+  constexpr int GROUPS = groups_of<T>();            // tasks in flight per pass
   constexpr int EPP = 16 / (int)sizeof(T);          // elements per 16-byte piece
   constexpr int PIECES = V / EPP;                   // pieces per row
   using T2 = typename Pair<T>::type;
@@ -230,7 +233,7 @@ __device__ __forceinline__ void tile_job(const DevState &a, int job, int chunk, 
 }
 
 template <typename T, int V>
-__global__ void __launch_bounds__(V / 2 * kGroups)
+__global__ void __launch_bounds__(threads_of<T, V>())
 k_tile_sweep(const DevState a, int job0, int slots_cap, int tasks_cap) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int nchunk = a.Nc8 / V;
@@ -279,7 +282,7 @@ __device__ bool wait_flag(const int *flag, int epoch, int *err) {
 // claimed in an order in which every upstream item comes first, by CTAs that are running,
 // so the earliest unfinished claimed item can always proceed.
 template <typename T, int V>
-__global__ void __launch_bounds__(V / 2 * kGroups)
+__global__ void __launch_bounds__(threads_of<T, V>())
 k_tile_sweep_dataflow(const DevState a, int epoch, int slots_cap, int tasks_cap) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int item_s, skip_s;
@@ -311,7 +314,7 @@ k_tile_sweep_dataflow(const DevState a, int epoch, int slots_cap, int tasks_cap)
 // item's upstream items (same member, same chunk) come first. A member's flags are cleared
 // before the launch and hold 1 once an item is done.
 template <typename T, int V>
-__global__ void __launch_bounds__(V / 2 * kGroups)
+__global__ void __launch_bounds__(threads_of<T, V>())
 k_tile_sweep_batch(const DevState *states, const int2 *items, int nitems, int slots_cap, int tasks_cap, int *counter,
                    int *err) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -352,13 +355,13 @@ void launch_batch(const DevState *states, const int2 *items, int nitems, int slo
   }
   const size_t smem = tile_smem_bytes(slots, tasks, stride, V * (int)sizeof(T));
   int nb = 1, nsm = 148;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_tile_sweep_batch<T, V>, V / 2 * kGroups, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_tile_sweep_batch<T, V>, threads_of<T, V>(), smem);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   long grid = (long)(nb < 1 ? 1 : nb) * nsm;
   if (grid > nitems) grid = nitems;
   if (grid < 1) return;
   cudaMemsetAsync(counter, 0, sizeof(int), st);
-  k_tile_sweep_batch<T, V><<<(unsigned)grid, V / 2 * kGroups, smem, st>>>(states, items, nitems, slots, tasks, counter,
+  k_tile_sweep_batch<T, V><<<(unsigned)grid, threads_of<T, V>(), smem, st>>>(states, items, nitems, slots, tasks, counter,
                                                                          err);
 }
 
@@ -378,7 +381,7 @@ void launch_dataflow(const DevState &s, int epoch, int slots, int tasks, cudaStr
   const size_t smem = tile_smem_bytes(slots, tasks, s.tv.steps_stride, V * (int)sizeof(T));
   if (per_sm_smem[dev] != smem) {
     int nb = 1, nsm = 148;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_tile_sweep_dataflow<T, V>, V / 2 * kGroups, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_tile_sweep_dataflow<T, V>, threads_of<T, V>(), smem);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     per_sm[dev][0] = nb < 1 ? 1 : nb;
     per_sm[dev][1] = nsm;
@@ -389,7 +392,7 @@ void launch_dataflow(const DevState &s, int epoch, int slots, int tasks, cudaStr
   if (grid > items) grid = items;
   if (grid < 1) return;
   cudaMemsetAsync(s.tv.counter, 0, sizeof(int), st);
-  k_tile_sweep_dataflow<T, V><<<(unsigned)grid, V / 2 * kGroups, smem, st>>>(s, epoch, slots, tasks);
+  k_tile_sweep_dataflow<T, V><<<(unsigned)grid, threads_of<T, V>(), smem, st>>>(s, epoch, slots, tasks);
 }
 
 template <typename T, int V>
@@ -403,7 +406,7 @@ void launch_one(const DevState &s, int job0, int njobs, int slots, int tasks, cu
   }
   const size_t smem = tile_smem_bytes(slots, tasks, s.tv.steps_stride, V * (int)sizeof(T));
   const unsigned grid = (unsigned)((size_t)njobs * (s.Nc8 / V));
-  k_tile_sweep<T, V><<<grid, V / 2 * kGroups, smem, st>>>(s, job0, slots, tasks);
+  k_tile_sweep<T, V><<<grid, threads_of<T, V>(), smem, st>>>(s, job0, slots, tasks);
 }
 
 }  // namespace
