@@ -271,33 +271,45 @@ __global__ void __launch_bounds__(256) k_walls(const DevState a, int begin, int 
     double aw[VPL];
 #pragma unroll
     for (int v = 0; v < VPL; ++v) aw[v] = dmul(a.accom, __ldg(a.w + lf + v));
-    for (int r = 0; r < P.nwr; ++r) {
-      const WWrite &W = P.wr[r];
-      const int so = W.src_o - 1, dso = W.dst_o - 1;
-      double src[VPL];
-      if (W.src_store == ST_F) ld_vpl<VPL>(a.h + hidx(node, so, Nc8, lf), src);
-      else if (W.src_store == ST_W) ld_vpl<VPL>(a.fw + hidx(corner, so, Nc8, lf), src);
-      else {
-        double n1v[VPL], farv[VPL];
-        ld_vpl<VPL>(a.h + hidx(nb[2 * zface], so, Nc8, lf), n1v);
-        const int code = nb[2 * zface + 1];
+    // re-emission in groups of four writes: the sources of a group are loaded before its
+    // stores (no write of a wall program reads a slot that an earlier write stores)
+    for (int r0 = 0; r0 < P.nwr; r0 += 4) {
+      double src[4][VPL];
 #pragma unroll
-        for (int v = 0; v < VPL; ++v) farv[v] = 0.0;
-        if (code >= 0) ld_vpl<VPL>(a.h + hidx(code, so, Nc8, lf), farv);
-        else if (code != -1) {
-          const int cc = -code - 2;
-          const double *plane = (cc & 1) ? a.ghostE[gbuf] : a.ghostW[gbuf];
-          ld_vpl<VPL>(plane + ((size_t)(cc >> 1) * 4 + plane_slot(so)) * Nc8 + lf, farv);
+      for (int k = 0; k < 4; ++k) {
+        if (r0 + k >= P.nwr) break;
+        const WWrite &W = P.wr[r0 + k];
+        const int so = W.src_o - 1;
+        if (W.src_store == ST_F) ld_vpl<VPL>(a.h + hidx(node, so, Nc8, lf), src[k]);
+        else if (W.src_store == ST_W) ld_vpl<VPL>(a.fw + hidx(corner, so, Nc8, lf), src[k]);
+        else {
+          double n1v[VPL], farv[VPL];
+          ld_vpl<VPL>(a.h + hidx(nb[2 * zface], so, Nc8, lf), n1v);
+          const int code = nb[2 * zface + 1];
+#pragma unroll
+          for (int v = 0; v < VPL; ++v) farv[v] = 0.0;
+          if (code >= 0) ld_vpl<VPL>(a.h + hidx(code, so, Nc8, lf), farv);
+          else if (code != -1) {
+            const int cc = -code - 2;
+            const double *plane = (cc & 1) ? a.ghostE[gbuf] : a.ghostW[gbuf];
+            ld_vpl<VPL>(plane + ((size_t)(cc >> 1) * 4 + plane_slot(so)) * Nc8 + lf, farv);
+          }
+#pragma unroll
+          for (int v = 0; v < VPL; ++v) src[k][v] = dadd(dmul(e1, n1v[v]), dmul(e2, farv[v]));
         }
-#pragma unroll
-        for (int v = 0; v < VPL; ++v) src[v] = dadd(dmul(e1, n1v[v]), dmul(e2, farv[v]));
       }
-      double val[VPL];
-      const double rf = W.face == 0 ? rho0 : W.face == 1 ? rho1 : rho2;
 #pragma unroll
-      for (int v = 0; v < VPL; ++v) val[v] = dadd(dmul(aw[v], rf), dmul(one_m, src[v]));
-      if (W.dst_store == ST_F) st_vpl<VPL>(a.h + hidx(node, dso, Nc8, lf), val);
-      else st_vpl<VPL>(a.fw + hidx(corner, dso, Nc8, lf), val);
+      for (int k = 0; k < 4; ++k) {
+        if (r0 + k >= P.nwr) break;
+        const WWrite &W = P.wr[r0 + k];
+        const int dso = W.dst_o - 1;
+        double val[VPL];
+        const double rf = W.face == 0 ? rho0 : W.face == 1 ? rho1 : rho2;
+#pragma unroll
+        for (int v = 0; v < VPL; ++v) val[v] = dadd(dmul(aw[v], rf), dmul(one_m, src[k][v]));
+        if (W.dst_store == ST_F) st_vpl<VPL>(a.h + hidx(node, dso, Nc8, lf), val);
+        else st_vpl<VPL>(a.fw + hidx(corner, dso, Nc8, lf), val);
+      }
     }
   }
 }

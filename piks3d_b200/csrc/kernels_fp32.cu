@@ -183,28 +183,41 @@ __global__ void __launch_bounds__(256) k_walls32(const DevState a, int begin, in
   for (int l0 = 0; l0 < Nc8; l0 += chunkw) {
     const int lf = l0 + lane * VPL;
     if (lf >= Nc8) continue;
-    for (int r = 0; r < P.nwr; ++r) {
-      const WWrite &W = P.wr[r];
-      const int so = W.src_o - 1, dso = W.dst_o - 1;
-      float src[VPL];
-      if (W.src_store == ST_F) ld32<VPL>(a.h32 + hidx(node, so, Nc8, lf), src);
-      else if (W.src_store == ST_W) ld32<VPL>(a.fw32 + hidx(corner, so, Nc8, lf), src);
-      else {
-        float nv[VPL], fv[VPL];
-        ld32<VPL>(a.h32 + hidx(nb[2 * zface], so, Nc8, lf), nv);
+    // re-emission in groups of four writes: the sources of a group are loaded before its
+    // stores (no write of a wall program reads a slot that an earlier write stores)
+    for (int r0 = 0; r0 < P.nwr; r0 += 4) {
+      float src[4][VPL];
 #pragma unroll
-        for (int v = 0; v < VPL; ++v) fv[v] = 0.f;
-        const float *fp = far_ptr(nb[2 * zface + 1], so, lf);
-        if (fp) ld32<VPL>(fp, fv);
+      for (int k = 0; k < 4; ++k) {
+        if (r0 + k >= P.nwr) break;
+        const WWrite &W = P.wr[r0 + k];
+        const int so = W.src_o - 1;
+        if (W.src_store == ST_F) ld32<VPL>(a.h32 + hidx(node, so, Nc8, lf), src[k]);
+        else if (W.src_store == ST_W) ld32<VPL>(a.fw32 + hidx(corner, so, Nc8, lf), src[k]);
+        else {
+          float nv[VPL], fv[VPL];
+          ld32<VPL>(a.h32 + hidx(nb[2 * zface], so, Nc8, lf), nv);
 #pragma unroll
-        for (int v = 0; v < VPL; ++v) src[v] = e1 * nv[v] + e2 * fv[v];
+          for (int v = 0; v < VPL; ++v) fv[v] = 0.f;
+          const float *fp = far_ptr(nb[2 * zface + 1], so, lf);
+          if (fp) ld32<VPL>(fp, fv);
+#pragma unroll
+          for (int v = 0; v < VPL; ++v) src[k][v] = e1 * nv[v] + e2 * fv[v];
+        }
       }
-      const double rf = W.face == 0 ? rho0 : W.face == 1 ? rho1 : rho2;
-      float val[VPL];
 #pragma unroll
-      for (int v = 0; v < VPL; ++v) val[v] = (float)(a.accom * __ldg(a.w + lf + v) * rf + one_m * (double)src[v]);
-      if (W.dst_store == ST_F) st32<VPL>(a.h32 + hidx(node, dso, Nc8, lf), val);
-      else st32<VPL>(a.fw32 + hidx(corner, dso, Nc8, lf), val);
+      for (int k = 0; k < 4; ++k) {
+        if (r0 + k >= P.nwr) break;
+        const WWrite &W = P.wr[r0 + k];
+        const int dso = W.dst_o - 1;
+        const double rf = W.face == 0 ? rho0 : W.face == 1 ? rho1 : rho2;
+        float val[VPL];
+#pragma unroll
+        for (int v = 0; v < VPL; ++v)
+          val[v] = (float)(a.accom * __ldg(a.w + lf + v) * rf + one_m * (double)src[k][v]);
+        if (W.dst_store == ST_F) st32<VPL>(a.h32 + hidx(node, dso, Nc8, lf), val);
+        else st32<VPL>(a.fw32 + hidx(corner, dso, Nc8, lf), val);
+      }
     }
   }
 }
@@ -236,6 +249,7 @@ __global__ void k_symmetry32(const DevState a) {
 
 // Moments in FP64 from FP32 values: a warp per node, lanes over velocities, partial sums
 // combined with a warp reduction (the FP32 path does not follow the reference's order).
+template <int VPL>
 __global__ void __launch_bounds__(256) k_moments32(const DevState a) {
   const int node = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   if (node >= a.NF) return;
@@ -243,14 +257,27 @@ __global__ void __launch_bounds__(256) k_moments32(const DevState a) {
   const int Nc8 = a.Nc8;
   const float *hp = a.h32 + (size_t)node * 8 * Nc8;
   double r = 0.0, ux = 0.0, uy = 0.0, uz = 0.0;
-  for (int l = lane; l < Nc8; l += 32) {
-    const double f1 = __ldcs(hp + 0 * Nc8 + l), f2 = __ldcs(hp + 1 * Nc8 + l), f3 = __ldcs(hp + 2 * Nc8 + l),
-                 f4 = __ldcs(hp + 3 * Nc8 + l), f5 = __ldcs(hp + 4 * Nc8 + l), f6 = __ldcs(hp + 5 * Nc8 + l),
-                 f7 = __ldcs(hp + 6 * Nc8 + l), f8 = __ldcs(hp + 7 * Nc8 + l);
-    r += ((f1 + f2) + (f3 + f4)) + ((f5 + f6) + (f7 + f8));
-    ux += __ldg(a.cx + l) * (((f1 - f2) + (f4 - f3)) + ((f5 - f6) + (f8 - f7)));
-    uy += __ldg(a.cy + l) * (((f1 + f2) - (f3 + f4)) + ((f5 + f6) - (f7 + f8)));
-    uz += __ldg(a.cz + l) * (((f1 + f2) + (f3 + f4)) - ((f5 + f6) + (f7 + f8)));
+  for (int l0 = lane * VPL; l0 < Nc8; l0 += 32 * VPL) {
+    float f[8][VPL];
+#pragma unroll
+    for (int o = 0; o < 8; ++o) {
+      if (VPL == 2) {
+        const float2 t = __ldcs(reinterpret_cast<const float2 *>(hp + (size_t)o * Nc8 + l0));
+        f[o][0] = t.x; f[o][VPL - 1] = t.y;
+      } else {
+        f[o][0] = __ldcs(hp + (size_t)o * Nc8 + l0);
+      }
+    }
+#pragma unroll
+    for (int v = 0; v < VPL; ++v) {
+      const int l = l0 + v;
+      const double f1 = f[0][v], f2 = f[1][v], f3 = f[2][v], f4 = f[3][v], f5 = f[4][v], f6 = f[5][v],
+                   f7 = f[6][v], f8 = f[7][v];
+      r += ((f1 + f2) + (f3 + f4)) + ((f5 + f6) + (f7 + f8));
+      ux += __ldg(a.cx + l) * (((f1 - f2) + (f4 - f3)) + ((f5 - f6) + (f8 - f7)));
+      uy += __ldg(a.cy + l) * (((f1 + f2) - (f3 + f4)) + ((f5 + f6) - (f7 + f8)));
+      uz += __ldg(a.cz + l) * (((f1 + f2) + (f3 + f4)) - ((f5 + f6) + (f7 + f8)));
+    }
   }
   for (int off = 16; off > 0; off >>= 1) {
     r += __shfl_down_sync(0xffffffffu, r, off);
@@ -317,7 +344,9 @@ void launch_symmetry32(const DevState &s, cudaStream_t st) {
   if (s.nsym) k_symmetry32<<<nblocks((size_t)s.nsym * s.Nc8, 256), 256, 0, st>>>(s);
 }
 void launch_moments32(const DevState &s, cudaStream_t st) {
-  if (s.NF) k_moments32<<<nblocks((size_t)s.NF * 32, 256), 256, 0, st>>>(s);
+  if (!s.NF) return;
+  if (s.Nc8 % 2 == 0) k_moments32<2><<<nblocks((size_t)s.NF * 32, 256), 256, 0, st>>>(s);
+  else k_moments32<1><<<nblocks((size_t)s.NF * 32, 256), 256, 0, st>>>(s);
 }
 void launch_widen(const float *src, double *dst, size_t n, cudaStream_t st) {
   if (n) k_widen<<<148 * 16, 256, 0, st>>>(src, dst, n);

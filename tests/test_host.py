@@ -200,3 +200,15 @@ def test_tile_jobs_cover_every_task_once():
         assert count > 0 and np.all(diag == diag[0])
         assert slots >= rows_per_job[jobs].max() and tmax >= ntask[jobs].max()
     assert s.schedule()["max_slots"] == rows_per_job.max()
+
+
+def test_wall_programs_read_no_slot_an_earlier_write_stores():
+    """The wall kernels load the sources of up to four re-emission writes before storing
+    them; that is only valid because no write of a program reads a slot that an earlier
+    write of the same program stores."""
+    from device_model import wall_programs
+    for lab, (faces, writes) in wall_programs().items():
+        stored = set()
+        for dst_st, dst_o, fi, src_st, src_o in writes:
+            assert (src_st, src_o) not in stored, lab
+            stored.add((dst_st, dst_o))
