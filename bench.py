@@ -39,9 +39,16 @@ UNIT = "Gupd/s"
 TOL = 1e-4
 
 
+# the large single solve: a 256^3 Gaussian random field (correlation length 6 voxels)
+# thresholded at porosity 0.20, x-percolating pore cluster kept, 512 velocities, Kn = 0.1
+LARGE = dict(kind="grf", n=256, porosity=0.20, corr=6.0, seed=2024, Nc_fundamental=4, Kn=0.1, wallExtOrder=1)
+
+
 def workload_image():
     from piks3d_b200 import images
     w = WORKLOAD
+    if w.get("kind") == "grf":
+        return images.gaussian_field(w["n"], w["porosity"], corr=w["corr"], seed=w["seed"])
     return images.sphere_pack(w["n"], w["porosity"], w["rmin"], w["rmax"], seed=w["seed"])
 
 
@@ -54,8 +61,15 @@ def workload_params(pk):
 
 def config_dict(extra=None):
     w = WORKLOAD
-    d = {"workload": "sphere-pack %d^3 porosity %.2f radii %g-%g seed %d, Nv=%d, Kn=%g, wallExtOrder %d" % (
-        w["n"], w["porosity"], w["rmin"], w["rmax"], w["seed"], 8 * w["Nc_fundamental"] ** 3, w["Kn"], w["wallExtOrder"]),
+    if w.get("kind") == "grf":
+        name = "Gaussian random field %d^3 corr %g porosity %.2f (x-percolating cluster) seed %d, Nv=%d, Kn=%g, " \
+               "wallExtOrder %d" % (w["n"], w["corr"], w["porosity"], w["seed"], 8 * w["Nc_fundamental"] ** 3, w["Kn"],
+                                    w["wallExtOrder"])
+    else:
+        name = "sphere-pack %d^3 porosity %.2f radii %g-%g seed %d, Nv=%d, Kn=%g, wallExtOrder %d" % (
+            w["n"], w["porosity"], w["rmin"], w["rmax"], w["seed"], 8 * w["Nc_fundamental"] ** 3, w["Kn"],
+            w["wallExtOrder"])
+    d = {"workload": name,
          "image": "%dx%dx%d uint8" % (w["n"], w["n"], w["n"]), "velocities": 8 * w["Nc_fundamental"] ** 3,
          "Kn": w["Kn"], "l2": "inputs larger than L2 (distribution function > 4 GB per rank)"}
     if extra:
@@ -447,19 +461,26 @@ def main():
     ap.add_argument("--cpu-iters", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-solve", action="store_true", help="skip the full solves (solve / e2e blocks)")
-    ap.add_argument("--workload", default="precision", choices=["precision", "batch", "serve"],
-                    help="precision: the 128^3 pack (default); batch: many images; serve: request stream")
+    ap.add_argument("--workload", default="precision", choices=["precision", "batch", "serve", "large"],
+                    help="precision: the 128^3 pack (default); batch: many images; serve: request stream; "
+                         "large: the 256^3 Gaussian random field (add --solve-large for the full solves)")
+    ap.add_argument("--solve-large", action="store_true")
     ap.add_argument("--images", type=int, default=64)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--max-step", type=int, default=20000)
     ap.add_argument("--rate", type=float, default=20.0)
     ap.add_argument("--duration", type=float, default=60.0)
-    ap.add_argument("--horizon", type=float, default=300.0)
+    ap.add_argument("--horizon", type=float, default=240.0)
     ap.add_argument("--edge-min", type=int, default=48)
     ap.add_argument("--edge-max", type=int, default=160)
     ap.add_argument("--edge", "--n", dest="n", type=int, default=None,
                     help="image edge (default 128); smaller edges are for profiling captures, not bench lines")
     args = ap.parse_args()
+    if args.workload == "large":
+        WORKLOAD.clear()
+        WORKLOAD.update(LARGE)
+        args.no_solve = args.no_solve or not args.solve_large
+        args.workload = "precision"
     if args.n:
         WORKLOAD["n"] = args.n
     world, rank, local = dist_setup(args)

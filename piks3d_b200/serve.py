@@ -84,6 +84,7 @@ def make_stream(rate, duration, seed, make_params, edge_range=(48, 160), porosit
         n = int(rng.integers(edge_range[0], edge_range[1] + 1))
         por = float(rng.uniform(*porosity_range))
         kn = float(np.exp(rng.uniform(np.log(kn_range[0]), np.log(kn_range[1]))))
-        img = images.sphere_pack(n, por, 4.0, 8.0, seed=int(seed * 1000 + i))
-        jobs.append(Job(img, make_params(n, kn), name="req%d" % i, arrival=t))
+        def make(n=n, por=por, sd=int(seed * 1000 + i)):
+            return images.sphere_pack(n, por, 4.0, 8.0, seed=sd)
+        jobs.append(Job(None, make_params(n, kn), name="req%d" % i, arrival=t, make_image=make, porosity=por))
     return jobs

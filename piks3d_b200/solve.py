@@ -99,8 +99,11 @@ class Convergence:
 class Job:
     """One solve request: an image (uint8, z-y-x) and its piks_params."""
 
-    def __init__(self, image, params, name=None, arrival=0.0):
+    def __init__(self, image, params, name=None, arrival=0.0, make_image=None, porosity=None):
+        # image may be None with make_image (a callable) given: it is then generated when the
+        # job is prepared, and `porosity` sizes the footprint estimate before that
         self.image, self.params, self.name, self.arrival = image, params, name, arrival
+        self.make_image, self.porosity = make_image, porosity
         self.solver = None
         self.conv = None
         self.phase = None             # "fp32" / "fp64"
@@ -118,8 +121,13 @@ def footprint_bytes(image, params, precision="refined"):
     plus the solid voxels next to fluid (walls) and a fixed overhead for tables. A refined
     solve holds FP32 and FP64 copies of f for the instant of the switch."""
     nc8 = params.Nc_fundamental ** 3
-    fluid = int(np.count_nonzero(np.asarray(image) == 0))
-    nodes = int(fluid * 1.7) + 2 * params.fluidlayer * image.shape[0] * image.shape[1]
+    if isinstance(image, tuple):      # (n voxels, porosity) before the image exists
+        fluid = int(image[0] * image[1])
+        face = int(round(image[0] ** (2.0 / 3.0)))
+    else:
+        fluid = int(np.count_nonzero(np.asarray(image) == 0))
+        face = image.shape[0] * image.shape[1]
+    nodes = int(fluid * 1.7) + 2 * params.fluidlayer * face
     f32 = nodes * 8 * nc8 * 4
     f64 = nodes * 8 * nc8 * 8
     moments = fluid * 32
@@ -132,6 +140,8 @@ def footprint_bytes(image, params, precision="refined"):
 
 
 def _prepare(job, device, precision):
+    if job.image is None:
+        job.image = job.make_image()
     s = Solver(job.params, device=device)
     if precision in ("fp32", "refined"):
         s.set_precision(PREC_FP32)
@@ -181,7 +191,12 @@ class BatchRunner:
 
     def try_admit(self, job, now):
         """Starts preprocessing `job` if its footprint fits; returns False when it must wait."""
-        fp = footprint_bytes(job.image, job.params, self.precision)
+        if job.image is None:
+            p = job.params
+            img = (p.Nx * p.Ny * p.Nz, job.porosity if job.porosity is not None else 1.0)
+        else:
+            img = job.image
+        fp = footprint_bytes(img, job.params, self.precision)
         slots = len(self.active) + len(self.preparing)
         if slots >= self.max_members or (self.reserved + fp > self.hbm_budget and slots > 0):
             return False
