@@ -151,7 +151,8 @@ enum { PIKS_PREC_FP64 = 0, PIKS_PREC_FP32 = 1 };
 piks_status piks_set_precision(piks_ctx *ctx, int32_t precision);
 piks_status piks_get_precision(piks_ctx *ctx, int32_t *precision);
 
-/* Sweep schedule. The default cuts the box into 8x4x4 tiles and sweeps, for each octant,
+/* Sweep schedule. The default cuts the box into 8x4x4 tiles (4x4x4 when the context is in
+ * FP32 at setup) and sweeps, for each octant,
  * the tiles in diagonal order, each tile's local hyperplanes in shared memory (one launch
  * per tile diagonal). tx = 0 selects the per-node hyperplane schedule (one launch per
  * voxel hyperplane u+v+w). Both give identical results; the tile schedule also falls back

@@ -393,6 +393,12 @@ piks_status piks_setup_physical_grid(piks_ctx *c, const uint8_t *raw, int64_t nb
   piks_status st = preprocess(c->setup, raw, nbytes, c->geo, err);
   if (st) return fail(st, err);
   c->have_host_geometry = true;
+  if (!c->tiles_explicit) {
+    // measured fastest on B200 for 512 velocities: 8x4x4 tiles for the FP64 sweep, 4x4x4 for
+    // the FP32 sweep (whose CTAs carry twice the velocities per row)
+    const int d = c->prec == PIKS_PREC_FP32 ? 4 : 8;
+    c->tile_dims[0] = d; c->tile_dims[1] = 4; c->tile_dims[2] = 4;
+  }
   build_tiles(c);
   if (c->device < 0) return PIKS_OK;
   const Geometry &g = c->geo;
@@ -743,6 +749,7 @@ piks_status piks_set_tiles(piks_ctx *c, int32_t tx, int32_t ty, int32_t tz) {
   if (tx < 0 || ty < 0 || tz < 0 || (tx > 0 && (ty < 2 || tz < 2 || tx < 2)) || (int64_t)tx * ty * tz > 65535)
     return fail(PIKS_ERR_ARG, "tile extents must be 0 (per-node schedule) or >= 2 with at most 65535 voxels");
   c->tile_dims[0] = tx; c->tile_dims[1] = tx ? ty : 0; c->tile_dims[2] = tx ? tz : 0;
+  c->tiles_explicit = true;
   return PIKS_OK;
 }
 

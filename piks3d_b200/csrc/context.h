@@ -29,6 +29,7 @@ struct piks_ctx {
   size_t dev_bytes = 0;
   int prec = PIKS_PREC_FP64;        // storage / sweep precision of the state
   int tile_dims[3] = {8, 4, 4};     // tile shape of the sweep schedule (0: per-node hyperplanes)
+  bool tiles_explicit = false;      // set by piks_set_tiles; otherwise chosen by precision at setup
   piks::TileJobs tiles;
   bool use_tiles = false;           // tile schedule built and uploaded
   int schedule = PIKS_SCHED_TILE_DIAGONALS;
