@@ -25,12 +25,20 @@ constexpr int kFwBit = 1 << 30;
 
 template <int VPL>
 __device__ __forceinline__ void ld32(const float *p, float (&v)[VPL]) {
-  if (VPL == 2) { const float2 t = __ldcg(reinterpret_cast<const float2 *>(p)); v[0] = t.x; v[VPL - 1] = t.y; }
-  else v[0] = __ldcg(p);
+  if constexpr (VPL == 4) {
+    const float4 t = __ldcg(reinterpret_cast<const float4 *>(p));
+    v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+  } else if constexpr (VPL == 2) {
+    const float2 t = __ldcg(reinterpret_cast<const float2 *>(p));
+    v[0] = t.x; v[1] = t.y;
+  } else {
+    v[0] = __ldcg(p);
+  }
 }
 template <int VPL>
 __device__ __forceinline__ void st32(float *p, const float (&v)[VPL]) {
-  if (VPL == 2) *reinterpret_cast<float2 *>(p) = make_float2(v[0], v[VPL - 1]);
+  if constexpr (VPL == 4) *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+  else if constexpr (VPL == 2) *reinterpret_cast<float2 *>(p) = make_float2(v[0], v[1]);
   else p[0] = v[0];
 }
 
@@ -114,11 +122,13 @@ __global__ void k_capture32(const DevState a, int buf) {
 
 // Walls: extrapolation and re-emission in FP32, the wall densities summed in FP64 (a warp
 // reduction) and the re-emitted value formed in FP64 before rounding.
-template <int VPL>
+template <int VPL, int LANES>
 __global__ void __launch_bounds__(256) k_walls32(const DevState a, int begin, int end, int gbuf) {
-  const int widx = begin + (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  // LANES lanes per wall (32 / LANES walls per warp), VPL velocities per lane
+  const int widx = begin + (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) / LANES);
   if (widx >= end) return;
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x % LANES;
+  const unsigned seg = LANES == 32 ? 0xffffffffu : (((1u << LANES) - 1u) << (threadIdx.x & 31 & ~(LANES - 1)));
   const int q = a.wall_order[widx];
   const int node = a.wall_node[q];
   const int corner = a.wall_corner[q];
@@ -127,7 +137,7 @@ __global__ void __launch_bounds__(256) k_walls32(const DevState a, int begin, in
   const int Nc8 = a.Nc8;
   const int *nb = a.wall_nb + 6 * q;
   const int nface = P.nface;
-  const int chunkw = 32 * VPL;
+  const int chunkw = LANES * VPL;
   auto far_ptr = [&](int code, int oo, int lf) -> const float * {
     if (code >= 0) return a.h32 + hidx(code, oo, Nc8, lf);
     if (code == -1) return nullptr;
@@ -173,7 +183,7 @@ __global__ void __launch_bounds__(256) k_walls32(const DevState a, int begin, in
       for (int v = 0; v < VPL; ++v) racc += tface[v];
     }
     // warp sum in FP64 (the FP32 path does not keep the reference's summation order)
-    for (int off = 16; off > 0; off >>= 1) racc += __shfl_xor_sync(0xffffffffu, racc, off);
+    for (int off = LANES / 2; off > 0; off >>= 1) racc += __shfl_xor_sync(seg, racc, off, LANES);
     if (fi == 0) rho0 = racc; else if (fi == 1) rho1 = racc; else rho2 = racc;
   }
   rho0 /= a.DiffFlux; rho1 /= a.DiffFlux; rho2 /= a.DiffFlux;
@@ -333,9 +343,10 @@ void launch_capture32(const DevState &s, int buf, cudaStream_t st) {
 }
 void launch_walls32(const DevState &s, int begin, int end, int gbuf, cudaStream_t st) {
   if (end <= begin) return;
-  const size_t threads = (size_t)(end - begin) * 32;
-  if (s.Nc8 % 64 == 0) k_walls32<2><<<nblocks(threads, 256), 256, 0, st>>>(s, begin, end, gbuf);
-  else k_walls32<1><<<nblocks(threads, 256), 256, 0, st>>>(s, begin, end, gbuf);
+  const size_t walls = (size_t)(end - begin);
+  if (s.Nc8 % 64 == 0) k_walls32<4, 16><<<nblocks(walls * 16, 256), 256, 0, st>>>(s, begin, end, gbuf);
+  else if (s.Nc8 == 8) k_walls32<1, 8><<<nblocks(walls * 8, 256), 256, 0, st>>>(s, begin, end, gbuf);
+  else k_walls32<1, 32><<<nblocks(walls * 32, 256), 256, 0, st>>>(s, begin, end, gbuf);
 }
 void launch_inlet_outlet32(const DevState &s, int buf, cudaStream_t st) {
   k_inlet_outlet32<<<nblocks((size_t)s.Ny * s.Nz * 4 * s.Nc8, 256), 256, 0, st>>>(s, buf);
