@@ -211,7 +211,8 @@ void enqueue_sweep(piks_ctx *c, cudaStream_t st, int n) {
       launch_tile_sweep_dataflow(s, f32, n, c->tiles.max_rows, c->tiles.max_tasks, st);
     } else if (c->use_tiles) {
       const auto &L = c->tiles.launches;
-      for (size_t k = 0; k + 3 < L.size(); k += 4) launch_tile_sweep(s, f32, L[k], L[k + 1], L[k + 2], L[k + 3], st);
+      for (size_t k = 0; k + 3 < L.size(); k += 4)
+        launch_tile_sweep(s, f32, L[k], L[k + 1], L[k + 2], L[k + 3], k > 0, st);
     } else {
       const auto &hs = c->geo.hyper_start;
       for (size_t h = 0; h + 1 < hs.size(); ++h) {

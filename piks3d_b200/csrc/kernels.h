@@ -91,7 +91,11 @@ void launch_moments32(const DevState &s, cudaStream_t st);
 // `slots` shared-memory rows and room for `tasks` task records per CTA. tile_sweep_velocities() is the chunk width V used for the precision.
 int tile_sweep_velocities(int Nc8, bool fp32);
 int tile_sweep_max_slots(int Nc8, bool fp32, int tile_voxels, int nsteps);
-void launch_tile_sweep(const DevState &s, bool fp32, int job0, int njobs, int slots, int tasks, cudaStream_t st);
+// pdl: launch as a programmatic dependent of the previous kernel in the stream: the next tile
+// diagonal's CTAs start their first loads (codes, records, moments) while the previous
+// diagonal finishes, and wait for it before reading rows. Only for diagonals after the first.
+void launch_tile_sweep(const DevState &s, bool fp32, int job0, int njobs, int slots, int tasks, bool pdl,
+                       cudaStream_t st);
 // Dataflow form: all jobs in one launch, ordered by the flags of `epoch` (> 0, one value per
 // sweep); slots / tasks are the largest of any job.
 void launch_tile_sweep_dataflow(const DevState &s, bool fp32, int epoch, int slots, int tasks, cudaStream_t st);

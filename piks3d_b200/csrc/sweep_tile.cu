@@ -88,6 +88,8 @@ __device__ __forceinline__ void tile_job(const DevState &a, int job, int chunk, 
   uint16_t *Steps = reinterpret_cast<uint16_t *>(Codes + ((size_t)slots_cap + 3) / 4 * 4);
   const T *h = state_h<T>(a);
   const T *fw = state_fw<T>(a);
+  // the next tile diagonal (launched as a programmatic dependent) may start its first round
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 
   // 1a. row codes, task records and step offsets -> shared memory
   for (int i = threadIdx.x; i < (nrows + 3) / 4; i += THREADS)
@@ -97,16 +99,18 @@ __device__ __forceinline__ void tile_job(const DevState &a, int job, int chunk, 
     cp_async16(Steps + 8 * i, tv.steps + (size_t)job * tv.steps_stride + 8 * i);
   cp_async_wait_all();
   __syncthreads();
-  // 1b. rows (slot 0 = zeros) and the moments of the tasks' nodes (FP64 Rho, Ux | Uy, Uz)
+  // 1b. the moments of the tasks' nodes (FP64 Rho, Ux | Uy, Uz; written by the previous
+  //     iteration), then, once the previous diagonal's rows are visible, the rows
+  for (int i = threadIdx.x; i < 2 * ntask; i += THREADS) {
+    const int m = Trec[i >> 1].x & ((1 << 27) - 1);
+    cp_async16(Mom + i, reinterpret_cast<const double2 *>(a.mom) + 2 * (size_t)m + (i & 1));
+  }
+  asm volatile("griddepcontrol.wait;" ::: "memory");
   for (int i = threadIdx.x; i < nrows * PIECES; i += THREADS) {
     const int r = i / PIECES, pc = i - r * PIECES;
     const int code = Codes[r];
     const T *src = ((code & kFwBit) ? fw : h) + (size_t)(code & ~kFwBit) * (size_t)Nc8 + l0 + pc * EPP;
     cp_async16(S + (size_t)(1 + r) * V + pc * EPP, src);
-  }
-  for (int i = threadIdx.x; i < 2 * ntask; i += THREADS) {
-    const int m = Trec[i >> 1].x & ((1 << 27) - 1);
-    cp_async16(Mom + i, reinterpret_cast<const double2 *>(a.mom) + 2 * (size_t)m + (i & 1));
   }
   if (threadIdx.x < PIECES) *reinterpret_cast<int4 *>(S + threadIdx.x * EPP) = make_int4(0, 0, 0, 0);
 
@@ -396,7 +400,7 @@ void launch_dataflow(const DevState &s, int epoch, int slots, int tasks, cudaStr
 }
 
 template <typename T, int V>
-void launch_one(const DevState &s, int job0, int njobs, int slots, int tasks, cudaStream_t st) {
+void launch_one(const DevState &s, int job0, int njobs, int slots, int tasks, bool pdl, cudaStream_t st) {
   static unsigned long long configured = 0;  // one bit per device
   int dev = 0;
   cudaGetDevice(&dev);
@@ -404,9 +408,17 @@ void launch_one(const DevState &s, int job0, int njobs, int slots, int tasks, cu
     allow_dynamic_smem(reinterpret_cast<const void *>(k_tile_sweep<T, V>), dev);
     configured |= 1ull << (dev & 63);
   }
-  const size_t smem = tile_smem_bytes(slots, tasks, s.tv.steps_stride, V * (int)sizeof(T));
-  const unsigned grid = (unsigned)((size_t)njobs * (s.Nc8 / V));
-  k_tile_sweep<T, V><<<grid, threads_of<T, V>(), smem, st>>>(s, job0, slots, tasks);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)((size_t)njobs * (s.Nc8 / V)));
+  cfg.blockDim = dim3(threads_of<T, V>());
+  cfg.dynamicSmemBytes = tile_smem_bytes(slots, tasks, s.tv.steps_stride, V * (int)sizeof(T));
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, k_tile_sweep<T, V>, s, job0, slots, tasks);
 }
 
 }  // namespace
@@ -424,16 +436,17 @@ int tile_sweep_max_slots(int Nc8, bool fp32, int tile_voxels, int nsteps) {
   return fixed >= cap ? 0 : (int)((cap - fixed) / (row + 4));
 }
 
-void launch_tile_sweep(const DevState &s, bool fp32, int job0, int njobs, int slots, int tasks, cudaStream_t st) {
+void launch_tile_sweep(const DevState &s, bool fp32, int job0, int njobs, int slots, int tasks, bool pdl,
+                       cudaStream_t st) {
   if (njobs <= 0) return;
   const int V = tile_sweep_velocities(s.Nc8, fp32);
   if (fp32) {
-    if (V == 32) launch_one<float, 32>(s, job0, njobs, slots, tasks, st);
-    else if (V == 16) launch_one<float, 16>(s, job0, njobs, slots, tasks, st);
-    else launch_one<float, 8>(s, job0, njobs, slots, tasks, st);
+    if (V == 32) launch_one<float, 32>(s, job0, njobs, slots, tasks, pdl, st);
+    else if (V == 16) launch_one<float, 16>(s, job0, njobs, slots, tasks, pdl, st);
+    else launch_one<float, 8>(s, job0, njobs, slots, tasks, pdl, st);
   } else {
-    if (V == 16) launch_one<double, 16>(s, job0, njobs, slots, tasks, st);
-    else launch_one<double, 8>(s, job0, njobs, slots, tasks, st);
+    if (V == 16) launch_one<double, 16>(s, job0, njobs, slots, tasks, pdl, st);
+    else launch_one<double, 8>(s, job0, njobs, slots, tasks, pdl, st);
   }
 }
 
