@@ -44,6 +44,41 @@ const WProg *wall_program(int label) {
   return nullptr;
 }
 
+bool make_wall_plan(const WProg &p, WPlan &out) {
+  out = WPlan{};
+  out.nface = p.nface;
+  out.nwr = p.nwr;
+  if (p.nface < 1 || p.nface > 3 || p.nwr > 12) return false;
+  for (int f = 0; f < p.nface; ++f) {
+    out.dir[f] = p.face[f].dir;
+    out.store[f] = p.face[f].store;
+    out.keep[f] = p.face[f].store == ST_Z ? 0 : 0xf;
+  }
+  for (int k = 0; k < p.nwr; ++k) {
+    const WWrite &w = p.wr[k];
+    int src = -1;
+    for (int f = 0; f < p.nface; ++f)
+      for (int m = 0; m < 4; ++m)
+        if (p.face[f].store == w.src_store && kIncoming[p.face[f].dir][m] == w.src_o) {
+          if (src >= 0) return false;  // two faces produce the value
+          src = f * 4 + m;
+        }
+    if (src < 0) return false;
+    for (int j = 0; j < k; ++j)  // an earlier write replaced the source slot
+      if (p.wr[j].dst_store == w.src_store && p.wr[j].dst_o == w.src_o) return false;
+    for (int j = 0; j < k; ++j)
+      if (p.wr[j].dst_store == w.dst_store && p.wr[j].dst_o == w.dst_o) return false;
+    for (int f = 0; f < p.nface; ++f)
+      for (int m = 0; m < 4; ++m)
+        if (p.face[f].store == w.dst_store && kIncoming[p.face[f].dir][m] == w.dst_o) out.keep[f] &= ~(1 << m);
+    out.dst_store[k] = w.dst_store;
+    out.dst_o[k] = w.dst_o - 1;
+    out.face[k] = w.face;
+    out.src[k] = src;
+  }
+  return true;
+}
+
 uint8_t face_mask(int v) {
   // The wall label names the fluid sides: E (+x), W (-x), N (+y), S (-y), F (+z), B (-z).
   switch (v) {

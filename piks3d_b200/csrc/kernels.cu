@@ -15,6 +15,8 @@ namespace {
 __constant__ uint8_t c_face[128];        // fluid-side bits per label
 __constant__ int8_t c_prog_of[128];      // label -> wall program index or -1
 __constant__ WProg c_prog[26];
+__constant__ WPlan c_plan[26];
+bool g_plan_ok = false;                  // every program resolved (make_wall_plan)
 __constant__ int c_incoming[6][4];
 
 __device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
@@ -30,6 +32,11 @@ __device__ __forceinline__ int dsz(int o) { return o < 4 ? 1 : -1; }
 __device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+// 16 bytes through L2 only (the moments read each value once).
+__device__ __forceinline__ void cp_async16_cg(void *smem, const void *gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
@@ -188,13 +195,20 @@ __device__ __forceinline__ void ld_vpl(const double *p, double (&v)[VPL]) {
   else v[0] = __ldcg(p);
 }
 template <int VPL>
+__device__ __forceinline__ void ld_vpl_sm(const double *p, double (&v)[VPL]) {
+  if (VPL == 2) { const double2 t = *reinterpret_cast<const double2 *>(p); v[0] = t.x; v[VPL - 1] = t.y; }
+  else v[0] = p[0];
+}
+template <int VPL>
 __device__ __forceinline__ void st_vpl(double *p, const double (&v)[VPL]) {
   if (VPL == 2) *reinterpret_cast<double2 *>(p) = make_double2(v[0], v[VPL - 1]);
   else p[0] = v[0];
 }
 
+// At most 51 registers (five 256-thread blocks per SM): a wall's time is mostly memory
+// round trips, so more resident walls pay (measured 1.38 -> 1.04 ms on a 128^3 pack).
 template <int VPL>
-__global__ void __launch_bounds__(256) k_walls(const DevState a, int begin, int end, int gbuf) {
+__global__ void __launch_bounds__(256, 5) k_walls(const DevState a, int begin, int end, int gbuf) {
   const int widx = begin + (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   if (widx >= end) return;  // whole warp
   const int lane = threadIdx.x & 31;
@@ -314,6 +328,107 @@ __global__ void __launch_bounds__(256) k_walls(const DevState a, int begin, int 
   }
 }
 
+// The diffuse wall for octants of at most 32 * VPL velocities (one pass of the warp), with
+// the extrapolated face values kept in shared memory: the re-emission reads them there
+// (WPlan) instead of re-loading the slots, and a face value is stored only where it is
+// the slot's final content. Same operations on the same operands as k_walls, in the same
+// order; per warp, 12 * Nc8 face values and Nc8 density terms.
+constexpr int kWallWarps = 8;
+template <int VPL>
+__global__ void __launch_bounds__(kWallWarps * 32, 4) k_walls_onchip(const DevState a, int begin, int end, int gbuf) {
+  extern __shared__ __align__(16) double wall_sm[];
+  const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int widx = begin + (int)blockIdx.x * kWallWarps + wib;
+  if (widx >= end) return;  // whole warp (only warp-level synchronisation below)
+  const int Nc8 = a.Nc8;
+  double *E = wall_sm + (size_t)wib * 13 * Nc8;
+  double *Tm = E + 12 * Nc8;
+  const int q = a.wall_order[widx];
+  const int node = a.wall_node[q];
+  const int corner = a.wall_corner[q];
+  const WPlan &P = c_plan[c_prog_of[a.wall_label[q]]];
+  const double e1 = a.wall_e[2 * q], e2 = a.wall_e[2 * q + 1];
+  const int *nb = a.wall_nb + 6 * q;
+  const int nface = P.nface;
+  const int lf = lane * VPL;
+  const bool lv = lf < Nc8;
+  double rho0 = 0.0, rho1 = 0.0, rho2 = 0.0;
+  for (int fi = 0; fi < nface; ++fi) {
+    const int dir = P.dir[fi], st = P.store[fi], keep = P.keep[fi];
+    const int n1 = nb[2 * fi], code = nb[2 * fi + 1];
+    if (lv) {
+      const double *plane = nullptr;
+      size_t prow = 0;
+      if (code < -1) {
+        const int cc = -code - 2;
+        plane = (cc & 1) ? a.ghostE[gbuf] : a.ghostW[gbuf];
+        prow = (size_t)(cc >> 1) * 4;
+      }
+      double near_[4][VPL], far_[4][VPL];
+#pragma unroll
+      for (int mm = 0; mm < 4; ++mm) {
+        const int oo = c_incoming[dir][mm] - 1;
+#pragma unroll
+        for (int v = 0; v < VPL; ++v) far_[mm][v] = 0.0;
+        ld_vpl<VPL>(a.h + hidx(n1, oo, Nc8, lf), near_[mm]);
+        if (code >= 0) ld_vpl<VPL>(a.h + hidx(code, oo, Nc8, lf), far_[mm]);
+        else if (plane) ld_vpl<VPL>(plane + (prow + plane_slot(oo)) * Nc8 + lf, far_[mm]);
+      }
+      double ext[4][VPL];
+#pragma unroll
+      for (int mm = 0; mm < 4; ++mm) {
+        const int oo = c_incoming[dir][mm] - 1;
+#pragma unroll
+        for (int v = 0; v < VPL; ++v) ext[mm][v] = dadd(dmul(e1, near_[mm][v]), dmul(e2, far_[mm][v]));
+        st_vpl<VPL>(E + (size_t)(fi * 4 + mm) * Nc8 + lf, ext[mm]);
+        if (keep >> mm & 1) {
+          if (st == ST_F) st_vpl<VPL>(a.h + hidx(node, oo, Nc8, lf), ext[mm]);
+          else st_vpl<VPL>(a.fw + hidx(corner, oo, Nc8, lf), ext[mm]);
+        }
+      }
+      double tface[VPL];
+#pragma unroll
+      for (int v = 0; v < VPL; ++v) {
+        const int l = lf + v;
+        const double ca = dir < 2 ? __ldg(a.cx + l) : dir < 4 ? __ldg(a.cy + l) : __ldg(a.cz + l);
+        tface[v] = dmul(ca, dadd(dadd(dadd(ext[0][v], ext[1][v]), ext[2][v]), ext[3][v]));
+      }
+      st_vpl<VPL>(Tm + lf, tface);
+    }
+    __syncwarp();
+    // rho_face = sum over l in ascending order (every lane, broadcast reads)
+    double racc = 0.0;
+    int l = 0;
+    for (; l + 8 <= Nc8; l += 8) {
+      double t[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) t[j] = Tm[l + j];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) racc = dadd(racc, t[j]);
+    }
+    for (; l < Nc8; ++l) racc = dadd(racc, Tm[l]);
+    __syncwarp();  // Tm is rewritten by the next face
+    if (fi == 0) rho0 = racc; else if (fi == 1) rho1 = racc; else rho2 = racc;
+  }
+  if (!lv) return;
+  rho0 = __ddiv_rn(rho0, a.DiffFlux);
+  if (nface > 1) rho1 = __ddiv_rn(rho1, a.DiffFlux);
+  if (nface > 2) rho2 = __ddiv_rn(rho2, a.DiffFlux);
+  const double one_m = dsub(1.0, a.accom);
+  double aw[VPL];
+#pragma unroll
+  for (int v = 0; v < VPL; ++v) aw[v] = dmul(a.accom, __ldg(a.w + lf + v));
+  for (int k = 0; k < P.nwr; ++k) {
+    double src[VPL], val[VPL];
+    ld_vpl_sm<VPL>(E + (size_t)P.src[k] * Nc8 + lf, src);
+    const double rf = P.face[k] == 0 ? rho0 : P.face[k] == 1 ? rho1 : rho2;
+#pragma unroll
+    for (int v = 0; v < VPL; ++v) val[v] = dadd(dmul(aw[v], rf), dmul(one_m, src[v]));
+    if (P.dst_store[k] == ST_F) st_vpl<VPL>(a.h + hidx(node, P.dst_o[k], Nc8, lf), val);
+    else st_vpl<VPL>(a.fw + hidx(corner, P.dst_o[k], Nc8, lf), val);
+  }
+}
+
 // Inlet x = 1 and outlet x = Nx with the pressure jump (solver.F90:1832-1862), reading the
 // ghost planes captured in the previous iteration.
 __global__ void k_inlet_outlet(const DevState a, int gbuf) {
@@ -403,6 +518,82 @@ __global__ void __launch_bounds__(kMomWarps * 32) k_moments(const DevState a) {
         ux = dadd(ux, dmul(__ldg(a.cx + l0 + s2), dx));
         uy = dadd(uy, dmul(__ldg(a.cy + l0 + s2), dy));
         uz = dadd(uz, dmul(__ldg(a.cz + l0 + s2), dz));
+      }
+    }
+    __syncwarp();
+    b ^= 1;
+  }
+  if (lane < nvalid) {
+    const int n = node0 + lane;
+    double2 *mp = reinterpret_cast<double2 *>(a.mom) + 2 * (size_t)n;
+    mp[0] = make_double2(r, ux);
+    mp[1] = make_double2(uy, uz);
+  }
+}
+
+// The same sums for octants whose velocity count is a multiple of 8: each stage moves 8
+// velocities of every (node, octant) of the warp's 32 nodes, a 64-byte segment per
+// (node, octant) in four 16-byte copies (four lanes per segment, eight segments per warp
+// request). A node's staged row holds 66 doubles (8 octants x 8 velocities + 2 pad), so a
+// quarter-warp's 16-byte reads cover all 32 banks.
+constexpr int kMomWWarps = 2;
+constexpr int kMomWL = 8;
+constexpr int kMomWStride = 8 * kMomWL + 2;
+struct MomWSmem { double buf[kMomWWarps][2][32 * kMomWStride]; };
+
+__global__ void __launch_bounds__(kMomWWarps * 32) k_moments_wide(const DevState a) {
+  extern __shared__ __align__(16) unsigned char mom_raw[];
+  MomWSmem &S = *reinterpret_cast<MomWSmem *>(mom_raw);
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int node0 = (blockIdx.x * kMomWWarps + wid) * 32;
+  if (node0 >= a.NF) return;  // whole warp
+  const int Nc8 = a.Nc8;
+  const int nvalid = min(32, a.NF - node0);
+  // piece p = lane + 32*r (r < 32) of a stage's 1024: segment (nn, o) = p / 4, quarter p % 4
+  const int pc = lane & 3;
+  auto issue = [&](int l0, int b) {
+    double *dst = S.buf[wid][b];
+#pragma unroll 8
+    for (int r = 0; r < 32; ++r) {
+      const int seg = (lane >> 2) + 8 * r;
+      const int nn = seg >> 3, o = seg & 7;
+      if (nn < nvalid)
+        cp_async16_cg(dst + nn * kMomWStride + o * kMomWL + 2 * pc, a.h + hidx(node0 + nn, o, Nc8, l0 + 2 * pc));
+    }
+    cp_async_commit();
+  };
+  double r = 0.0, ux = 0.0, uy = 0.0, uz = 0.0;
+  issue(0, 0);
+  int b = 0;
+  for (int l0 = 0; l0 < Nc8; l0 += kMomWL) {
+    if (l0 + kMomWL < Nc8) { issue(l0 + kMomWL, b ^ 1); cp_async_wait<1>(); }
+    else cp_async_wait<0>();
+    __syncwarp();
+    double cxs[kMomWL], cys[kMomWL], czs[kMomWL];
+#pragma unroll
+    for (int s2 = 0; s2 < kMomWL; ++s2) {
+      cxs[s2] = __ldg(a.cx + l0 + s2); cys[s2] = __ldg(a.cy + l0 + s2); czs[s2] = __ldg(a.cz + l0 + s2);
+    }
+    const double *mine = S.buf[wid][b] + lane * kMomWStride;
+    if (lane < nvalid) {
+#pragma unroll
+      for (int j = 0; j < kMomWL / 2; ++j) {
+        double2 g[8];
+#pragma unroll
+        for (int o = 0; o < 8; ++o) g[o] = *reinterpret_cast<const double2 *>(mine + o * kMomWL + 2 * j);
+#pragma unroll
+        for (int h2 = 0; h2 < 2; ++h2) {
+          const double f1 = h2 ? g[0].y : g[0].x, f2 = h2 ? g[1].y : g[1].x, f3 = h2 ? g[2].y : g[2].x,
+                       f4 = h2 ? g[3].y : g[3].x, f5 = h2 ? g[4].y : g[4].x, f6 = h2 ? g[5].y : g[5].x,
+                       f7 = h2 ? g[6].y : g[6].x, f8 = h2 ? g[7].y : g[7].x;
+          r = dadd(dadd(dadd(dadd(dadd(dadd(dadd(dadd(r, f1), f2), f3), f4), f5), f6), f7), f8);
+          const double dx = dadd(dsub(dsub(dadd(dadd(dsub(dsub(f1, f2), f3), f4), f5), f6), f7), f8);
+          const double dy = dsub(dsub(dadd(dadd(dsub(dsub(dadd(f1, f2), f3), f4), f5), f6), f7), f8);
+          const double dz = dsub(dsub(dsub(dsub(dadd(dadd(dadd(f1, f2), f3), f4), f5), f6), f7), f8);
+          ux = dadd(ux, dmul(cxs[2 * j + h2], dx));
+          uy = dadd(uy, dmul(cys[2 * j + h2], dy));
+          uz = dadd(uz, dmul(czs[2 * j + h2], dz));
+        }
       }
     }
     __syncwarp();
@@ -594,6 +785,11 @@ void upload_tables() {
   cudaMemcpyToSymbol(c_prog_of, prog_of, sizeof prog_of);
   cudaMemcpyToSymbol(c_prog, progs, sizeof progs);
   cudaMemcpyToSymbol(c_incoming, kIncoming, sizeof(int) * 24);
+  WPlan plans[26];
+  int ok = n == 26;
+  for (int i = 0; i < n; ++i) ok &= make_wall_plan(progs[i], plans[i]) ? 1 : 0;
+  g_plan_ok = ok != 0;
+  cudaMemcpyToSymbol(c_plan, plans, sizeof plans);
 }
 
 void launch_sweep_hyperplane(const DevState &s, long t0, long ntask, cudaStream_t st) {
@@ -636,13 +832,34 @@ void launch_moments(const DevState &s, cudaStream_t st) {
   cudaGetDevice(&dev);
   if (!(configured >> (dev & 63) & 1ull)) {
     cudaFuncSetAttribute(k_moments, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MomSmem));
+    cudaFuncSetAttribute(k_moments_wide, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MomWSmem));
     configured |= 1ull << (dev & 63);
+  }
+  if (s.Nc8 % kMomWL == 0) {
+    k_moments_wide<<<blocks_for((size_t)s.NF, kMomWWarps * 32), kMomWWarps * 32, sizeof(MomWSmem), st>>>(s);
+    return;
   }
   k_moments<<<blocks_for((size_t)s.NF, kMomWarps * 32), kMomWarps * 32, sizeof(MomSmem), st>>>(s);
 }
 
 void launch_walls(const DevState &s, int begin, int end, int gbuf, cudaStream_t st) {
   if (end <= begin) return;
+  if (g_plan_ok && s.Nc8 <= 64 && (s.Nc8 <= 32 || s.Nc8 % 2 == 0)) {
+    static unsigned long long configured = 0;  // one bit per device
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!(configured >> (dev & 63) & 1ull)) {
+      const int most = kWallWarps * 13 * 64 * (int)sizeof(double);
+      cudaFuncSetAttribute(k_walls_onchip<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
+      cudaFuncSetAttribute(k_walls_onchip<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
+      configured |= 1ull << (dev & 63);
+    }
+    const size_t smem = (size_t)kWallWarps * 13 * s.Nc8 * sizeof(double);
+    const unsigned grid = blocks_for((size_t)(end - begin), kWallWarps);
+    if (s.Nc8 > 32) k_walls_onchip<2><<<grid, kWallWarps * 32, smem, st>>>(s, begin, end, gbuf);
+    else k_walls_onchip<1><<<grid, kWallWarps * 32, smem, st>>>(s, begin, end, gbuf);
+    return;
+  }
   const size_t threads = (size_t)(end - begin) * 32;
   if (s.Nc8 % 64 == 0) k_walls<2><<<blocks_for(threads, 256), 256, 0, st>>>(s, begin, end, gbuf);
   else k_walls<1><<<blocks_for(threads, 256), 256, 0, st>>>(s, begin, end, gbuf);

@@ -14,6 +14,8 @@ namespace piks {
 namespace {
 
 __constant__ WProg c32_prog[26];
+__constant__ WPlan c32_plan[26];
+bool g32_plan_ok = false;  // every program resolved (make_wall_plan)
 __constant__ int8_t c32_prog_of[128];
 __constant__ int c32_incoming[6][4];
 
@@ -232,6 +234,89 @@ __global__ void __launch_bounds__(256) k_walls32(const DevState a, int begin, in
   }
 }
 
+// The FP32 diffuse wall for octants of at most LANES * VPL velocities (one pass of the
+// lane segment), with the extrapolated face values kept in shared memory (12 * Nc8 floats
+// per wall): the re-emission reads them there (WPlan) instead of re-loading the slots,
+// and a face value is stored only where it is the slot's final content.
+template <int VPL, int LANES>
+__global__ void __launch_bounds__(256, 4) k_walls32_onchip(const DevState a, int begin, int end, int gbuf) {
+  extern __shared__ __align__(16) float wall32_sm[];
+  const int wib = threadIdx.x / LANES;
+  const int widx = begin + (int)blockIdx.x * (256 / LANES) + wib;
+  if (widx >= end) return;  // whole segment
+  const int lane = threadIdx.x % LANES;
+  const unsigned seg = LANES == 32 ? 0xffffffffu : (((1u << LANES) - 1u) << (threadIdx.x & 31 & ~(LANES - 1)));
+  const int Nc8 = a.Nc8;
+  float *E = wall32_sm + (size_t)wib * 12 * Nc8;
+  const int q = a.wall_order[widx];
+  const int node = a.wall_node[q];
+  const int corner = a.wall_corner[q];
+  const WPlan &P = c32_plan[c32_prog_of[a.wall_label[q]]];
+  const float e1 = (float)a.wall_e[2 * q], e2 = (float)a.wall_e[2 * q + 1];
+  const int *nb = a.wall_nb + 6 * q;
+  const int nface = P.nface;
+  const int lf = lane * VPL;
+  const bool lv = lf < Nc8;
+  auto far_ptr = [&](int code, int oo) -> const float * {
+    if (code >= 0) return a.h32 + hidx(code, oo, Nc8, lf);
+    if (code == -1) return nullptr;
+    const int cc = -code - 2;
+    const float *plane = (cc & 1) ? a.ghostE32[gbuf] : a.ghostW32[gbuf];
+    return plane + ((size_t)(cc >> 1) * 4 + plane_slot(oo)) * Nc8 + lf;
+  };
+  double rho0 = 0.0, rho1 = 0.0, rho2 = 0.0;
+  for (int fi = 0; fi < nface; ++fi) {
+    const int dir = P.dir[fi], st = P.store[fi], keep = P.keep[fi];
+    const int n1 = nb[2 * fi], code = nb[2 * fi + 1];
+    double racc = 0.0;
+    if (lv) {
+      float nv[4][VPL], fv[4][VPL];
+#pragma unroll
+      for (int mm = 0; mm < 4; ++mm) {
+        const int oo = c32_incoming[dir][mm] - 1;
+#pragma unroll
+        for (int v = 0; v < VPL; ++v) fv[mm][v] = 0.f;
+        ld32<VPL>(a.h32 + hidx(n1, oo, Nc8, lf), nv[mm]);
+        const float *fp = far_ptr(code, oo);
+        if (fp) ld32<VPL>(fp, fv[mm]);
+      }
+      float ext[4][VPL];
+#pragma unroll
+      for (int mm = 0; mm < 4; ++mm) {
+        const int oo = c32_incoming[dir][mm] - 1;
+#pragma unroll
+        for (int v = 0; v < VPL; ++v) ext[mm][v] = e1 * nv[mm][v] + e2 * fv[mm][v];
+        st32<VPL>(E + (size_t)(fi * 4 + mm) * Nc8 + lf, ext[mm]);
+        if (keep >> mm & 1) {
+          if (st == ST_F) st32<VPL>(a.h32 + hidx(node, oo, Nc8, lf), ext[mm]);
+          else st32<VPL>(a.fw32 + hidx(corner, oo, Nc8, lf), ext[mm]);
+        }
+      }
+#pragma unroll
+      for (int v = 0; v < VPL; ++v) {
+        const int l = lf + v;
+        const double ca = dir < 2 ? __ldg(a.cx + l) : dir < 4 ? __ldg(a.cy + l) : __ldg(a.cz + l);
+        racc += ca * (((double)ext[0][v] + (double)ext[1][v]) + (double)ext[2][v] + (double)ext[3][v]);
+      }
+    }
+    // segment sum in FP64 (the FP32 path does not keep the reference's summation order)
+    for (int off = LANES / 2; off > 0; off >>= 1) racc += __shfl_xor_sync(seg, racc, off, LANES);
+    if (fi == 0) rho0 = racc; else if (fi == 1) rho1 = racc; else rho2 = racc;
+  }
+  if (!lv) return;
+  const double r0 = rho0 / a.DiffFlux, r1 = rho1 / a.DiffFlux, r2 = rho2 / a.DiffFlux;
+  const double one_m = 1.0 - a.accom;
+  for (int k = 0; k < P.nwr; ++k) {
+    const float *sp = E + (size_t)P.src[k] * Nc8 + lf;
+    const double rf = P.face[k] == 0 ? r0 : P.face[k] == 1 ? r1 : r2;
+    float val[VPL];
+#pragma unroll
+    for (int v = 0; v < VPL; ++v) val[v] = (float)(a.accom * __ldg(a.w + lf + v) * rf + one_m * (double)sp[v]);
+    if (P.dst_store[k] == ST_F) st32<VPL>(a.h32 + hidx(node, P.dst_o[k], Nc8, lf), val);
+    else st32<VPL>(a.fw32 + hidx(corner, P.dst_o[k], Nc8, lf), val);
+  }
+}
+
 __global__ void k_inlet_outlet32(const DevState a, int gbuf) {
   const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (size_t)a.Ny * a.Nz * 4 * a.Nc8) return;
@@ -257,21 +342,24 @@ __global__ void k_symmetry32(const DevState a) {
   if (f & 8) { hp[4 * S] = hp[0 * S]; hp[5 * S] = hp[1 * S]; hp[6 * S] = hp[2 * S]; hp[7 * S] = hp[3 * S]; }
 }
 
-// Moments in FP64 from FP32 values: a warp per node, lanes over velocities, partial sums
-// combined with a warp reduction (the FP32 path does not follow the reference's order).
-template <int VPL>
+// Moments in FP64 from FP32 values: LANES lanes per node (32 / LANES nodes per warp), VPL
+// velocities per lane, partial sums combined with a segment reduction (the FP32 path does
+// not follow the reference's order). A whole warp per node measured fastest for 512
+// velocities (half a warp with 16-byte rows: 0.40 vs 0.37 ms on a 128^3 pack).
+template <int VPL, int LANES>
 __global__ void __launch_bounds__(256) k_moments32(const DevState a) {
-  const int node = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-  if (node >= a.NF) return;
-  const int lane = threadIdx.x & 31;
+  const int node = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) / LANES);
+  if (node >= a.NF) return;  // whole segment
+  const int lane = threadIdx.x % LANES;
+  const unsigned seg = LANES == 32 ? 0xffffffffu : (((1u << LANES) - 1u) << (threadIdx.x & 31 & ~(LANES - 1)));
   const int Nc8 = a.Nc8;
   const float *hp = a.h32 + (size_t)node * 8 * Nc8;
   double r = 0.0, ux = 0.0, uy = 0.0, uz = 0.0;
-  for (int l0 = lane * VPL; l0 < Nc8; l0 += 32 * VPL) {
+  for (int l0 = lane * VPL; l0 < Nc8; l0 += LANES * VPL) {
     float f[8][VPL];
 #pragma unroll
     for (int o = 0; o < 8; ++o) {
-      if (VPL == 2) {
+      if constexpr (VPL == 2) {
         const float2 t = __ldcs(reinterpret_cast<const float2 *>(hp + (size_t)o * Nc8 + l0));
         f[o][0] = t.x; f[o][VPL - 1] = t.y;
       } else {
@@ -289,11 +377,11 @@ __global__ void __launch_bounds__(256) k_moments32(const DevState a) {
       uz += __ldg(a.cz + l) * (((f1 + f2) + (f3 + f4)) - ((f5 + f6) + (f7 + f8)));
     }
   }
-  for (int off = 16; off > 0; off >>= 1) {
-    r += __shfl_down_sync(0xffffffffu, r, off);
-    ux += __shfl_down_sync(0xffffffffu, ux, off);
-    uy += __shfl_down_sync(0xffffffffu, uy, off);
-    uz += __shfl_down_sync(0xffffffffu, uz, off);
+  for (int off = LANES / 2; off > 0; off >>= 1) {
+    r += __shfl_down_sync(seg, r, off, LANES);
+    ux += __shfl_down_sync(seg, ux, off, LANES);
+    uy += __shfl_down_sync(seg, uy, off, LANES);
+    uz += __shfl_down_sync(seg, uz, off, LANES);
   }
   if (lane == 0) {
     double2 *mp = reinterpret_cast<double2 *>(a.mom) + 2 * (size_t)node;
@@ -328,6 +416,11 @@ void upload_tables_fp32() {
   cudaMemcpyToSymbol(c32_prog_of, prog_of, sizeof prog_of);
   cudaMemcpyToSymbol(c32_prog, progs, sizeof progs);
   cudaMemcpyToSymbol(c32_incoming, kIncoming, sizeof(int) * 24);
+  WPlan plans[26];
+  int ok = n == 26;
+  for (int i = 0; i < n; ++i) ok &= make_wall_plan(progs[i], plans[i]) ? 1 : 0;
+  g32_plan_ok = ok != 0;
+  cudaMemcpyToSymbol(c32_plan, plans, sizeof plans);
 }
 
 void launch_sweep_hyperplane32(const DevState &s, long t0, long ntask, cudaStream_t st) {
@@ -344,6 +437,22 @@ void launch_capture32(const DevState &s, int buf, cudaStream_t st) {
 void launch_walls32(const DevState &s, int begin, int end, int gbuf, cudaStream_t st) {
   if (end <= begin) return;
   const size_t walls = (size_t)(end - begin);
+  if (g32_plan_ok && (s.Nc8 == 64 || s.Nc8 <= 32)) {
+    static unsigned long long configured = 0;  // one bit per device
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!(configured >> (dev & 63) & 1ull)) {
+      cudaFuncSetAttribute(k_walls32_onchip<4, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 16 * 12 * 64 * 4);
+      configured |= 1ull << (dev & 63);
+    }
+    const size_t smem_per_wall = (size_t)12 * s.Nc8 * sizeof(float);
+    if (s.Nc8 == 64)
+      k_walls32_onchip<4, 16><<<nblocks(walls * 16, 256), 256, 16 * smem_per_wall, st>>>(s, begin, end, gbuf);
+    else if (s.Nc8 <= 8)
+      k_walls32_onchip<1, 8><<<nblocks(walls * 8, 256), 256, 32 * smem_per_wall, st>>>(s, begin, end, gbuf);
+    else k_walls32_onchip<1, 32><<<nblocks(walls * 32, 256), 256, 8 * smem_per_wall, st>>>(s, begin, end, gbuf);
+    return;
+  }
   if (s.Nc8 % 64 == 0) k_walls32<4, 16><<<nblocks(walls * 16, 256), 256, 0, st>>>(s, begin, end, gbuf);
   else if (s.Nc8 == 8) k_walls32<1, 8><<<nblocks(walls * 8, 256), 256, 0, st>>>(s, begin, end, gbuf);
   else k_walls32<1, 32><<<nblocks(walls * 32, 256), 256, 0, st>>>(s, begin, end, gbuf);
@@ -356,8 +465,8 @@ void launch_symmetry32(const DevState &s, cudaStream_t st) {
 }
 void launch_moments32(const DevState &s, cudaStream_t st) {
   if (!s.NF) return;
-  if (s.Nc8 % 2 == 0) k_moments32<2><<<nblocks((size_t)s.NF * 32, 256), 256, 0, st>>>(s);
-  else k_moments32<1><<<nblocks((size_t)s.NF * 32, 256), 256, 0, st>>>(s);
+  if (s.Nc8 % 2 == 0) k_moments32<2, 32><<<nblocks((size_t)s.NF * 32, 256), 256, 0, st>>>(s);
+  else k_moments32<1, 32><<<nblocks((size_t)s.NF * 32, 256), 256, 0, st>>>(s);
 }
 void launch_widen(const float *src, double *dst, size_t n, cudaStream_t st) {
   if (n) k_widen<<<148 * 16, 256, 0, st>>>(src, dst, n);

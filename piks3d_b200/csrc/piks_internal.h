@@ -42,6 +42,22 @@ struct WProg { int label, nface; WFace face[3]; int nwr; WWrite wr[12]; };
 const WProg *wall_program(int label);
 extern const int kIncoming[6][4];  // 1-based octants arriving from each fluid side
 
+// A wall program resolved for kernels that keep a wall's extrapolated values on chip:
+// every write's source is the extrapolation v(face, m) of one of the wall's faces, so a
+// write reads it from there; a face value is stored only where no write later replaces
+// it (the slot's final content is then the face value).
+struct WPlan {
+  int nface;
+  int dir[3], store[3];
+  int keep[3];        // per face: bit m set when v(face, m) is the final content of its slot
+  int nwr;
+  int dst_store[12], dst_o[12], face[12];  // 0-based destination octant
+  int src[12];        // producing face * 4 + m
+};
+// Resolves `p`; false if some write reads a value that is not a face extrapolation, reads
+// a slot that an earlier write replaced, or two writes share a destination.
+bool make_wall_plan(const WProg &p, WPlan &out);
+
 struct Velocity {
   int Nc_fundamental = 0, Nc = 0, Nc8 = 0;
   std::vector<double> cx, cy, cz, w;

@@ -212,3 +212,26 @@ def test_wall_programs_read_no_slot_an_earlier_write_stores():
         for dst_st, dst_o, fi, src_st, src_o in writes:
             assert (src_st, src_o) not in stored, lab
             stored.add((dst_st, dst_o))
+
+
+INCOMING = [(2, 3, 6, 7), (1, 4, 5, 8), (3, 4, 7, 8), (1, 2, 5, 6), (5, 6, 7, 8), (1, 2, 3, 4)]
+
+
+def test_wall_program_sources_are_face_values():
+    """The on-chip wall kernels take every re-emission source from the wall's own face
+    extrapolations and store a face value only where no write replaces it. Valid because,
+    in every program, each source (store, octant) is produced by exactly one face, and no
+    two writes share a destination."""
+    from device_model import wall_programs
+    progs = wall_programs()
+    assert len(progs) == 26
+    for lab, (faces, writes) in progs.items():
+        produced = {}
+        for fi, (d, st) in enumerate(faces):
+            for m, o in enumerate(INCOMING[d]):
+                produced.setdefault((st, o), []).append(fi * 4 + m)
+        dsts = [(w[0], w[1]) for w in writes]
+        assert len(set(dsts)) == len(dsts), lab
+        for dst_st, dst_o, fi, src_st, src_o in writes:
+            assert len(produced.get((src_st, src_o), [])) == 1, (lab, src_st, src_o)
+            assert dst_st != 1, lab  # writes go to the slots or the corner array
