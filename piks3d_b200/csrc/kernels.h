@@ -71,6 +71,8 @@ struct DevState {
 constexpr int kVtab = 29;
 void launch_sweep_hyperplane(const DevState &s, long t0, long ntask, cudaStream_t st);
 void launch_commit(const DevState &s, cudaStream_t st);
+// Wall-slot commits as 16-byte row copies (FP64 rows need an even Nc8, FP32 rows Nc8 % 4 == 0).
+void launch_commit_rows(const DevState &s, bool fp32, cudaStream_t st);
 void launch_capture(const DevState &s, int buf, cudaStream_t st);
 void launch_walls(const DevState &s, int begin, int end, int gbuf, cudaStream_t st);
 void launch_inlet_outlet(const DevState &s, int buf, cudaStream_t st);

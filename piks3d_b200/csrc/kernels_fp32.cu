@@ -429,6 +429,7 @@ void launch_sweep_hyperplane32(const DevState &s, long t0, long ntask, cudaStrea
   else k_sweep32<8, 1><<<nblocks((size_t)ntask * s.nchunk * 8, 256), 256, 0, st>>>(s, t0, ntask);
 }
 void launch_commit32(const DevState &s, cudaStream_t st) {
+  if (s.ncommit && s.Nc8 % 4 == 0) return launch_commit_rows(s, true, st);
   if (s.ncommit) k_commit32<<<nblocks((size_t)s.ncommit * s.Nc8, 256), 256, 0, st>>>(s);
 }
 void launch_capture32(const DevState &s, int buf, cudaStream_t st) {
