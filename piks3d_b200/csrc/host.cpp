@@ -15,6 +15,7 @@
 #include <fstream>
 #include <map>
 #include <sstream>
+#include <thread>
 
 #include "piks_internal.h"
 
@@ -594,39 +595,56 @@ piks_status preprocess(const Setup &s, const uint8_t *raw, int64_t nbytes, Geome
       if (src < 8) return n * 8 + src;
       return (int32_t)(1 << 30) | (g.bcorner[n - g.NF] * 8 + o);
     };
+    // one thread per octant: per-octant counts per hyperplane give every octant its own
+    // positions (within a hyperplane, octant by octant, voxels in raster order)
+    std::vector<std::vector<int64_t>> ocount(8, std::vector<int64_t>((size_t)nhyper, 0));
+    auto sweep_octant = [&](int o, int pass, std::vector<int64_t> *fillpos) {
+      const int sx = oct_sx(o), sy = oct_sy(o), sz = oct_sz(o);
+      for (int k = 1; k <= Nz; ++k)
+        for (int j = 1; j <= Ny; ++j)
+          for (int i = 1; i <= Nx; ++i) {
+            if (LAB(i, j, k) != L_FLUID) continue;
+            const int u = local(i, Nx, sx), v = local(j, Ny, sy), w = local(k, Nz, sz);
+            if (u < 1 || v < 1 || w < 1) continue;  // inflow planes are not swept
+            const int h = u + v + w - 3;
+            if (pass == 0) { ocount[(size_t)o][(size_t)h]++; continue; }
+            // first-order flags (physicalGrid.F90:1269-1298 and the seven sibling blocks)
+            const bool fx = (u == 1) || (face_mask(LAB(i - sx, j, k)) & (sx > 0 ? FACE_E : FACE_W));
+            const bool fy = (v == 1) || (face_mask(LAB(i, j - sy, k)) & (sy > 0 ? FACE_N : FACE_S));
+            const bool fz = (w == 1) || (face_mask(LAB(i, j, k - sz)) & (sz > 0 ? FACE_F : FACE_B));
+            int32_t *t = &g.tasks[(size_t)(*fillpos)[(size_t)h]++ * 8];
+            t[0] = g.nodemap[g.ghost_index(i, j, k)];
+            t[1] = o | (fx ? 8 : 0) | (fy ? 16 : 0) | (fz ? 32 : 0);
+            t[2] = upwind_code(i - sx, j, k, o, 0, false);
+            t[3] = upwind_code(i - 2 * sx, j, k, o, 1, fx);
+            t[4] = upwind_code(i, j - sy, k, o, 2, false);
+            t[5] = upwind_code(i, j - 2 * sy, k, o, 3, fy);
+            t[6] = upwind_code(i, j, k - sz, o, 4, false);
+            t[7] = upwind_code(i, j, k - 2 * sz, o, 5, fz);
+          }
+    };
+    std::vector<std::vector<int64_t>> fill(8);
     for (int pass = 0; pass < 2; ++pass) {
-      std::vector<int64_t> fillpos;
       if (pass == 1) {
         g.hyper_start.assign(nhyper + 1, 0);
-        for (int h = 0; h < nhyper; ++h) g.hyper_start[h + 1] = g.hyper_start[h] + count[h];
+        for (int h = 0; h < nhyper; ++h) {
+          count[h] = 0;
+          for (int o = 0; o < 8; ++o) count[h] += ocount[(size_t)o][(size_t)h];
+          g.hyper_start[h + 1] = g.hyper_start[h] + count[h];
+        }
         g.tasks.assign((size_t)g.hyper_start[nhyper] * 8, 0);
-        fillpos.assign(g.hyper_start.begin(), g.hyper_start.end() - 1);
+        for (int o = 0; o < 8; ++o) {
+          fill[(size_t)o].resize((size_t)nhyper);
+          for (int h = 0; h < nhyper; ++h) {
+            int64_t before = 0;
+            for (int o2 = 0; o2 < o; ++o2) before += ocount[(size_t)o2][(size_t)h];
+            fill[(size_t)o][(size_t)h] = g.hyper_start[h] + before;
+          }
+        }
       }
-      for (int o = 0; o < 8; ++o) {
-        const int sx = oct_sx(o), sy = oct_sy(o), sz = oct_sz(o);
-        for (int k = 1; k <= Nz; ++k)
-          for (int j = 1; j <= Ny; ++j)
-            for (int i = 1; i <= Nx; ++i) {
-              if (LAB(i, j, k) != L_FLUID) continue;
-              const int u = local(i, Nx, sx), v = local(j, Ny, sy), w = local(k, Nz, sz);
-              if (u < 1 || v < 1 || w < 1) continue;  // inflow planes are not swept
-              const int h = u + v + w - 3;
-              if (pass == 0) { count[h]++; continue; }
-              // first-order flags (physicalGrid.F90:1269-1298 and the seven sibling blocks)
-              const bool fx = (u == 1) || (face_mask(LAB(i - sx, j, k)) & (sx > 0 ? FACE_E : FACE_W));
-              const bool fy = (v == 1) || (face_mask(LAB(i, j - sy, k)) & (sy > 0 ? FACE_N : FACE_S));
-              const bool fz = (w == 1) || (face_mask(LAB(i, j, k - sz)) & (sz > 0 ? FACE_F : FACE_B));
-              int32_t *t = &g.tasks[(size_t)fillpos[h]++ * 8];
-              t[0] = g.nodemap[g.ghost_index(i, j, k)];
-              t[1] = o | (fx ? 8 : 0) | (fy ? 16 : 0) | (fz ? 32 : 0);
-              t[2] = upwind_code(i - sx, j, k, o, 0, false);
-              t[3] = upwind_code(i - 2 * sx, j, k, o, 1, fx);
-              t[4] = upwind_code(i, j - sy, k, o, 2, false);
-              t[5] = upwind_code(i, j - 2 * sy, k, o, 3, fy);
-              t[6] = upwind_code(i, j, k - sz, o, 4, false);
-              t[7] = upwind_code(i, j, k - 2 * sz, o, 5, fz);
-            }
-      }
+      std::vector<std::thread> th;
+      for (int o = 0; o < 8; ++o) th.emplace_back(sweep_octant, o, pass, &fill[(size_t)o]);
+      for (auto &t : th) t.join();
     }
   }
 

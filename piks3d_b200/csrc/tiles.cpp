@@ -1,10 +1,51 @@
 // Tile-wavefront schedule of the sweep tasks (TileJobs, declared in piks_internal.h).
 #include <algorithm>
 #include <numeric>
+#include <thread>
 
 #include "piks_internal.h"
 
 namespace piks {
+
+namespace {
+
+// Runs fn(begin, end) over [0, n) split into contiguous chunks on up to 16 threads.
+template <typename F>
+void parallel_chunks(int64_t n, F fn) {
+  unsigned hw = std::thread::hardware_concurrency();
+  int nt = (int)std::min<unsigned>(hw ? hw : 1, 16u);
+  if (n < 4096) nt = 1;
+  if (nt <= 1) { fn((int64_t)0, n); return; }
+  std::vector<std::thread> th;
+  th.reserve((size_t)nt);
+  for (int i = 0; i < nt; ++i) {
+    const int64_t b = n * i / nt, e = n * (i + 1) / nt;
+    th.emplace_back([=, &fn] { fn(b, e); });
+  }
+  for (auto &t : th) t.join();
+}
+
+// Row de-duplication inside one job: open addressing on the row index, cleared by a
+// generation count.
+struct RowSet {
+  std::vector<int64_t> key;
+  std::vector<int32_t> val, gen;
+  int32_t cur = 0;
+  unsigned mask = 0;
+  explicit RowSet(unsigned cap) : key(cap), val(cap), gen(cap, -1), mask(cap - 1) {}
+  void clear() { ++cur; }
+  // slot of `k`, inserting `next` if absent (then *added = true)
+  int32_t find_or_add(int64_t k, int32_t next, bool *added) {
+    unsigned h = (unsigned)((uint64_t)k * 0x9E3779B97F4A7C15ull >> 40) & mask;
+    for (;;) {
+      if (gen[h] != cur) { gen[h] = cur; key[h] = k; val[h] = next; *added = true; return next; }
+      if (key[h] == k) { *added = false; return val[h]; }
+      h = (h + 1) & mask;
+    }
+  }
+};
+
+}  // namespace
 
 bool build_tile_jobs(const Geometry &g, int TX, int TY, int TZ, int max_slots, TileJobs &tj) {
   tj = TileJobs{};
@@ -17,127 +58,179 @@ bool build_tile_jobs(const Geometry &g, int TX, int TY, int TZ, int max_slots, T
   const int ndiag = nTx + nTy + nTz - 2;
   const int64_t ntiles = (int64_t)nTx * nTy * nTz;
   const int64_t GX = g.GX, GXY = (int64_t)g.GX * g.GY;
-  const size_t ntask = g.tasks.size() / 8;
-  // job of every task: (diagonal, octant) and tile; local step inside the tile
-  std::vector<int32_t> dio(ntask);   // diagonal * 8 + octant
-  std::vector<int64_t> tile(ntask);
-  std::vector<uint16_t> step(ntask);
-  for (size_t t = 0; t < ntask; ++t) {
-    const int32_t *r = &g.tasks[t * 8];
-    const int node = r[0], o = r[1] & 7;
-    const int64_t gi = g.node_g[node];
-    const int x = (int)(gi % GX) - 2, y = (int)((gi / GX) % g.GY) - 2, z = (int)(gi / GXY) - 2;
-    const int a = x / TX, b = y / TY, c = z / TZ;
-    const int sx = oct_sx(o), sy = oct_sy(o), sz = oct_sz(o);
-    const int diag = (sx > 0 ? a : nTx - 1 - a) + (sy > 0 ? b : nTy - 1 - b) + (sz > 0 ? c : nTz - 1 - c);
-    const int xhi = std::min((a + 1) * TX, Nx) - 1, yhi = std::min((b + 1) * TY, Ny) - 1,
-              zhi = std::min((c + 1) * TZ, Nz) - 1;
-    const int u = sx > 0 ? x - a * TX : xhi - x;
-    const int v = sy > 0 ? y - b * TY : yhi - y;
-    const int w = sz > 0 ? z - c * TZ : zhi - z;
-    step[t] = (uint16_t)(u + v + w);
-    dio[t] = diag * 8 + o;
-    tile[t] = a + (int64_t)nTx * (b + (int64_t)nTy * c);
-  }
-  // stable counting sorts by step, then tile, then (diagonal, octant)
-  std::vector<int64_t> order(ntask), tmp(ntask);
-  std::iota(order.begin(), order.end(), (int64_t)0);
-  auto counting_sort = [&](int64_t nb, auto keyf) {
-    std::vector<int64_t> cnt((size_t)nb + 1, 0);
-    for (size_t q = 0; q < ntask; ++q) cnt[(size_t)keyf(order[q]) + 1]++;
-    for (int64_t k = 0; k < nb; ++k) cnt[(size_t)k + 1] += cnt[(size_t)k];
-    for (size_t q = 0; q < ntask; ++q) tmp[(size_t)cnt[(size_t)keyf(order[q])]++] = order[q];
-    order.swap(tmp);
+  const int64_t ntask = (int64_t)(g.tasks.size() / 8);
+  const int nsteps = tj.nsteps;
+  // (octant, tile) pair and local step of every task
+  std::vector<int32_t> pair_of((size_t)ntask);
+  std::vector<uint16_t> step((size_t)ntask);
+  parallel_chunks(ntask, [&](int64_t b, int64_t e) {
+    for (int64_t t = b; t < e; ++t) {
+      const int32_t *r = &g.tasks[(size_t)t * 8];
+      const int node = r[0], o = r[1] & 7;
+      const int64_t gi = g.node_g[(size_t)node];
+      const int x = (int)(gi % GX) - 2, y = (int)((gi / GX) % g.GY) - 2, z = (int)(gi / GXY) - 2;
+      const int a = x / TX, bb = y / TY, c = z / TZ;
+      const int xhi = std::min((a + 1) * TX, Nx) - 1, yhi = std::min((bb + 1) * TY, Ny) - 1,
+                zhi = std::min((c + 1) * TZ, Nz) - 1;
+      const int u = oct_sx(o) > 0 ? x - a * TX : xhi - x;
+      const int v = oct_sy(o) > 0 ? y - bb * TY : yhi - y;
+      const int w = oct_sz(o) > 0 ? z - c * TZ : zhi - z;
+      step[(size_t)t] = (uint16_t)(u + v + w);
+      pair_of[(size_t)t] = (int32_t)((int64_t)o * ntiles + a + (int64_t)nTx * (bb + (int64_t)nTy * c));
+    }
+  });
+  // jobs = non-empty pairs, ordered by (diagonal * 8 + octant), then tile (counting sort)
+  const int64_t npairs = ntiles * 8;
+  std::vector<int32_t> pair_tasks((size_t)npairs, 0);
+  for (int64_t t = 0; t < ntask; ++t) pair_tasks[(size_t)pair_of[(size_t)t]]++;
+  auto dio_of = [&](int64_t pr) {
+    const int o = (int)(pr / ntiles);
+    const int64_t tl = pr % ntiles;
+    const int a = (int)(tl % nTx), bb = (int)((tl / nTx) % nTy), c = (int)(tl / ((int64_t)nTx * nTy));
+    const int diag = (oct_sx(o) > 0 ? a : nTx - 1 - a) + (oct_sy(o) > 0 ? bb : nTy - 1 - bb) +
+                     (oct_sz(o) > 0 ? c : nTz - 1 - c);
+    return diag * 8 + o;
   };
-  counting_sort(tj.nsteps, [&](int64_t t) { return (int64_t)step[(size_t)t]; });
-  counting_sort(ntiles, [&](int64_t t) { return tile[(size_t)t]; });
-  counting_sort((int64_t)ndiag * 8, [&](int64_t t) { return (int64_t)dio[(size_t)t]; });
-  tmp.clear(); tmp.shrink_to_fit();
-  auto same_job = [&](int64_t a, int64_t b) { return dio[(size_t)a] == dio[(size_t)b] && tile[(size_t)a] == tile[(size_t)b]; };
+  std::vector<int64_t> dcnt((size_t)ndiag * 8 + 1, 0);
+  for (int64_t pr = 0; pr < npairs; ++pr)
+    if (pair_tasks[(size_t)pr]) dcnt[(size_t)dio_of(pr) + 1]++;
+  for (size_t k = 1; k < dcnt.size(); ++k) dcnt[k] += dcnt[k - 1];
+  const int32_t njobs = (int32_t)dcnt.back();
+  std::vector<int64_t> job_pair((size_t)njobs);
+  std::vector<int32_t> job_of_pair((size_t)npairs, -1);
+  {
+    // within one (diagonal, octant) the pairs of one octant come in tile order
+    std::vector<int64_t> pos(dcnt.begin(), dcnt.end() - 1);
+    for (int o = 0; o < 8; ++o)
+      for (int64_t tl = 0; tl < ntiles; ++tl) {
+        const int64_t pr = (int64_t)o * ntiles + tl;
+        if (!pair_tasks[(size_t)pr]) continue;
+        const int64_t j = pos[(size_t)dio_of(pr)]++;
+        job_pair[(size_t)j] = pr;
+        job_of_pair[(size_t)pr] = (int32_t)j;
+      }
+  }
+  // tasks in job order, then local step, then their original order (stable placement)
+  tj.task_begin.assign((size_t)njobs + 1, 0);
+  for (int32_t j = 0; j < njobs; ++j)
+    tj.task_begin[(size_t)j + 1] = tj.task_begin[(size_t)j] + pair_tasks[(size_t)job_pair[(size_t)j]];
+  std::vector<int32_t> jstep((size_t)njobs * nsteps + 1, 0);  // tasks per (job, step), then positions
+  for (int64_t t = 0; t < ntask; ++t)
+    jstep[(size_t)job_of_pair[(size_t)pair_of[(size_t)t]] * nsteps + step[(size_t)t]]++;
+  {
+    int64_t acc = 0;
+    for (size_t k = 0; k + 1 < jstep.size(); ++k) { const int32_t c = jstep[k]; jstep[k] = (int32_t)acc; acc += c; }
+  }
+  std::vector<int64_t> order((size_t)ntask);
+  for (int64_t t = 0; t < ntask; ++t)
+    order[(size_t)jstep[(size_t)job_of_pair[(size_t)pair_of[(size_t)t]] * nsteps + step[(size_t)t]]++] = t;
+  jstep.clear(); jstep.shrink_to_fit();
+  pair_of.clear(); pair_of.shrink_to_fit();
 
   const int64_t nrows_h = ((int64_t)g.NF + g.NB) * 8;
-  const int64_t nrows_all = nrows_h + (int64_t)g.nCorner * 8;
-  std::vector<int32_t> stamp((size_t)nrows_all, -1), slot_of((size_t)nrows_all, 0);
   auto row_index = [&](int32_t code) -> int64_t {
     return (code & (1 << 30)) ? nrows_h + (code & ~(1 << 30)) : (int64_t)code;
   };
-  tj.tasks.reserve(ntask * 4);
-  tj.rows.reserve(ntask * 2);
+  unsigned cap = 64;
+  while (cap < (unsigned)std::max(2 * max_slots, 64)) cap <<= 1;
+  // pass 1: rows (slots - 1) of every job
+  tj.row_count.assign((size_t)njobs, 0);
+  parallel_chunks(njobs, [&](int64_t jb, int64_t je) {
+    RowSet set(cap);
+    for (int64_t j = jb; j < je; ++j) {
+      set.clear();
+      const int64_t q = tj.task_begin[(size_t)j], e = tj.task_begin[(size_t)j + 1];
+      int32_t n = 0;
+      bool added;
+      for (int64_t p = q; p < e; ++p) {
+        const int32_t *r = &g.tasks[(size_t)order[(size_t)p] * 8];
+        set.find_or_add(r[0] * 8 + (r[1] & 7), n + 1, &added);
+        n += added;
+      }
+      for (int64_t p = q; p < e && n < max_slots; ++p) {
+        const int32_t *r = &g.tasks[(size_t)order[(size_t)p] * 8];
+        for (int k = 0; k < 6; ++k) {
+          const int32_t code = r[2 + k];
+          if (code < 0) continue;
+          set.find_or_add(row_index(code), n + 1, &added);
+          n += added;
+        }
+      }
+      tj.row_count[(size_t)j] = n;
+    }
+  });
+  for (int32_t j = 0; j < njobs; ++j)
+    if (tj.row_count[(size_t)j] + 1 > max_slots) return false;
+  tj.row_begin.assign((size_t)njobs + 1, 0);
+  for (int32_t j = 0; j < njobs; ++j)
+    tj.row_begin[(size_t)j + 1] = tj.row_begin[(size_t)j] + (tj.row_count[(size_t)j] + 3) / 4 * 4;
+  tj.rows.assign((size_t)tj.row_begin.back(), 0);
+  tj.tasks.assign((size_t)ntask * 4, 0);
+  tj.steps.assign((size_t)njobs * tj.steps_stride, 0);
+  // pass 2: rows (own rows first, in task order, then the others as first read), task
+  // records with slots, local step offsets
+  parallel_chunks(njobs, [&](int64_t jb, int64_t je) {
+    RowSet set(cap);
+    for (int64_t j = jb; j < je; ++j) {
+      set.clear();
+      const int64_t q = tj.task_begin[(size_t)j], e = tj.task_begin[(size_t)j + 1];
+      int32_t *rows = &tj.rows[(size_t)tj.row_begin[(size_t)j]];
+      int32_t n = 0;
+      bool added;
+      for (int64_t p = q; p < e; ++p) {
+        const int32_t *r = &g.tasks[(size_t)order[(size_t)p] * 8];
+        const int32_t own = r[0] * 8 + (r[1] & 7);
+        set.find_or_add(own, n + 1, &added);
+        if (added) rows[n++] = own;
+      }
+      for (int64_t p = q; p < e; ++p) {
+        const int32_t *r = &g.tasks[(size_t)order[(size_t)p] * 8];
+        int32_t sl[6];
+        for (int k = 0; k < 6; ++k) {
+          const int32_t code = r[2 + k];
+          if (code < 0) { sl[k] = 0; continue; }
+          sl[k] = set.find_or_add(row_index(code), n + 1, &added);
+          if (added) rows[n++] = code;
+        }
+        const int fl = r[1];
+        int32_t *tr = &tj.tasks[(size_t)p * 4];
+        tr[0] = r[0] | ((fl & 8) ? 1 << 27 : 0) | ((fl & 16) ? 1 << 28 : 0) | ((fl & 32) ? 1 << 29 : 0);
+        tr[1] = sl[0] | (sl[1] << 16);
+        tr[2] = sl[2] | (sl[3] << 16);
+        tr[3] = sl[4] | (sl[5] << 16);
+      }
+      uint16_t *st = &tj.steps[(size_t)j * tj.steps_stride];
+      for (int64_t p = q; p < e; ++p) st[step[(size_t)order[(size_t)p]] + 1]++;
+      for (int s2 = 0; s2 < nsteps; ++s2) st[s2 + 1] = (uint16_t)(st[s2 + 1] + st[s2]);
+    }
+  });
+  // per-diagonal bounds
   tj.diag_begin.assign((size_t)ndiag + 1, 0);
   tj.diag_rows.assign((size_t)ndiag, 0);
   tj.diag_tasks.assign((size_t)ndiag, 0);
-  int32_t njobs = 0;
-  std::vector<int64_t> job_tile;
-  std::vector<int8_t> job_oct;
-  size_t q = 0;
-  while (q < ntask) {
-    size_t e = q;
-    while (e < ntask && same_job(order[e], order[q])) ++e;
-    const int diag = dio[(size_t)order[q]] / 8;
-    job_tile.push_back(tile[(size_t)order[q]]);
-    job_oct.push_back((int8_t)(dio[(size_t)order[q]] % 8));
-    const int64_t rb = (int64_t)tj.rows.size();
-    tj.row_begin.push_back(rb);
-    tj.task_begin.push_back((int64_t)(tj.tasks.size() / 4));
-    for (size_t p = q; p < e; ++p) {  // own rows, in task order
-      const int32_t *r = &g.tasks[(size_t)order[p] * 8];
-      const int32_t own = r[0] * 8 + (r[1] & 7);
-      stamp[(size_t)own] = njobs;
-      slot_of[(size_t)own] = (int32_t)(1 + (p - q));
-      tj.rows.push_back(own);
-    }
-    for (size_t p = q; p < e; ++p) {
-      const int32_t *r = &g.tasks[(size_t)order[p] * 8];
-      int32_t sl[6];
-      for (int n = 0; n < 6; ++n) {
-        const int32_t code = r[2 + n];
-        if (code < 0) { sl[n] = 0; continue; }
-        const int64_t idx = row_index(code);
-        if (stamp[(size_t)idx] != njobs) {
-          stamp[(size_t)idx] = njobs;
-          slot_of[(size_t)idx] = (int32_t)(1 + ((int64_t)tj.rows.size() - rb));
-          tj.rows.push_back(code);
-        }
-        sl[n] = slot_of[(size_t)idx];
-      }
-      const int fl = r[1];
-      tj.tasks.push_back(r[0] | ((fl & 8) ? 1 << 27 : 0) | ((fl & 16) ? 1 << 28 : 0) | ((fl & 32) ? 1 << 29 : 0));
-      tj.tasks.push_back(sl[0] | (sl[1] << 16));
-      tj.tasks.push_back(sl[2] | (sl[3] << 16));
-      tj.tasks.push_back(sl[4] | (sl[5] << 16));
-    }
-    const int32_t nslots = (int32_t)(1 + ((int64_t)tj.rows.size() - rb));
-    if (nslots > max_slots) return false;
-    tj.row_count.push_back(nslots - 1);
-    while (tj.rows.size() % 4) tj.rows.push_back(0);
+  for (int32_t j = 0; j < njobs; ++j) {
+    const int diag = dio_of(job_pair[(size_t)j]) / 8;
+    const int32_t nslots = tj.row_count[(size_t)j] + 1;
+    const int32_t nt = (int32_t)(tj.task_begin[(size_t)j + 1] - tj.task_begin[(size_t)j]);
     tj.diag_rows[(size_t)diag] = std::max(tj.diag_rows[(size_t)diag], nslots);
-    tj.diag_tasks[(size_t)diag] = std::max(tj.diag_tasks[(size_t)diag], (int32_t)(e - q));
+    tj.diag_tasks[(size_t)diag] = std::max(tj.diag_tasks[(size_t)diag], nt);
     tj.max_rows = std::max(tj.max_rows, nslots);
-    tj.max_tasks = std::max(tj.max_tasks, (int32_t)(e - q));
-    // step offsets
-    const size_t sb = tj.steps.size();
-    tj.steps.resize(sb + (size_t)tj.steps_stride, 0);
-    for (size_t p = q; p < e; ++p) tj.steps[sb + step[order[p]] + 1]++;
-    for (int s = 0; s < tj.nsteps; ++s) tj.steps[sb + s + 1] = (uint16_t)(tj.steps[sb + s + 1] + tj.steps[sb + s]);
-    tj.diag_begin[(size_t)diag + 1] = njobs + 1;
-    ++njobs;
-    q = e;
+    tj.max_tasks = std::max(tj.max_tasks, nt);
+    tj.diag_begin[(size_t)diag + 1] = j + 1;
   }
-  tj.row_begin.push_back((int64_t)tj.rows.size());
-  tj.task_begin.push_back((int64_t)(tj.tasks.size() / 4));
   for (int d = 0; d < ndiag; ++d) tj.diag_begin[(size_t)d + 1] = std::max(tj.diag_begin[(size_t)d + 1], tj.diag_begin[(size_t)d]);
   // upstream jobs: the neighbour tiles on the upwind side of each axis, same octant
-  std::vector<int32_t> job_of((size_t)ntiles * 8, -1);
-  for (int32_t j = 0; j < njobs; ++j) job_of[(size_t)job_tile[(size_t)j] * 8 + job_oct[(size_t)j]] = j;
   tj.up.assign((size_t)njobs * 4, -1);
   for (int32_t j = 0; j < njobs; ++j) {
-    const int64_t t = job_tile[(size_t)j];
-    const int o = job_oct[(size_t)j];
+    const int64_t pr = job_pair[(size_t)j];
+    const int o = (int)(pr / ntiles);
+    const int64_t t = pr % ntiles;
     const int a = (int)(t % nTx), b = (int)((t / nTx) % nTy), c = (int)(t / ((int64_t)nTx * nTy));
     const int na = a - oct_sx(o), nb = b - oct_sy(o), nc = c - oct_sz(o);
-    if (na >= 0 && na < nTx) tj.up[(size_t)j * 4 + 0] = job_of[(size_t)(na + (int64_t)nTx * (b + (int64_t)nTy * c)) * 8 + o];
-    if (nb >= 0 && nb < nTy) tj.up[(size_t)j * 4 + 1] = job_of[(size_t)(a + (int64_t)nTx * (nb + (int64_t)nTy * c)) * 8 + o];
-    if (nc >= 0 && nc < nTz) tj.up[(size_t)j * 4 + 2] = job_of[(size_t)(a + (int64_t)nTx * (b + (int64_t)nTy * nc)) * 8 + o];
+    const int64_t base = (int64_t)o * ntiles;
+    if (na >= 0 && na < nTx) tj.up[(size_t)j * 4 + 0] = job_of_pair[(size_t)(base + na + (int64_t)nTx * (b + (int64_t)nTy * c))];
+    if (nb >= 0 && nb < nTy) tj.up[(size_t)j * 4 + 1] = job_of_pair[(size_t)(base + a + (int64_t)nTx * (nb + (int64_t)nTy * c))];
+    if (nc >= 0 && nc < nTz) tj.up[(size_t)j * 4 + 2] = job_of_pair[(size_t)(base + a + (int64_t)nTx * (b + (int64_t)nTy * nc))];
   }
   plan_tile_launches(tj, 1, 0.0);
   return true;
