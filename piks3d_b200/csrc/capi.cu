@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <future>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -72,7 +73,10 @@ piks_status zeros(piks_ctx *c, size_t n, T **out) {
   return PIKS_OK;
 }
 
+void drop_graphs(piks_ctx *c);
+
 void free_device(piks_ctx *c) {
+  drop_graphs(c);
   for (auto &a : c->allocations) cudaFree(a.first);
   c->allocations.clear();
   c->dev_bytes = 0;
@@ -171,7 +175,7 @@ void drain_timing(piks_ctx *c) {
 // The dataflow sweep's error flag: set when a dependency wait gave up (the values of that
 // sweep are then not the solver's).
 piks_status check_sweep_error(piks_ctx *c) {
-  if (!c->use_tiles || !c->ds.tv.err) return PIKS_OK;
+  if (!c->use_tiles || !c->ds.tv.err || !c->dataflow_used) return PIKS_OK;
   int e = 0;
   piks_status st = cuda_check(cudaMemcpyAsync(&e, c->ds.tv.err, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "err D2H");
   if (!st) st = cuda_check(cudaStreamSynchronize(c->stream), "err sync");
@@ -208,6 +212,7 @@ void enqueue_sweep(piks_ctx *c, cudaStream_t st, int n) {
   {
     Timed t(c, KT_SWEEP);
     if (c->use_tiles && c->schedule == PIKS_SCHED_TILE_DATAFLOW) {
+      c->dataflow_used = true;
       launch_tile_sweep_dataflow(s, f32, n, c->tiles.max_rows, c->tiles.max_tasks, st);
     } else if (c->use_tiles) {
       const auto &L = c->tiles.launches;
@@ -223,6 +228,13 @@ void enqueue_sweep(piks_ctx *c, cudaStream_t st, int n) {
   }
 }
 
+void drop_graphs(piks_ctx *c) {
+  for (auto &g : c->graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  c->graph_key = -1;
+  c->graph_warm = 0;
+}
+
 // One source iteration (solver.F90:111-1940) as a launch sequence on the context stream.
 void enqueue_iteration(piks_ctx *c) {
   const int n = c->iStep + 1;          // the iteration being run (1-based)
@@ -234,14 +246,34 @@ void enqueue_iteration(piks_ctx *c) {
 
 // Tile schedule of the context's tile_dims on the host (false: not usable, e.g. a job needs
 // more shared memory than a block has).
+// Shared-memory rows a tile job may use: what both precisions' sweep kernels can hold.
+int tile_slots(const piks_ctx *c, const int *dims) {
+  const int vox = dims[0] * dims[1] * dims[2];
+  const int nst = dims[0] + dims[1] + dims[2] - 2;
+  return std::min(tile_sweep_max_slots(c->vel.Nc8, false, vox, nst), tile_sweep_max_slots(c->vel.Nc8, true, vox, nst));
+}
+
+// Default tile shape of a precision, measured fastest on B200 for 512 velocities: 8x4x4
+// for the FP64 sweep, 4x4x4 for the FP32 sweep (whose CTAs carry twice the velocities per row).
+void default_tile_dims(int prec, int *dims) {
+  dims[0] = prec == PIKS_PREC_FP32 ? 4 : 8;
+  dims[1] = 4;
+  dims[2] = 4;
+}
+
+// Waits for a background tile build and drops its result.
+void drop_tiles_next(piks_ctx *c) {
+  if (c->tiles_next_ready.valid()) c->tiles_next_ready.wait();
+  c->tiles_next_ready = std::future<bool>();
+  c->tiles_next = TileJobs{};
+  c->tiles_next_dims[0] = c->tiles_next_dims[1] = c->tiles_next_dims[2] = 0;
+}
+
 bool build_tiles(piks_ctx *c) {
   c->use_tiles = false;
   c->tiles = TileJobs{};
   if (c->tile_dims[0] <= 0) return false;
-  const int vox = c->tile_dims[0] * c->tile_dims[1] * c->tile_dims[2];
-  const int nst = c->tile_dims[0] + c->tile_dims[1] + c->tile_dims[2] - 2;
-  const int slots = std::min(tile_sweep_max_slots(c->vel.Nc8, false, vox, nst),
-                             tile_sweep_max_slots(c->vel.Nc8, true, vox, nst));
+  const int slots = tile_slots(c, c->tile_dims);
   c->use_tiles = build_tile_jobs(c->geo, c->tile_dims[0], c->tile_dims[1], c->tile_dims[2], slots, c->tiles);
   if (!c->use_tiles) c->tiles = TileJobs{};
   return c->use_tiles;
@@ -388,18 +420,15 @@ piks_status piks_create(const piks_params *p, int32_t device, piks_ctx **out) {
 
 piks_status piks_setup_physical_grid(piks_ctx *c, const uint8_t *raw, int64_t nbytes) {
   if (!c) return fail(PIKS_ERR_ARG, "null context");
+  drop_tiles_next(c);
   if (c->device >= 0) { cudaSetDevice(c->device); free_device(c); }
   c->have_host_geometry = false;
   std::string err;
   piks_status st = preprocess(c->setup, raw, nbytes, c->geo, err);
   if (st) return fail(st, err);
   c->have_host_geometry = true;
-  if (!c->tiles_explicit) {
-    // measured fastest on B200 for 512 velocities: 8x4x4 tiles for the FP64 sweep, 4x4x4 for
-    // the FP32 sweep (whose CTAs carry twice the velocities per row)
-    const int d = c->prec == PIKS_PREC_FP32 ? 4 : 8;
-    c->tile_dims[0] = d; c->tile_dims[1] = 4; c->tile_dims[2] = 4;
-  }
+  c->tiles_tuned = false;
+  if (!c->tiles_explicit) default_tile_dims(c->prec, c->tile_dims);
   build_tiles(c);
   if (c->device < 0) return PIKS_OK;
   const Geometry &g = c->geo;
@@ -487,6 +516,15 @@ piks_status piks_setup_physical_grid(piks_ctx *c, const uint8_t *raw, int64_t nb
   c->have_geometry = true;
   c->version += 1;
   c->iStep = 0;
+  if (c->prec == PIKS_PREC_FP32 && c->use_tiles && !c->tiles_explicit) {
+    // a refined solve switches to FP64 later: its schedule is built meanwhile
+    default_tile_dims(PIKS_PREC_FP64, c->tiles_next_dims);
+    const int slots = tile_slots(c, c->tiles_next_dims);
+    c->tiles_next_ready = std::async(std::launch::async, [c, slots] {
+      return build_tile_jobs(c->geo, c->tiles_next_dims[0], c->tiles_next_dims[1], c->tiles_next_dims[2], slots,
+                             c->tiles_next);
+    });
+  }
   c->mass = 1.0;  // flow.F90:97
   c->error = 1.0;
   c->permeability = 0.0;
@@ -499,7 +537,46 @@ piks_status piks_iterate(piks_ctx *c, int32_t nsteps) {
   if (!c->have_geometry) return fail(PIKS_ERR_STATE, "piks_setup_physical_grid has not been called");
   if (nsteps < 0) return fail(PIKS_ERR_ARG, "nsteps < 0");
   cudaSetDevice(c->device);
-  for (int n = 0; n < nsteps; ++n) enqueue_iteration(c);
+  // The dataflow sweep takes the iteration number as its epoch and per-kernel timing records
+  // events, so both launch plainly; otherwise one graph launch per iteration replaces about
+  // a hundred kernel launches (the host would otherwise leave the GPU idle after every
+  // convergence check while it re-fills the stream).
+  const bool graphs = !c->graph_failed && !c->timing && !(c->use_tiles && c->schedule == PIKS_SCHED_TILE_DATAFLOW);
+  for (int n = 0; n < nsteps; ++n) {
+    if (!graphs) { enqueue_iteration(c); continue; }
+    const int key = c->version * 8 + c->schedule;
+    if (key != c->graph_key) { drop_graphs(c); c->graph_key = key; }
+    if (c->graph_warm < 2) { enqueue_iteration(c); ++c->graph_warm; continue; }
+    const int it = c->iStep + 1;
+    const int par = it & 1;
+    if (!c->graph[par]) {
+      if (!c->cap_stream && cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        c->graph_failed = true;
+        enqueue_iteration(c);
+        continue;
+      }
+      cudaGraph_t g = nullptr;
+      bool ok = cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+      if (ok) {
+        enqueue_sweep(c, c->cap_stream, it);
+        enqueue_boundaries_timed(c, c->cap_stream, it);
+        ok = cudaStreamEndCapture(c->cap_stream, &g) == cudaSuccess && g;
+      }
+      if (ok) ok = cudaGraphInstantiate(&c->graph[par], g, 0) == cudaSuccess;
+      if (g) cudaGraphDestroy(g);
+      if (!ok) {  // plain launches from here on
+        cudaGetLastError();
+        c->graph[par] = nullptr;
+        c->graph_failed = true;
+        enqueue_iteration(c);
+        continue;
+      }
+    }
+    piks_status st = cuda_check(cudaGraphLaunch(c->graph[par], c->stream), "iteration graph launch");
+    if (st) return st;
+    c->iStep = it;
+  }
   return cuda_check(cudaGetLastError(), "iterate launch");
 }
 
@@ -711,6 +788,30 @@ piks_status piks_run(piks_ctx *c, const char *results_path, const char *out_dir,
   return PIKS_OK;
 }
 
+// After a precision switch: the new precision's default tile shape, from the background
+// build when it made that shape, else built now (the schedule does not change any value).
+static piks_status retile_for_precision(piks_ctx *c) {
+  int d[3];
+  default_tile_dims(c->prec, d);
+  if (d[0] == c->tile_dims[0] && d[1] == c->tile_dims[1] && d[2] == c->tile_dims[2]) return PIKS_OK;
+  TileJobs tj;
+  bool ok = false;
+  if (c->tiles_next_ready.valid() && d[0] == c->tiles_next_dims[0] && d[1] == c->tiles_next_dims[1] &&
+      d[2] == c->tiles_next_dims[2]) {
+    ok = c->tiles_next_ready.get();
+    if (ok) tj = std::move(c->tiles_next);
+  } else {
+    ok = build_tile_jobs(c->geo, d[0], d[1], d[2], tile_slots(c, d), tj);
+  }
+  drop_tiles_next(c);
+  if (!ok) return PIKS_OK;  // keep the current schedule
+  c->tiles = std::move(tj);
+  c->tile_dims[0] = d[0]; c->tile_dims[1] = d[1]; c->tile_dims[2] = d[2];
+  piks_status st = upload_tiles(c);
+  if (!st) st = cuda_check(cudaStreamSynchronize(c->stream), "retile");
+  return st;
+}
+
 piks_status piks_set_precision(piks_ctx *c, int32_t precision) {
   if (!c) return fail(PIKS_ERR_ARG, "null context");
   if (precision != PIKS_PREC_FP64 && precision != PIKS_PREC_FP32) return fail(PIKS_ERR_ARG, "unknown precision");
@@ -741,6 +842,7 @@ piks_status piks_set_precision(piks_ctx *c, int32_t precision) {
   if (st) return st;
   free_state(c, c->prec);
   c->prec = precision;
+  if (c->use_tiles && !c->tiles_explicit && !c->tiles_tuned && (st = retile_for_precision(c))) return st;
   c->version += 1;
   return PIKS_OK;
 }
@@ -820,6 +922,7 @@ piks_status piks_autotune(piks_ctx *c, const int32_t *cand, int32_t ncand, int32
   build_tiles(c);
   if ((st = upload_tiles(c))) return st;
   c->schedule = k[3];
+  c->tiles_tuned = true;
   // the trial sweeps changed f: back to the state of setupFlow (all zero)
   const StateSizes z = state_sizes(c);
   DevState &s = c->ds;
@@ -981,11 +1084,13 @@ piks_status piks_synchronize(piks_ctx *c) {
 
 piks_status piks_destroy(piks_ctx *c) {
   if (!c) return PIKS_OK;
+  drop_tiles_next(c);
   if (c->device < 0) { delete c; return PIKS_OK; }
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
   for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
   free_device(c);
+  if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
   return PIKS_OK;

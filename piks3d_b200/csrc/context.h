@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <future>
 #include <string>
 #include <utility>
 #include <vector>
@@ -30,6 +31,12 @@ struct piks_ctx {
   int prec = PIKS_PREC_FP64;        // storage / sweep precision of the state
   int tile_dims[3] = {8, 4, 4};     // tile shape of the sweep schedule (0: per-node hyperplanes)
   bool tiles_explicit = false;      // set by piks_set_tiles; otherwise chosen by precision at setup
+  bool tiles_tuned = false;         // chosen by piks_autotune (kept across precision switches)
+  // the schedule of the other precision's default tile shape, built on a host thread while
+  // an FP32 state iterates (taken up by the switch to FP64)
+  piks::TileJobs tiles_next;
+  int tiles_next_dims[3] = {0, 0, 0};
+  std::future<bool> tiles_next_ready;
   piks::TileJobs tiles;
   bool use_tiles = false;           // tile schedule built and uploaded
   int schedule = PIKS_SCHED_TILE_DIAGONALS;
@@ -39,6 +46,13 @@ struct piks_ctx {
   bool timing = false;
   double kt_ms[piks::KT_N] = {0};
   int64_t kt_n[piks::KT_N] = {0};
+  // one iteration of each parity as a CUDA graph (tile diagonals, hyperplanes), valid for
+  // graph_key = version * 8 + schedule; the first two iterations after a change run plain
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  int graph_key = -1, graph_warm = 0;
+  bool graph_failed = false;
+  bool dataflow_used = false;       // a dataflow sweep ran (its error flag needs reading)
+  cudaStream_t cap_stream = nullptr;
   std::vector<cudaEvent_t> ev_pool;
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
   size_t ev_next = 0;

@@ -625,36 +625,50 @@ __global__ void __launch_bounds__(kMomWWarps * 32) k_moments_wide(const DevState
 // accumulates them serially. Runs over the plane in tiles of kFluxTile entries.
 constexpr int kFluxTile = 4096;
 __global__ void __launch_bounds__(256) k_flux(const DevState a, double ds, double sqrt_half, double inv_refl2) {
-  __shared__ double ux[kFluxTile];
+  __shared__ double tm[kFluxTile];
   __shared__ double part[9];
+  __shared__ int fg[10];
   __shared__ int gi_s;
   __shared__ double acc_s;
-  const int total = a.flux_groups[9];
+  if (threadIdx.x < 10) fg[threadIdx.x] = a.flux_groups[threadIdx.x];
   if (threadIdx.x == 0) { gi_s = 0; acc_s = 0.0; }
+  __syncthreads();
+  const int total = fg[9];
   for (int base = 0; base < total; base += kFluxTile) {
     const int cnt = min(kFluxTile, total - base);
-    __syncthreads();
+    // every entry's term (dx*dx*Ux, halved on the edges, quartered at the corners)
     for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
-      const int n = a.flux_list[base + e];
-      ux[e] = n >= 0 ? a.mom[4 * (size_t)n + 1] : 0.0;
+      const int idx = base + e;
+      const int n = a.flux_list[idx];
+      int g = 0;
+      while (g < 8 && idx >= fg[g + 1]) ++g;
+      double term = dmul(dmul(n >= 0 ? a.mom[4 * (size_t)n + 1] : 0.0, ds), ds);
+      if (g >= 1 && g <= 4) term = dmul(term, 0.5);
+      else if (g >= 5) term = dmul(term, 0.25);
+      tm[e] = term;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
+      // the serial sums in the reference's order, one group segment at a time
       int gi = gi_s;
       double s = acc_s;
-      for (int e = 0; e < cnt; ++e) {
-        const int idx = base + e;
-        while (idx >= a.flux_groups[gi + 1]) { part[gi] = s; ++gi; s = 0.0; }
-        double term = dmul(dmul(ux[e], ds), ds);
-        if (gi >= 1 && gi <= 4) term = dmul(term, 0.5);
-        else if (gi >= 5) term = dmul(term, 0.25);
-        s = gi <= 4 ? dadd(s, term) : term;
+      int idx = base;
+      const int end = base + cnt;
+      while (idx < end) {
+        while (idx >= fg[gi + 1]) { part[gi] = s; ++gi; s = 0.0; }
+        const int seg_end = min(end, fg[gi + 1]);
+        if (gi <= 4) {
+#pragma unroll 8
+          for (; idx < seg_end; ++idx) s = dadd(s, tm[idx - base]);
+        } else {
+          for (; idx < seg_end; ++idx) s = tm[idx - base];
+        }
       }
       gi_s = gi;
       acc_s = s;
     }
+    __syncthreads();
   }
-  __syncthreads();
   if (threadIdx.x == 0) {
     int gi = gi_s;
     double s = acc_s;

@@ -147,3 +147,25 @@ def test_fp32_tile_and_hyperplane_schedules_agree():
     err = np.abs(fa - fb).max() / np.abs(fb).max()
     print("fp32 tiles vs hyperplanes after 20 iterations: max rel diff %.3e, mass rel diff %.3e" % (err, _rel(ma, mb)))
     assert err <= 1e-5 and _rel(ma, mb) <= 1e-5
+
+
+def test_switch_to_fp64_takes_the_fp64_tile_shape():
+    """An FP32 state built with the default tiles (4x4x4) moves to the FP64 default shape
+    (8x4x4, built on a host thread meanwhile) when it switches to FP64; the FP64 values do
+    not depend on the schedule, so they equal those of a state that keeps 4x4x4 tiles."""
+    img = images.sphere_pack(16, 0.5, 1.5, 3.5, seed=1)
+    p = base_params(16, Nc_fundamental=4, Kn=0.5, fluidlayer=2)
+    out = []
+    for explicit in (False, True):
+        with pk.Solver(p, device=0) as s:
+            if explicit:
+                s.set_tiles(4, 4, 4)
+            s.set_precision(pk.PREC_FP32)
+            s.setup_physical_grid(img)
+            assert s.schedule()["TX"] == 4
+            s.iterate(6)
+            s.set_precision(pk.PREC_FP64)
+            assert s.schedule()["TX"] == (4 if explicit else 8)
+            s.iterate(5)
+            out.append((s.get_f()[0], s.chk_converge()))
+    assert np.array_equal(out[0][0], out[1][0]) and out[0][1] == out[1][1]

@@ -74,6 +74,29 @@ def test_iterations_bit_exact(name, make, kw, schedule):
     s.close()
 
 
+def test_graph_replay_equals_plain_launches():
+    """Iterations replayed from the per-parity CUDA graphs (the default) give the values of
+    plain launches (per-kernel timing on forces those), across a precision switch, which
+    re-captures the graphs, for the tile-diagonal and the per-node hyperplane schedules."""
+    img = images.sphere_pack(14, 0.5, 1.5, 3.5, seed=1)
+    p = base_params(14, Nc_fundamental=4, Kn=0.5, fluidlayer=2)
+    for tiles in ((4, 4, 4), (0, 0, 0)):
+        out = []
+        for timing in (True, False):
+            with pk.Solver(p, device=0) as s:
+                s.enable_timing(timing)
+                s.set_tiles(*tiles)
+                s.set_precision(pk.PREC_FP32)
+                s.setup_physical_grid(img)
+                s.iterate(7)
+                m32 = s.chk_converge()
+                s.set_precision(pk.PREC_FP64)
+                s.iterate(6)
+                out.append((s.get_f()[0], m32, s.chk_converge()))
+        (fa, m32a, ma), (fb, m32b, mb) = out
+        assert np.array_equal(fa, fb) and m32a == m32b and ma == mb, tiles
+
+
 def test_converged_permeability_sphere32():
     """32^3 box with a centred sphere of radius 12, 64 velocities, Kn = 1: the solve
     converges to the same permeability and step count as the oracle."""
