@@ -289,9 +289,17 @@ piks_status upload_tiles(piks_ctx *c) {
                         (const void *)tv.counter})
     if (p) release(c, const_cast<void *>(p));
   tv = TileView{};
-  if (!c->use_tiles) return PIKS_OK;
-  const TileJobs &tj = c->tiles;
   piks_status st;
+  if (!c->use_tiles) {
+    // the per-node hyperplane sweep reads the task list (uploaded once, only if needed)
+    if (!c->ds.tasks) {
+      int32_t *pt = nullptr;
+      if ((st = upload(c, c->geo.tasks, &pt))) return st;
+      c->ds.tasks = pt;
+    }
+    return PIKS_OK;
+  }
+  const TileJobs &tj = c->tiles;
   int32_t *pi = nullptr;
   int64_t *p64 = nullptr;
   uint16_t *p16 = nullptr;
@@ -499,7 +507,6 @@ piks_status piks_setup_physical_grid(piks_ctx *c, const uint8_t *raw, int64_t nb
       pv2 = pd;
       s.vtab2 = reinterpret_cast<const double2 *>(pv2);
     }
-    UP(g.tasks, tasks, pi);
   }
 #undef UP
   if ((st = upload_tiles(c))) return st;
