@@ -44,8 +44,8 @@ piks_status cuda_check(cudaError_t e, const char *what) {
 
 namespace {
 
-template <typename T>
-piks_status upload(piks_ctx *c, const std::vector<T> &v, T **out, size_t min_count = 1) {
+template <typename T, typename A>
+piks_status upload(piks_ctx *c, const std::vector<T, A> &v, T **out, size_t min_count = 1) {
   size_t n = v.size() < min_count ? min_count : v.size();
   void *p = nullptr;
   piks_status st = cuda_check(cudaMalloc(&p, n * sizeof(T)), "cudaMalloc");

@@ -632,7 +632,8 @@ piks_status preprocess(const Setup &s, const uint8_t *raw, int64_t nbytes, Geome
           for (int o = 0; o < 8; ++o) count[h] += ocount[(size_t)o][(size_t)h];
           g.hyper_start[h + 1] = g.hyper_start[h] + count[h];
         }
-        g.tasks.assign((size_t)g.hyper_start[nhyper] * 8, 0);
+        g.tasks.clear();
+        g.tasks.resize((size_t)g.hyper_start[nhyper] * 8);  // every entry is written below
         for (int o = 0; o < 8; ++o) {
           fill[(size_t)o].resize((size_t)nhyper);
           for (int h = 0; h < nhyper; ++h) {

@@ -1,12 +1,30 @@
 // Internal host-side structures of libpiks3d_b200 (not part of the C ABI).
 #pragma once
 #include <cstdint>
+#include <memory>
+#include <new>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "piks3d_gpu.h"
 
 namespace piks {
+
+// std::allocator that leaves new elements uninitialised: for the large host arrays that
+// are written in full right after they are sized (their pages are then first touched by
+// the threads that fill them).
+template <typename T>
+struct NoInitAlloc : std::allocator<T> {
+  template <typename U> struct rebind { using other = NoInitAlloc<U>; };
+  NoInitAlloc() = default;
+  template <typename U> NoInitAlloc(const NoInitAlloc<U> &) {}
+  template <typename U> void construct(U *p) noexcept { ::new (static_cast<void *>(p)) U; }
+  template <typename U, typename... A> void construct(U *p, A &&...a) {
+    ::new (static_cast<void *>(p)) U(std::forward<A>(a)...);
+  }
+};
+template <typename T> using BigVec = std::vector<T, NoInitAlloc<T>>;
 
 // Voxel labels of PIKS3D (physicalGrid.F90:127-134).
 enum : int {
@@ -99,7 +117,7 @@ struct Geometry {
   // Record (8 x int32): node, flags (octant | fx<<3 | fy<<4 | fz<<5), then the value
   // source of the x1, x2, y1, y2, z1, z2 upwind neighbours (row node*8+slot of h, or with
   // bit 30 set row corner*8+octant of fw, or -2 for a ghost that is only multiplied by 0).
-  std::vector<int32_t> tasks;
+  BigVec<int32_t> tasks;
   std::vector<int64_t> hyper_start;   // task offset of each hyperplane (+1 end entry)
   int32_t flux_groups[10] = {0};   // offsets of the 9 partial sums
   int64_t ghost_index(int i, int j, int k) const {
@@ -120,12 +138,12 @@ struct TileJobs {
   // in task order, then the other rows it reads; shared-memory slot = 1 + position
   // (slot 0 is a row of zeros)
   // (each job's list starts at a multiple of 4 entries, for 16-byte copies)
-  std::vector<int32_t> rows;
+  BigVec<int32_t> rows;
   std::vector<int64_t> row_begin;    // njobs + 1
   std::vector<int32_t> row_count;    // njobs
   // per task: node | fx<<27 | fy<<28 | fz<<29, then the slots of x1 | x2<<16, y1 | y2<<16,
   // z1 | z2<<16; the task's own slot is 1 + its index within the job
-  std::vector<int32_t> tasks;        // 4 int32 per task
+  BigVec<int32_t> tasks;             // 4 int32 per task
   std::vector<int64_t> task_begin;   // njobs + 1
   std::vector<uint16_t> steps;       // [njobs][steps_stride] task offsets within the job
   int steps_stride = 0;              // nsteps + 1 rounded up to a multiple of 8

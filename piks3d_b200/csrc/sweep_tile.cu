@@ -23,9 +23,10 @@ namespace piks {
 namespace {
 
 constexpr int kFwBit = 1 << 30;
-// Task groups per CTA (tasks of one local hyperplane in flight): 16 for FP64, 8 for FP32,
-// whose groups have twice the lanes (V = 32 velocities); both measured fastest on B200.
-template <typename T> constexpr int groups_of() { return sizeof(T) == 8 ? 16 : 8; }
+// Task groups per CTA (tasks of one local hyperplane in flight): 16 for FP64, 6 for FP32,
+// whose groups have twice the lanes (V = 32 velocities); both measured fastest on B200
+// (FP32 sweep of a 128^3 pack per iteration: 4 groups 2.76 ms, 6: 2.69, 8: 2.74, 12: 3.39).
+template <typename T> constexpr int groups_of() { return sizeof(T) == 8 ? 16 : 6; }
 template <typename T, int V> constexpr int threads_of() { return V / 2 * groups_of<T>(); }
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {

@@ -61,8 +61,8 @@ bool build_tile_jobs(const Geometry &g, int TX, int TY, int TZ, int max_slots, T
   const int64_t ntask = (int64_t)(g.tasks.size() / 8);
   const int nsteps = tj.nsteps;
   // (octant, tile) pair and local step of every task
-  std::vector<int32_t> pair_of((size_t)ntask);
-  std::vector<uint16_t> step((size_t)ntask);
+  BigVec<int32_t> pair_of((size_t)ntask);
+  BigVec<uint16_t> step((size_t)ntask);
   parallel_chunks(ntask, [&](int64_t b, int64_t e) {
     for (int64_t t = b; t < e; ++t) {
       const int32_t *r = &g.tasks[(size_t)t * 8];
@@ -121,7 +121,7 @@ bool build_tile_jobs(const Geometry &g, int TX, int TY, int TZ, int max_slots, T
     int64_t acc = 0;
     for (size_t k = 0; k + 1 < jstep.size(); ++k) { const int32_t c = jstep[k]; jstep[k] = (int32_t)acc; acc += c; }
   }
-  std::vector<int64_t> order((size_t)ntask);
+  BigVec<int64_t> order((size_t)ntask);
   for (int64_t t = 0; t < ntask; ++t)
     order[(size_t)jstep[(size_t)job_of_pair[(size_t)pair_of[(size_t)t]] * nsteps + step[(size_t)t]]++] = t;
   jstep.clear(); jstep.shrink_to_fit();
@@ -164,8 +164,8 @@ bool build_tile_jobs(const Geometry &g, int TX, int TY, int TZ, int max_slots, T
   tj.row_begin.assign((size_t)njobs + 1, 0);
   for (int32_t j = 0; j < njobs; ++j)
     tj.row_begin[(size_t)j + 1] = tj.row_begin[(size_t)j] + (tj.row_count[(size_t)j] + 3) / 4 * 4;
-  tj.rows.assign((size_t)tj.row_begin.back(), 0);
-  tj.tasks.assign((size_t)ntask * 4, 0);
+  tj.rows.resize((size_t)tj.row_begin.back());  // written below, padding included
+  tj.tasks.resize((size_t)ntask * 4);
   tj.steps.assign((size_t)njobs * tj.steps_stride, 0);
   // pass 2: rows (own rows first, in task order, then the others as first read), task
   // records with slots, local step offsets
@@ -199,6 +199,7 @@ bool build_tile_jobs(const Geometry &g, int TX, int TY, int TZ, int max_slots, T
         tr[2] = sl[2] | (sl[3] << 16);
         tr[3] = sl[4] | (sl[5] << 16);
       }
+      for (int32_t k = n; k < (int32_t)(tj.row_begin[(size_t)j + 1] - tj.row_begin[(size_t)j]); ++k) rows[k] = 0;
       uint16_t *st = &tj.steps[(size_t)j * tj.steps_stride];
       for (int64_t p = q; p < e; ++p) st[step[(size_t)order[(size_t)p]] + 1]++;
       for (int s2 = 0; s2 < nsteps; ++s2) st[s2 + 1] = (uint16_t)(st[s2 + 1] + st[s2]);
