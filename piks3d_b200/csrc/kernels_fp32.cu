@@ -390,6 +390,56 @@ __global__ void __launch_bounds__(256) k_moments32(const DevState a) {
   }
 }
 
+// The same sums for 64 velocities per octant, a warp over two nodes at a time: the sixteen
+// row loads of both nodes are in flight together (each node's sums as in k_moments32).
+__global__ void __launch_bounds__(256) k_moments32_pair(const DevState a) {
+  const int node0 = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 2;
+  if (node0 >= a.NF) return;  // whole warp
+  const int lane = threadIdx.x & 31;
+  const int l0 = lane * 2;
+  const bool two = node0 + 1 < a.NF;
+  float f[2][8][2];
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const float *hp = a.h32 + (size_t)(two ? node0 + k : node0) * 8 * 64;
+#pragma unroll
+    for (int o = 0; o < 8; ++o) {
+      const float2 t = __ldcs(reinterpret_cast<const float2 *>(hp + (size_t)o * 64 + l0));
+      f[k][o][0] = t.x; f[k][o][1] = t.y;
+    }
+  }
+  const double cx0 = __ldg(a.cx + l0), cx1 = __ldg(a.cx + l0 + 1), cy0 = __ldg(a.cy + l0), cy1 = __ldg(a.cy + l0 + 1),
+               cz0 = __ldg(a.cz + l0), cz1 = __ldg(a.cz + l0 + 1);
+  double acc[2][4];
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    double r = 0.0, ux = 0.0, uy = 0.0, uz = 0.0;
+#pragma unroll
+    for (int v = 0; v < 2; ++v) {
+      const double f1 = f[k][0][v], f2 = f[k][1][v], f3 = f[k][2][v], f4 = f[k][3][v], f5 = f[k][4][v],
+                   f6 = f[k][5][v], f7 = f[k][6][v], f8 = f[k][7][v];
+      r += ((f1 + f2) + (f3 + f4)) + ((f5 + f6) + (f7 + f8));
+      ux += (v ? cx1 : cx0) * (((f1 - f2) + (f4 - f3)) + ((f5 - f6) + (f8 - f7)));
+      uy += (v ? cy1 : cy0) * (((f1 + f2) - (f3 + f4)) + ((f5 + f6) - (f7 + f8)));
+      uz += (v ? cz1 : cz0) * (((f1 + f2) + (f3 + f4)) - ((f5 + f6) + (f7 + f8)));
+    }
+    acc[k][0] = r; acc[k][1] = ux; acc[k][2] = uy; acc[k][3] = uz;
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+    for (int k = 0; k < 2; ++k)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[k][q] += __shfl_down_sync(0xffffffffu, acc[k][q], off);
+  if (lane == 0) {
+    for (int k = 0; k < (two ? 2 : 1); ++k) {
+      double2 *mp = reinterpret_cast<double2 *>(a.mom) + 2 * (size_t)(node0 + k);
+      mp[0] = make_double2(acc[k][0], acc[k][1]);
+      mp[1] = make_double2(acc[k][2], acc[k][3]);
+    }
+  }
+}
+
 __global__ void k_widen(const float *src, double *dst, size_t n) {
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     dst[i] = (double)src[i];
@@ -466,7 +516,8 @@ void launch_symmetry32(const DevState &s, cudaStream_t st) {
 }
 void launch_moments32(const DevState &s, cudaStream_t st) {
   if (!s.NF) return;
-  if (s.Nc8 % 2 == 0) k_moments32<2, 32><<<nblocks((size_t)s.NF * 32, 256), 256, 0, st>>>(s);
+  if (s.Nc8 == 64) k_moments32_pair<<<nblocks((size_t)(s.NF + 1) / 2 * 32, 256), 256, 0, st>>>(s);
+  else if (s.Nc8 % 2 == 0) k_moments32<2, 32><<<nblocks((size_t)s.NF * 32, 256), 256, 0, st>>>(s);
   else k_moments32<1, 32><<<nblocks((size_t)s.NF * 32, 256), 256, 0, st>>>(s);
 }
 void launch_widen(const float *src, double *dst, size_t n, cudaStream_t st) {
