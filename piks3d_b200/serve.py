@@ -46,7 +46,10 @@ class Server:
         queue = collections.deque()
         done = []
         busy = 0.0
-        while incoming or queue or self.runner.active or self.runner.preparing:
+        def ended():  # jobs the runner finished without running them (refused, failed to prepare)
+            return bool(getattr(self.runner, "refused", ()))
+
+        while incoming or queue or self.runner.active or self.runner.preparing or ended():
             now = self.clock() - t0
             if self.horizon is not None and now > self.horizon:
                 break
@@ -54,7 +57,7 @@ class Server:
                 queue.append(incoming.popleft())
             while queue and self.runner.try_admit(queue[0], now):
                 queue.popleft()
-            if not self.runner.active and not self.runner.preparing:
+            if not self.runner.active and not self.runner.preparing and not ended():
                 if incoming:
                     self.sleep(max(0.0, min(0.05, incoming[0].arrival - now)))
                 continue
@@ -64,9 +67,12 @@ class Server:
                 done.append(job)
             busy += self.clock() - t1
         wall = self.clock() - t0
+        failed = [j for j in done if j.result is not None and ("refused" in j.result or "error" in j.result)]
+        done = [j for j in done if j not in failed]
         lat = [j.latency for j in done]
         return {
-            "requests": len(jobs), "completed": len(done), "unfinished": len(jobs) - len(done),
+            "requests": len(jobs), "completed": len(done), "refused_or_failed": len(failed),
+            "unfinished": len(jobs) - len(done) - len(failed),
             "wall_s": wall, "busy_s": busy, "solves_per_s": len(done) / wall if wall > 0 else 0.0,
             "latency_p50_s": percentile(lat, 50), "latency_p99_s": percentile(lat, 99),
             "latency_max_s": max(lat) if lat else None, "jobs": done,

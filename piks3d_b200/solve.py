@@ -37,11 +37,16 @@ class Convergence:
     the early transient of the source iteration or by rounding noise in the FP32 phase of a
     refined solve; the gate on the size of the changes keeps it from stopping where a fast
     mode and a slow mode of opposite sign cancel for a few checks (the mass flux passing
-    through a turning point looks converged there)."""
+    through a turning point looks converged there). A watchdog flags divergence (`diverged`)."""
 
     def __init__(self, eps=1e-8, tol=None, stall_checks=5, window=6, min_checks=8, consec=2, safety=0.5,
-                 maxres=0.35, gate=0.02, gate_run=3):
+                 maxres=0.35, gate=0.02, gate_run=3, blowup=1e6):
         self.eps, self.tol, self.stall_checks = eps, tol, stall_checks
+        # watchdog: a non-finite mass flux or error, or a mass flux `blowup` times the largest
+        # of the first checks, marks the iteration as diverged (the reference would run on to
+        # maxStep)
+        self.blowup = blowup
+        self.diverged = False
         self.window, self.min_checks, self.consec, self.safety, self.maxres = window, min_checks, consec, safety, maxres
         self.gate, self.gate_run = gate, gate_run
         self._gate_ok = 0
@@ -60,6 +65,10 @@ class Convergence:
 
     def update(self, mass, error):
         """Records one check; returns True when the solve has converged."""
+        if not (math.isfinite(mass) and math.isfinite(error)):
+            self.diverged = True
+        elif self.masses and abs(mass) > self.blowup * max(abs(m) for m in self.masses[:self.window]):
+            self.diverged = True
         self.masses.append(mass)
         if error < self.best:
             self.best, self.since_best = error, 0
@@ -143,9 +152,13 @@ def _prepare(job, device, precision):
     if job.image is None:
         job.image = job.make_image()
     s = Solver(job.params, device=device)
-    if precision in ("fp32", "refined"):
-        s.set_precision(PREC_FP32)
-    s.setup_physical_grid(job.image)
+    try:
+        if precision in ("fp32", "refined"):
+            s.set_precision(PREC_FP32)
+        s.setup_physical_grid(job.image)
+    except Exception:
+        s.close()
+        raise
     return s
 
 
@@ -171,6 +184,7 @@ class BatchRunner:
         self.batch = Batch(device=device)
         self.active = []
         self.preparing = []           # (job, future)
+        self.refused = []             # jobs finished without running (refused or failed to prepare)
         self.reserved = 0
 
     def close(self):
@@ -197,6 +211,14 @@ class BatchRunner:
         else:
             img = job.image
         fp = footprint_bytes(img, job.params, self.precision)
+        if fp > self.hbm_budget:
+            # can never fit, not even alone: refused rather than left to fail on allocation
+            job.footprint = 0
+            job.admitted = now
+            job.result = {"refused": "footprint %d bytes exceeds the HBM budget %d" % (fp, self.hbm_budget),
+                          "converged": False}
+            self.refused.append(job)
+            return True
         slots = len(self.active) + len(self.preparing)
         if slots >= self.max_members or (self.reserved + fp > self.hbm_budget and slots > 0):
             return False
@@ -210,7 +232,13 @@ class BatchRunner:
         still = []
         for job, fut in self.preparing:
             if block or fut.done():
-                job.solver = fut.result()
+                try:
+                    job.solver = fut.result()
+                except Exception as e:  # bad image, allocation failure: the job ends with the error
+                    job.result = {"error": "%s: %s" % (type(e).__name__, e), "converged": False}
+                    self.reserved -= job.footprint
+                    self.refused.append(job)
+                    continue
                 job.phase = "fp64" if self.precision == "fp64" else "fp32"
                 job.conv = self._new_conv(job)
                 self.batch.add(job.solver)
@@ -227,10 +255,14 @@ class BatchRunner:
 
     def step(self):
         """Admitted jobs that finished preprocessing join; one chkConvergeStep of iterations;
-        one check; finished jobs leave. Returns the jobs that finished."""
+        one check; finished jobs leave. Returns the jobs that finished (refused and failed
+        jobs included, with the reason in their result)."""
         self._join_ready(block=not self.active and bool(self.preparing))
+        ended, self.refused = self.refused, []
+        for job in ended:
+            job.finished = time.perf_counter()
         if not self.active:
-            return []
+            return ended
         chk = self._chk_step()
         self.batch.iterate(chk)
         mass, perm, err = self.batch.chk_converge()
@@ -248,14 +280,17 @@ class BatchRunner:
                 job.conv = self._new_conv(job)
                 job.conv.masses = [mass[i]]
                 continue
-            if conv or job.steps >= job.params.maxStep:
+            if conv or job.conv.diverged or job.steps >= job.params.maxStep:
                 job.result = {"steps": job.steps, "steps32": job.steps32, "mass": float(mass[i]),
                               "permeability": float(perm[i]), "error": float(err[i]),
-                              "converged": bool(conv), "estimate": job.conv.estimate}
+                              "converged": bool(conv), "diverged": job.conv.diverged,
+                              "estimate": job.conv.estimate}
                 if self.keep_fields:
                     job.result["macro"] = job.solver.get_macro()
                 done.append(job)
-        for job in done:
+        done_solved = list(done)
+        done = ended + done
+        for job in done_solved:
             self.batch.remove(job.solver)
             self.active.remove(job)
             job.solver.close()
@@ -269,7 +304,7 @@ class BatchRunner:
         t0 = time.perf_counter()
         pending = list(jobs)
         finished = []
-        while pending or self.active or self.preparing:
+        while pending or self.active or self.preparing or self.refused:
             now = time.perf_counter() - t0
             while pending and self.try_admit(pending[0], now):
                 pending.pop(0)
@@ -306,9 +341,9 @@ def solve_one(image, params, device=0, precision="fp64", tol=None, eps=None, swi
             conv = Convergence(eps=base_eps, tol=tol)
             conv.masses = [m]
             continue
-        if ok or steps >= params.maxStep:
+        if ok or conv.diverged or steps >= params.maxStep:
             res = {"steps": steps, "steps32": steps32, "mass": m, "permeability": k, "error": e,
-                   "converged": bool(ok), "estimate": conv.estimate}
+                   "converged": bool(ok), "diverged": conv.diverged, "estimate": conv.estimate}
             if keep_fields:
                 res["macro"] = s.get_macro()
             s.close()

@@ -154,3 +154,91 @@ def test_tolerance_rule_waits_past_a_turning_point():
     stop = next(k for k, m in enumerate(ms) if c.update(m, 1.0))
     assert abs(ms[stop] - ms[-1]) / abs(ms[-1]) <= 1e-4
     assert stop * 10 > 1000
+
+
+def test_watchdog_flags_non_finite_and_blowup():
+    c = Convergence(tol=1e-4)
+    for m in (1.0, 0.9, 0.85):
+        c.update(m, 0.1)
+    assert not c.diverged
+    c.update(float("nan"), float("nan"))
+    assert c.diverged
+    c = Convergence(eps=1e-8)
+    c.update(1e-2, 1.0)
+    c.update(5e-2, 1.0)
+    assert not c.diverged
+    c.update(1e5, 1.0)  # 1e7 times the first checks
+    assert c.diverged
+    c = Convergence(tol=1e-4)
+    for k in range(1, 200):
+        c.update(2.0 * (1.0 - 0.5 * 0.9 ** k), 0.1)
+    assert not c.diverged
+
+
+def _runner_without_gpu(budget):
+    """A BatchRunner whose admission and bookkeeping run without a device."""
+    from piks3d_b200.solve import BatchRunner
+    r = object.__new__(BatchRunner)
+    r.device, r.precision, r.tol, r.eps = 0, "refined", 1e-4, None
+    r.switch_eps, r.switch_change, r.max_members, r.keep_fields = 1e-6, 1e-6, 4, False
+    r.hbm_budget = budget
+    r.active, r.preparing, r.refused, r.reserved = [], [], [], 0
+    return r
+
+
+def test_admission_refuses_a_job_that_can_never_fit():
+    p = pk.default_params(Nx=64, Ny=64, Nz=64, Nc_fundamental=4)
+    img = np.zeros((64, 64, 64), np.uint8)
+    r = _runner_without_gpu(budget=footprint_bytes(img, p) // 2)
+    j = Job(img, p, name="big")
+    assert r.try_admit(j, 0.0)             # consumed from the queue ...
+    assert r.reserved == 0 and not r.preparing
+    assert "refused" in j.result and not j.result["converged"]
+    out = r.step()                         # ... and handed back as finished
+    assert out == [j] and j.finished is not None and r.refused == []
+
+
+def test_failed_preparation_ends_the_job_with_its_error():
+    import concurrent.futures as cf
+    p = pk.default_params(Nx=16, Ny=16, Nz=16, Nc_fundamental=2)
+    img = np.zeros((16, 16, 16), np.uint8)
+    r = _runner_without_gpu(budget=1 << 40)
+    j = Job(img, p, name="bad")
+    j.footprint = footprint_bytes(img, p)
+    r.reserved = j.footprint
+    fut = cf.Future()
+    fut.set_exception(pk.PiksError(3, "invalid image data file"))
+    r.preparing.append((j, fut))
+    out = r.step()
+    assert out == [j] and "error" in j.result and r.reserved == 0 and not r.active
+
+
+def test_server_reports_refused_jobs_apart():
+    clock = FakeClock()
+
+    class RefusingRunner(FakeRunner):
+        def __init__(self, clock):
+            super().__init__(clock, slots=2)
+            self.refused = []
+
+        def try_admit(self, job, now):
+            if job.name == "huge":
+                job.result = {"refused": "footprint", "converged": False}
+                self.refused.append(job)
+                return True
+            return super().try_admit(job, now)
+
+        def step(self):
+            ended, self.refused = self.refused, []
+            for j in ended:
+                j.finished = self.clock.t
+            return ended + super().step()
+
+    jobs = []
+    for i, name in enumerate(["a", "huge", "b"]):
+        j = Job(None, None, name=name, arrival=0.01 * i)
+        j.work = 2
+        jobs.append(j)
+    rep = Server(RefusingRunner(clock), clock=clock, sleep=clock.sleep).run(jobs)
+    assert rep["completed"] == 2 and rep["refused_or_failed"] == 1 and rep["unfinished"] == 0
+    assert sorted(j.name for j in rep["jobs"]) == ["a", "b"]
