@@ -140,6 +140,15 @@ piks_status piks_selftest_division(int32_t device, int64_t samples, uint64_t see
  * Has no counterpart in the reference, which has no device code. */
 piks_status piks_selftest_division_noalloc(int32_t device, int64_t samples, uint64_t seed, int64_t *mismatches);
 
+/* Self-test of the bounded waits of the dataflow sweep: runs one tile-dataflow sweep of
+ * the context in which one job waits on a flag that no job sets. Its wait gives up after
+ * its iteration limit (about a second), sets the sweep's error flag, and every job finishes;
+ * the call restores the schedule, clears the flag, and stores the sweep's duration in
+ * *seconds. Returns PIKS_OK when the wait ran out as designed, PIKS_ERR_STATE when it did not
+ * (or the context has no tile schedule). The sweep overwrites f with values that are not the
+ * solver's: set the image up again before iterating. Has no counterpart in the reference. */
+piks_status piks_selftest_wait_timeout(piks_ctx *ctx, double *seconds);
+
 /* Storage and sweep precision of a context. PIKS_PREC_FP64 (the default) is the
  * reference's arithmetic, operation for operation. PIKS_PREC_FP32 stores f, the 3-fold
  * corner slots and the x ghost planes in FP32 and sweeps in FP32, while the moments

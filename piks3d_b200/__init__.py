@@ -100,6 +100,7 @@ def load_library(path=LIB_PATH):
         "piks_batch_synchronize": (i32, [c_void_p]),
         "piks_batch_destroy": (i32, [c_void_p]),
         "piks_synchronize": (i32, [c_void_p]),
+        "piks_selftest_wait_timeout": (i32, [c_void_p, P(dbl)]),
         "piks_destroy": (i32, [c_void_p]),
         "piks_last_error": (ctypes.c_char_p, []),
     }
@@ -250,6 +251,14 @@ class Solver:
 
     def synchronize(self):
         _check(self.lib.piks_synchronize(self._ctx))
+
+    def selftest_wait_timeout(self):
+        """Runs one dataflow sweep in which a job waits on a flag nothing sets; returns the
+        sweep's duration (s) once the wait has given up as designed (piks_selftest_wait_timeout).
+        The state's values are not the solver's afterwards: set the image up again."""
+        sec = ctypes.c_double()
+        _check(self.lib.piks_selftest_wait_timeout(self._ctx, ctypes.byref(sec)))
+        return sec.value
 
     # -- data out -----------------------------------------------------------------------
     def info(self):

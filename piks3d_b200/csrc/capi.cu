@@ -316,7 +316,8 @@ piks_status upload_tiles(piks_ctx *c) {
 #undef UPT
   tv.njobs = (int)(tj.row_count.size());
   int *pw = nullptr;
-  if ((st = zeros(c, (size_t)tv.njobs * (size_t)(c->vel.Nc8 / 8 > 0 ? c->vel.Nc8 / 8 : 1), &pw))) return st;
+  // one more job's worth of flags than jobs: that job never publishes (wait self-test)
+  if ((st = zeros(c, (size_t)(tv.njobs + 1) * (size_t)(c->vel.Nc8 / 8 > 0 ? c->vel.Nc8 / 8 : 1), &pw))) return st;
   tv.flags = pw;
   if ((st = zeros(c, (size_t)2, &pw))) return st;
   tv.counter = pw;
@@ -1078,6 +1079,46 @@ piks_status piks_launches_per_iteration(piks_ctx *c, int64_t *n) {
   k += (s.ncommit > 0) + 1 /*capture*/ + (int64_t)(c->geo.level_start.size() - 1) + 1 /*inlet*/ +
        (s.nsym > 0) + (s.NF > 0);
   *n = k;
+  return PIKS_OK;
+}
+
+piks_status piks_selftest_wait_timeout(piks_ctx *c, double *seconds) {
+  if (!c || !seconds) return fail(PIKS_ERR_ARG, "null argument");
+  if (c->device < 0 || !c->have_geometry || !c->use_tiles || c->ds.tv.njobs < 1)
+    return fail(PIKS_ERR_STATE, "the wait self-test needs a device state with a tile schedule");
+  cudaSetDevice(c->device);
+  DevState &s = c->ds;
+  TileView &tv = s.tv;
+  // job 0's first upstream entry -> the job index njobs, whose flags nothing sets
+  int32_t *up = const_cast<int32_t *>(tv.up);
+  int32_t old_up = 0;
+  const int32_t never = tv.njobs;
+  piks_status st = cuda_check(cudaMemcpy(&old_up, up, sizeof(int32_t), cudaMemcpyDeviceToHost), "selftest up");
+  if (!st) st = cuda_check(cudaMemcpy(up, &never, sizeof(int32_t), cudaMemcpyHostToDevice), "selftest up");
+  if (st) return st;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  // a negative epoch: no flag of an earlier sweep holds it, and no later iteration uses it
+  static int calls = 0;
+  const int epoch = -(++calls);
+  const bool f32 = c->prec == PIKS_PREC_FP32;
+  cudaEventRecord(e0, c->stream);
+  launch_tile_sweep_dataflow(s, f32, epoch, c->tiles.max_rows, c->tiles.max_tasks, c->stream);
+  cudaEventRecord(e1, c->stream);
+  st = cuda_check(cudaStreamSynchronize(c->stream), "selftest sweep");
+  float ms = 0.f;
+  if (!st) cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  int err = 0;
+  if (!st) st = cuda_check(cudaMemcpy(&err, tv.err, sizeof(int), cudaMemcpyDeviceToHost), "selftest err");
+  // restore the schedule and clear the error flag in any case
+  cudaMemcpy(up, &old_up, sizeof(int32_t), cudaMemcpyHostToDevice);
+  cudaMemset(tv.err, 0, sizeof(int));
+  if (st) return st;
+  *seconds = ms * 1e-3;
+  if (!err) return fail(PIKS_ERR_STATE, "the dataflow wait did not give up");
   return PIKS_OK;
 }
 

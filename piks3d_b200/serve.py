@@ -67,7 +67,7 @@ class Server:
                 done.append(job)
             busy += self.clock() - t1
         wall = self.clock() - t0
-        failed = [j for j in done if j.result is not None and ("refused" in j.result or "error" in j.result)]
+        failed = [j for j in done if j.result is not None and ("refused" in j.result or "failed" in j.result)]
         done = [j for j in done if j not in failed]
         lat = [j.latency for j in done]
         return {

@@ -235,7 +235,7 @@ class BatchRunner:
                 try:
                     job.solver = fut.result()
                 except Exception as e:  # bad image, allocation failure: the job ends with the error
-                    job.result = {"error": "%s: %s" % (type(e).__name__, e), "converged": False}
+                    job.result = {"failed": "%s: %s" % (type(e).__name__, e), "converged": False}
                     self.reserved -= job.footprint
                     self.refused.append(job)
                     continue

@@ -210,7 +210,7 @@ def test_failed_preparation_ends_the_job_with_its_error():
     fut.set_exception(pk.PiksError(3, "invalid image data file"))
     r.preparing.append((j, fut))
     out = r.step()
-    assert out == [j] and "error" in j.result and r.reserved == 0 and not r.active
+    assert out == [j] and "failed" in j.result and r.reserved == 0 and not r.active
 
 
 def test_server_reports_refused_jobs_apart():
@@ -239,6 +239,8 @@ def test_server_reports_refused_jobs_apart():
         j = Job(None, None, name=name, arrival=0.01 * i)
         j.work = 2
         jobs.append(j)
+    for j in jobs:  # solved jobs carry the reference's error value in their result
+        j.result = {"error": 1e-9, "converged": True} if j.name != "huge" else None
     rep = Server(RefusingRunner(clock), clock=clock, sleep=clock.sleep).run(jobs)
     assert rep["completed"] == 2 and rep["refused_or_failed"] == 1 and rep["unfinished"] == 0
     assert sorted(j.name for j in rep["jobs"]) == ["a", "b"]
