@@ -182,3 +182,35 @@ def test_autotune_then_bit_exact():
     _compare_state(o, s, nodes)
     assert o.chk_converge() == s.chk_converge()
     s.close()
+
+
+@pytest.mark.parametrize("nf", [6, 8])
+def test_larger_velocity_sets_bit_exact(nf):
+    """6 and 8 abscissae per axis (216 and 512 velocities per octant): the sweep on rows of
+    other widths and the wall and moment kernels that loop over several velocity chunks,
+    for both schedules; FP64 bit for bit against the oracle, FP32 within 1e-5 of it."""
+    img = images.sphere_pack(10, 0.55, 1.2, 2.5, seed=4)
+    p = base_params(10, Nc_fundamental=nf, Kn=0.3, pressDrop=0.1, fluidlayer=1)
+    o = Oracle(p, img.tobytes(), nthreads=8)
+    o.iterate(3)
+    mo = o.chk_converge()
+    for tiles in ((4, 4, 4), (0, 0, 0)):
+        with pk.Solver(p, device=0) as s:
+            s.set_tiles(*tiles)
+            s.setup_physical_grid(img)
+            s.iterate(3)
+            nodes = s.geometry_array("node_g")
+            _compare_state(o, s, nodes)
+            assert s.chk_converge() == mo
+    with pk.Solver(p, device=0) as s:
+        s.set_precision(pk.PREC_FP32)
+        s.setup_physical_grid(img)
+        s.iterate(3)
+        m32 = s.chk_converge()[0]
+        nc8 = s.info()["Nc8"]
+        nodes = s.geometry_array("node_g")
+        fo = o.f().reshape(8, nc8, -1)[:, :, nodes]
+        fs = s.get_f()[0].reshape(8, nc8, -1)[:, :, nodes]
+        err = np.abs(fs - fo).max() / np.abs(fo).max()
+        print("Nc_fundamental %d: FP32 after 3 iterations max |f32 - f64| / max |f64| = %.3e" % (nf, err))
+        assert err <= 1e-5 and abs(m32 - mo[0]) / abs(mo[0]) <= 1e-5
