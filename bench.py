@@ -27,6 +27,7 @@ import json
 import os
 import statistics
 import subprocess
+import tempfile
 import sys
 import time
 
@@ -87,7 +88,10 @@ class ClockSampler:
     def __init__(self, gpu_index):
         self.gpu = gpu_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", "clocks_rank%d.csv" % gpu_index)
+        # raw samples go to $PIKS_CLOCKS_DIR (default: the temporary directory); the JSON line
+        # carries their summary
+        out = os.environ.get("PIKS_CLOCKS_DIR") or tempfile.gettempdir()
+        self.path = os.path.join(out, "clocks_rank%d.csv" % gpu_index)
 
     def start(self):
         try:

@@ -2,8 +2,8 @@
 
 The FP64 path evaluates every value with the oracle's operation order and rounding, so
 the distribution function, the moments and the mass flux must match the oracle bit for
-bit after each iteration (tolerance 0). Converged permeability must match within the
-1e-8 relative bound of the north-star (and is in fact identical).
+bit after each iteration (tolerance 0). Converged permeability must match within a
+relative 1e-8 (and is in fact identical).
 """
 import numpy as np
 import pytest
