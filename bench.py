@@ -98,10 +98,17 @@ class ClockSampler:
             os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.QUERY,
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=self.fh, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return
+        # wait (at most 5 s) until nvidia-smi writes, so that the timed region is sampled from
+        # its start; stop() reads only the lines written after this point
+        t0 = time.time()
+        while time.time() - t0 < 5.0 and os.path.getsize(self.path) == 0 and self.proc.poll() is None:
+            time.sleep(0.01)
+        self.offset = os.path.getsize(self.path)
 
     def stop(self):
         if self.proc is None:
@@ -114,7 +121,10 @@ class ClockSampler:
         self.fh.close()
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
+        with open(self.path) as fh:
+            fh.seek(getattr(self, "offset", 0))
+            lines = fh.read().splitlines()
+        for line in lines:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) < 9:
                 continue
