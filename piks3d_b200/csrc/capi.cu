@@ -1011,6 +1011,7 @@ piks_status piks_geometry_array(piks_ctx *c, const char *name, void *out, int64_
   ARR("tile_tasks", tj.tasks)
   ARR("tile_task_begin", tj.task_begin) ARR("tile_steps", tj.steps) ARR("tile_diag_begin", tj.diag_begin)
   ARR("tile_diag_rows", tj.diag_rows) ARR("tile_job_list", tj.job_list) ARR("tile_launches", tj.launches)
+  ARR("tile_up", tj.up)
 #undef ARR
   if (nm == "flux_groups") { src = g.flux_groups; n = 10; esz = sizeof(int32_t); }
   if (!esz) return fail(PIKS_ERR_ARG, "unknown geometry array " + nm);

@@ -235,3 +235,109 @@ def test_wall_program_sources_are_face_values():
         for dst_st, dst_o, fi, src_st, src_o in writes:
             assert len(produced.get((src_st, src_o), [])) == 1, (lab, src_st, src_o)
             assert dst_st != 1, lab  # writes go to the slots or the corner array
+
+
+def _tile_jobs_model(s, TX, TY, TZ):
+    """The tile schedule restated in Python from its contract: jobs are the non-empty
+    (tile, octant) pairs ordered by (tile diagonal of the octant's frame, octant, tile index);
+    a job's tasks are ordered by local hyperplane (step), then by their index in the per-node
+    task list; its rows are its own rows in task order, then every other row in the order
+    its tasks first read them (slot = 1 + position, 0 = the zero row); each job's row list is
+    padded with zeros to a multiple of 4; steps hold the task offset of each local
+    hyperplane; up holds the jobs of the upwind neighbour tiles (same octant) or -1."""
+    inf = s.info()
+    Nx, Ny, Nz = inf["Nx"], inf["Ny"], inf["Nz"]
+    GX, GY = Nx + 4, Ny + 4
+    t = s.geometry_array("tasks").reshape(-1, 8).astype(np.int64)
+    node_g = s.geometry_array("node_g").astype(np.int64)
+    nrows_h = inf["nNodes"] * 8
+    nTx, nTy, nTz = -(-Nx // TX), -(-Ny // TY), -(-Nz // TZ)
+    sx = lambda o: 1 if o in (0, 3, 4, 7) else -1
+    sy = lambda o: 1 if o in (0, 1, 4, 5) else -1
+    sz = lambda o: 1 if o < 4 else -1
+    keys = []
+    for i, r in enumerate(t):
+        o = int(r[1]) & 7
+        gi = int(node_g[r[0]])
+        x, y, z = gi % GX - 2, (gi // GX) % GY - 2, gi // (GX * GY) - 2
+        a, b, c = x // TX, y // TY, z // TZ
+        diag = (a if sx(o) > 0 else nTx - 1 - a) + (b if sy(o) > 0 else nTy - 1 - b) + (c if sz(o) > 0 else nTz - 1 - c)
+        u = x - a * TX if sx(o) > 0 else min((a + 1) * TX, Nx) - 1 - x
+        v = y - b * TY if sy(o) > 0 else min((b + 1) * TY, Ny) - 1 - y
+        w = z - c * TZ if sz(o) > 0 else min((c + 1) * TZ, Nz) - 1 - z
+        keys.append((diag * 8 + o, a + nTx * (b + nTy * c), u + v + w, i))
+    keys.sort()
+    nsteps = TX + TY + TZ - 2
+    stride = (nsteps + 1 + 7) // 8 * 8
+    ndiag = nTx + nTy + nTz - 2
+    rows, row_begin, row_count, tasks, task_begin, steps = [], [], [], [], [], []
+    diag_begin = [0] * (ndiag + 1)
+    job_of, job_key = {}, []
+    q = 0
+    while q < len(keys):
+        e = q
+        while e < len(keys) and keys[e][:2] == keys[q][:2]:
+            e += 1
+        j = len(row_begin)
+        dio, tile = keys[q][:2]
+        job_of[(tile, dio % 8)] = j
+        job_key.append((tile, dio % 8))
+        row_begin.append(len(rows))
+        task_begin.append(len(tasks) // 4)
+        slot, mine = {}, []
+        for k in range(q, e):
+            r = t[keys[k][3]]
+            own = int(r[0]) * 8 + (int(r[1]) & 7)
+            slot[own] = len(mine) + 1
+            mine.append(own)
+        for k in range(q, e):
+            r = t[keys[k][3]]
+            sl = []
+            for code in (int(x) for x in r[2:8]):
+                if code < 0:
+                    sl.append(0)
+                    continue
+                idx = nrows_h + (code & ~(1 << 30)) if code & (1 << 30) else code
+                if idx not in slot:
+                    slot[idx] = len(mine) + 1
+                    mine.append(code)
+                sl.append(slot[idx])
+            fl = int(r[1])
+            tasks += [int(r[0]) | (1 << 27 if fl & 8 else 0) | (1 << 28 if fl & 16 else 0) | (1 << 29 if fl & 32 else 0),
+                      sl[0] | sl[1] << 16, sl[2] | sl[3] << 16, sl[4] | sl[5] << 16]
+        row_count.append(len(mine))
+        rows += mine + [0] * (-len(mine) % 4)
+        st = [0] * stride
+        for k in range(q, e):
+            st[keys[k][2] + 1] += 1
+        for h in range(nsteps):
+            st[h + 1] += st[h]
+        steps += st
+        diag_begin[dio // 8 + 1] = j + 1
+        q = e
+    row_begin.append(len(rows))
+    task_begin.append(len(tasks) // 4)
+    for d in range(ndiag):
+        diag_begin[d + 1] = max(diag_begin[d + 1], diag_begin[d])
+    up = []
+    for tile, o in job_key:
+        a, b, c = tile % nTx, (tile // nTx) % nTy, tile // (nTx * nTy)
+        for na, nb, nc in ((a - sx(o), b, c), (a, b - sy(o), c), (a, b, c - sz(o))):
+            ok = 0 <= na < nTx and 0 <= nb < nTy and 0 <= nc < nTz
+            up.append(job_of.get((na + nTx * (nb + nTy * nc), o), -1) if ok else -1)
+        up.append(-1)
+    return dict(tile_rows=rows, tile_row_begin=row_begin, tile_row_count=row_count, tile_tasks=tasks,
+                tile_task_begin=task_begin, tile_steps=steps, tile_diag_begin=diag_begin, tile_up=up)
+
+
+@pytest.mark.parametrize("tiles,kw", [((4, 4, 4), {}), ((8, 4, 4), dict(fluidlayer=2)), ((4, 3, 5), dict(wallExtOrder=1))])
+def test_tile_jobs_match_their_contract(tiles, kw):
+    img = images.sphere_pack(14, 0.45, 1.5, 3.5, seed=5)
+    p = base_params(14, **kw)
+    s = pk.Solver(p, device=-1)
+    s.set_tiles(*tiles)
+    s.setup_physical_grid(img)
+    model = _tile_jobs_model(s, *tiles)
+    for name, want in model.items():
+        got = s.geometry_array(name)
+        assert np.array_equal(got.astype(np.int64), np.array(want, dtype=np.int64)), name
