@@ -341,3 +341,40 @@ def test_tile_jobs_match_their_contract(tiles, kw):
     for name, want in model.items():
         got = s.geometry_array(name)
         assert np.array_equal(got.astype(np.int64), np.array(want, dtype=np.int64)), name
+
+
+@pytest.mark.parametrize("n,kw", [(14, {}), (12, dict(fluidlayer=2)), (13, dict(block_repx=2))])
+def test_sweep_tasks_follow_their_order(n, kw):
+    """The per-node sweep tasks (generated one thread per octant) are ordered by the
+    hyperplane index u+v+w of their octant's frame, then by octant, then by voxel in raster
+    order; hyper_start gives each hyperplane's first task; every swept (fluid node, octant)
+    appears once."""
+    img = images.sphere_pack(n, 0.45, 1.5, 3.5, seed=11)
+    p = base_params(n, **kw)
+    s = pk.Solver(p, device=-1)
+    s.setup_physical_grid(img)
+    inf = s.info()
+    Nx, Ny, Nz = inf["Nx"], inf["Ny"], inf["Nz"]
+    GX, GY = Nx + 4, Ny + 4
+    t = s.geometry_array("tasks").reshape(-1, 8).astype(np.int64)
+    hs = s.geometry_array("hyper_start").astype(np.int64)
+    gi = s.geometry_array("node_g").astype(np.int64)[t[:, 0]]
+    i, j, k = gi % GX - 1, (gi // GX) % GY - 1, gi // (GX * GY) - 1   # 1-based voxel indices
+    o = t[:, 1] & 7
+    sx = np.where(np.isin(o, (0, 3, 4, 7)), 1, -1)
+    sy = np.where(np.isin(o, (0, 1, 4, 5)), 1, -1)
+    sz = np.where(o < 4, 1, -1)
+    u = np.where(sx > 0, i - 1, Nx - i)
+    v = np.where(sy > 0, j - 1, Ny - j)
+    w = np.where(sz > 0, k - 1, Nz - k)
+    assert np.all((u >= 1) & (v >= 1) & (w >= 1))     # inflow planes are not swept
+    h = u + v + w - 3
+    key = np.stack([h, o, gi], axis=1)
+    assert np.all(np.diff(key[:, 0]) >= 0)
+    same_h = np.diff(key[:, 0]) == 0
+    assert np.all(np.diff(key[:, 1])[same_h] >= 0)
+    same_ho = same_h & (np.diff(key[:, 1]) == 0)
+    assert np.all(np.diff(key[:, 2])[same_ho] > 0)
+    assert np.array_equal(hs[:-1], np.searchsorted(h, np.arange(len(hs) - 1)))
+    assert hs[-1] == len(t)
+    assert len(np.unique(t[:, 0] * 8 + o)) == len(t)
