@@ -85,3 +85,39 @@ def test_batch_chk_converge_matches_members():
         for s in ss:
             b.remove(s)
             s.close()
+
+
+def test_batch_with_216_velocity_members_equals_alone():
+    """Members with 216 velocities per octant (narrower sweep CTAs, several velocity chunks)
+    batched with 8- and 64-velocity members, FP32 and FP64: each equals its solo run."""
+    extra = [
+        (lambda: images.sphere_pack(10, 0.55, 1.2, 2.5, seed=4), dict(Nc_fundamental=6, Kn=0.3, pressDrop=0.1), pk.PREC_FP64),
+        (lambda: images.sphere_pack(10, 0.5, 1.2, 2.5, seed=8), dict(Nc_fundamental=6, Kn=0.5), pk.PREC_FP32),
+    ]
+
+    def solver(make, kw, prec):
+        img = make()
+        s = pk.Solver(base_params(img.shape[0], **kw), device=0)
+        s.set_precision(prec)
+        s.setup_physical_grid(img)
+        return s
+
+    members = [MEMBERS[0], MEMBERS[2]] + extra
+    alone = []
+    for m in members:
+        s = solver(*m)
+        s.iterate(6)
+        alone.append((s.get_f()[0], s.chk_converge()))
+        s.close()
+    with pk.Batch(device=0) as b:
+        ss = [solver(*m) for m in members]
+        for s in ss:
+            b.add(s)
+        b.iterate(6)
+        b.synchronize()
+        for k, s in enumerate(ss):
+            assert np.array_equal(s.get_f()[0], alone[k][0]), "member %d differs" % k
+            assert s.chk_converge()[:2] == alone[k][1][:2]
+        for s in ss:
+            b.remove(s)
+            s.close()

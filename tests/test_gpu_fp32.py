@@ -169,3 +169,17 @@ def test_switch_to_fp64_takes_the_fp64_tile_shape():
             s.iterate(5)
             out.append((s.get_f()[0], s.chk_converge()))
     assert np.array_equal(out[0][0], out[1][0]) and out[0][1] == out[1][1]
+
+
+def test_fp32_dataflow_216_velocities_matches_diagonals():
+    img = images.sphere_pack(10, 0.5, 1.2, 2.5, seed=8)
+    p = base_params(10, Nc_fundamental=6, Kn=0.5)
+    out = []
+    for sched in (pk.SCHED_TILE_DATAFLOW, pk.SCHED_TILE_DIAGONALS):
+        with pk.Solver(p, device=0) as s:
+            s.set_precision(pk.PREC_FP32)
+            s.set_schedule(sched)
+            s.setup_physical_grid(img)
+            s.iterate(5)
+            out.append((s.get_f()[0], s.chk_converge()))
+    assert np.array_equal(out[0][0], out[1][0]) and out[0][1] == out[1][1]
