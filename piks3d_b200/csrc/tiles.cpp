@@ -79,10 +79,23 @@ bool build_tile_jobs(const Geometry &g, int TX, int TY, int TZ, int max_slots, T
       pair_of[(size_t)t] = (int32_t)((int64_t)o * ntiles + a + (int64_t)nTx * (bb + (int64_t)nTy * c));
     }
   });
+  // The passes over all tasks below run one thread per octant: the pairs, jobs and output
+  // positions of different octants are disjoint, and each thread visits its tasks in order.
+  auto by_octant = [&](auto fn) {
+    if (ntask < 4096) { for (int o = 0; o < 8; ++o) fn((int64_t)o * ntiles, (int64_t)(o + 1) * ntiles); return; }
+    std::vector<std::thread> th;
+    for (int o = 0; o < 8; ++o) th.emplace_back([&fn, o, ntiles] { fn((int64_t)o * ntiles, (int64_t)(o + 1) * ntiles); });
+    for (auto &x : th) x.join();
+  };
   // jobs = non-empty pairs, ordered by (diagonal * 8 + octant), then tile (counting sort)
   const int64_t npairs = ntiles * 8;
   std::vector<int32_t> pair_tasks((size_t)npairs, 0);
-  for (int64_t t = 0; t < ntask; ++t) pair_tasks[(size_t)pair_of[(size_t)t]]++;
+  by_octant([&](int64_t lo, int64_t hi) {
+    for (int64_t t = 0; t < ntask; ++t) {
+      const int64_t pr = pair_of[(size_t)t];
+      if (pr >= lo && pr < hi) pair_tasks[(size_t)pr]++;
+    }
+  });
   auto dio_of = [&](int64_t pr) {
     const int o = (int)(pr / ntiles);
     const int64_t tl = pr % ntiles;
@@ -115,15 +128,23 @@ bool build_tile_jobs(const Geometry &g, int TX, int TY, int TZ, int max_slots, T
   for (int32_t j = 0; j < njobs; ++j)
     tj.task_begin[(size_t)j + 1] = tj.task_begin[(size_t)j] + pair_tasks[(size_t)job_pair[(size_t)j]];
   std::vector<int32_t> jstep((size_t)njobs * nsteps + 1, 0);  // tasks per (job, step), then positions
-  for (int64_t t = 0; t < ntask; ++t)
-    jstep[(size_t)job_of_pair[(size_t)pair_of[(size_t)t]] * nsteps + step[(size_t)t]]++;
+  by_octant([&](int64_t lo, int64_t hi) {
+    for (int64_t t = 0; t < ntask; ++t) {
+      const int64_t pr = pair_of[(size_t)t];
+      if (pr >= lo && pr < hi) jstep[(size_t)job_of_pair[(size_t)pr] * nsteps + step[(size_t)t]]++;
+    }
+  });
   {
     int64_t acc = 0;
     for (size_t k = 0; k + 1 < jstep.size(); ++k) { const int32_t c = jstep[k]; jstep[k] = (int32_t)acc; acc += c; }
   }
   BigVec<int64_t> order((size_t)ntask);
-  for (int64_t t = 0; t < ntask; ++t)
-    order[(size_t)jstep[(size_t)job_of_pair[(size_t)pair_of[(size_t)t]] * nsteps + step[(size_t)t]]++] = t;
+  by_octant([&](int64_t lo, int64_t hi) {
+    for (int64_t t = 0; t < ntask; ++t) {
+      const int64_t pr = pair_of[(size_t)t];
+      if (pr >= lo && pr < hi) order[(size_t)jstep[(size_t)job_of_pair[(size_t)pr] * nsteps + step[(size_t)t]]++] = t;
+    }
+  });
   jstep.clear(); jstep.shrink_to_fit();
   pair_of.clear(); pair_of.shrink_to_fit();
 
