@@ -12,7 +12,8 @@ Precision: a "refined" solve runs the FP32 sweep (FP64 moments, wall densities, 
 convergence test) until it meets the stopping rule or its mass flux changes by less than
 `switch_change` (relative) per check twice in a row (the FP32 iterate then sits near its
 rounding floor); it then widens its state to FP64 on the device and continues in FP64
-until the rule holds there.
+until the rule holds there. The FP64 phase runs the same iteration, so its rule starts from
+the contraction per check fitted in the FP32 phase instead of waiting for checks of its own.
 """
 import concurrent.futures as cf
 import math
@@ -40,8 +41,12 @@ class Convergence:
     through a turning point looks converged there). A watchdog flags divergence (`diverged`)."""
 
     def __init__(self, eps=1e-8, tol=None, stall_checks=5, window=6, min_checks=8, consec=2, safety=0.5,
-                 maxres=0.35, gate=0.02, gate_run=3, blowup=1e6):
+                 maxres=0.35, gate=0.02, gate_run=3, blowup=1e6, prior_r=None):
         self.eps, self.tol, self.stall_checks = eps, tol, stall_checks
+        # contraction per check already measured on the same iteration (the FP32 phase of a
+        # refined solve): until enough checks exist for a fit of its own, the estimate uses it
+        self.prior_r = prior_r
+        self.last_r = None            # contraction of the last fit that met the residual bound
         # watchdog: a non-finite mass flux or error, or a mass flux `blowup` times the largest
         # of the first checks, marks the iteration as diverged (the reference would run on to
         # maxStep)
@@ -78,7 +83,13 @@ class Convergence:
             return error <= self.eps
         w = self.window
         if len(self.masses) < max(w + 1, self.min_checks):
-            return False
+            if self.prior_r is None or len(self.masses) < 2:
+                return False
+            r = self.prior_r
+            self.estimate = self.last_change() * r / (1.0 - r)
+            self._ok_run = self._ok_run + 1 if self.estimate <= self.safety * self.tol else 0
+            self._gate_ok = self._gate_ok + 1 if self.last_change() <= self.gate * self.tol else 0
+            return self._ok_run >= self.consec and self._gate_ok >= self.gate_run
         m = self.masses
         d = np.array([abs(m[-w + i] - m[-w + i - 1]) / max(abs(m[-w + i]), 1e-300) for i in range(w)])
         if d[-1] == 0.0:
@@ -91,7 +102,10 @@ class Convergence:
             b, a = np.polyfit(x, y, 1)
             res = float(np.std(y - (a + b * x)))
             r = math.exp(b)
-            self.estimate = math.exp(a + b * (w - 1)) * r / (1.0 - r) if (r < 1.0 and res <= self.maxres) else math.inf
+            good = r < 1.0 and res <= self.maxres
+            if good:
+                self.last_r = r
+            self.estimate = math.exp(a + b * (w - 1)) * r / (1.0 - r) if good else math.inf
         self._ok_run = self._ok_run + 1 if self.estimate <= self.safety * self.tol else 0
         self._gate_ok = self._gate_ok + 1 if self.last_change() <= self.gate * self.tol else 0
         return self._ok_run >= self.consec and self._gate_ok >= self.gate_run
@@ -277,7 +291,9 @@ class BatchRunner:
                 # the FP64 phase continues from the widened FP32 iterate
                 job.solver.set_precision(PREC_FP64)
                 job.phase = "fp64"
+                prior = job.conv.last_r
                 job.conv = self._new_conv(job)
+                job.conv.prior_r = prior
                 job.conv.masses = [mass[i]]
                 continue
             if conv or job.conv.diverged or job.steps >= job.params.maxStep:
@@ -338,7 +354,7 @@ def solve_one(image, params, device=0, precision="fp64", tol=None, eps=None, swi
         if phase == "fp32" and precision == "refined" and (ok or small):
             s.set_precision(PREC_FP64)
             phase = "fp64"
-            conv = Convergence(eps=base_eps, tol=tol)
+            conv = Convergence(eps=base_eps, tol=tol, prior_r=conv.last_r)
             conv.masses = [m]
             continue
         if ok or conv.diverged or steps >= params.maxStep:

@@ -244,3 +244,32 @@ def test_server_reports_refused_jobs_apart():
     rep = Server(RefusingRunner(clock), clock=clock, sleep=clock.sleep).run(jobs)
     assert rep["completed"] == 2 and rep["refused_or_failed"] == 1 and rep["unfinished"] == 0
     assert sorted(j.name for j in rep["jobs"]) == ["a", "b"]
+
+
+def test_refinement_phase_uses_the_measured_contraction():
+    """After a switch (the FP32 iterate as the starting mass, a small jump, then the same
+    contraction), a rule given the contraction of the first phase stops within the tolerance,
+    and checks earlier than a rule that has to fit it again."""
+    r, tol = 0.8, 1e-4
+    limit = 2.0
+    first = Convergence(tol=tol)
+    k = 0
+    while True:
+        k += 1
+        m = limit * (1.0 + 3e-4 * r ** k)
+        if first.update(m, 0.1):
+            break
+    assert first.last_r is not None and abs(first.last_r - r) < 0.02
+    m32 = m * (1.0 + 1e-5)                  # the FP32 phase ends slightly off the FP64 limit path
+
+    def run(prior):
+        c = Convergence(tol=tol, prior_r=prior)
+        c.masses = [m32]
+        for j in range(1, 200):
+            mj = limit * (1.0 + 2e-5 * r ** j)
+            if c.update(mj, 0.1):
+                return j, mj
+    j_prior, m_prior = run(first.last_r)
+    j_fresh, m_fresh = run(None)
+    assert abs(m_prior - limit) / limit <= tol and abs(m_fresh - limit) / limit <= tol
+    assert j_prior < j_fresh
