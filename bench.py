@@ -8,11 +8,12 @@ tutorials: with second-order extrapolation the scheme diverges on packs with one
 channels). A step is one source iteration (8 octant sweeps, halo, walls, inlet/outlet,
 symmetry, moments).
 
-value: fluid voxel-velocity updates per second of the refined solver's iteration (FP32
-sweep, FP64 moments / wall densities / flux), whole job; the same for the plain FP64
-iteration is in "fp64". "solve": both solvers run to convergence at a 1e-4 permeability
-tolerance (solves/s, iterations, permeability difference, velocity-field difference);
-"e2e" is the refined solve through the public API, image upload to field download.
+value: fluid voxel-velocity updates per second of the plain FP64 iteration (the reference's
+arithmetic, operation for operation), whole job; the same for the refined solver's iteration
+(FP32 sweep, FP64 moments / wall densities / flux) is in "fp32". "solve": both solvers run to
+convergence at a 1e-4 permeability tolerance (solves/s, iterations, permeability difference,
+velocity-field difference); "e2e" is the plain FP64 solve through the public API, host image
+in to fields out ("solve.e2e_refined" the same for the refined solve).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--no-solve]
 
@@ -53,14 +54,31 @@ def workload_image():
     return images.sphere_pack(w["n"], w["porosity"], w["rmin"], w["rmax"], seed=w["seed"])
 
 
-def workload_params(pk):
+def workload_overrides():
     w = WORKLOAD
-    return pk.default_params(Nx=w["n"], Ny=w["n"], Nz=w["n"], Nc_fundamental=w["Nc_fundamental"],
-                             Kn=w["Kn"], pressDrop=1.0, eps=1e-8, chkConvergeStep=10, maxStep=20000,
-                             wallExtOrder=w["wallExtOrder"])
+    return dict(Nx=w["n"], Ny=w["n"], Nz=w["n"], Nc_fundamental=w["Nc_fundamental"], Kn=w["Kn"], pressDrop=1.0,
+                eps=1e-8, chkConvergeStep=10, maxStep=20000, wallExtOrder=w["wallExtOrder"])
 
 
-def config_dict(extra=None):
+def workload_params(pk):
+    return pk.default_params(**workload_overrides())
+
+
+# initParams' defaults (parameters.F90:91-98), as plain values: the reference arm hands these
+# to the oracle without loading the product library
+PARAM_DEFAULTS = dict(Nx=0, Ny=0, Nz=0, wallExtOrder=2, fluidlayer=0, Ref_L=1.0, Nc_fundamental=0, halfRange=1,
+                      mpi_xdim=1, mpi_ydim=1, mpi_zdim=1, block_repx=1, block_repy=1, block_repz=1, maxStep=1000,
+                      chkConvergeStep=10, saveStep=1 << 30, eps=1e-8, saveLast=1, saveFormat=1, Kn=0.0,
+                      pressDrop=0.0, accom=1.0)
+
+
+def workload_param_dict():
+    d = dict(PARAM_DEFAULTS)
+    d.update(workload_overrides())
+    return d
+
+
+def config_dict():
     w = WORKLOAD
     if w.get("kind") == "grf":
         name = "Gaussian random field %d^3 corr %g porosity %.2f (x-percolating cluster) seed %d, Nv=%d, Kn=%g, " \
@@ -72,9 +90,8 @@ def config_dict(extra=None):
             w["wallExtOrder"])
     d = {"workload": name,
          "image": "%dx%dx%d uint8" % (w["n"], w["n"], w["n"]), "velocities": 8 * w["Nc_fundamental"] ** 3,
-         "Kn": w["Kn"], "l2": "inputs larger than L2 (distribution function > 4 GB per rank)"}
-    if extra:
-        d.update(extra)
+         "Kn": w["Kn"], "l2": "inputs larger than L2 (distribution function > 4 GB per rank)",
+         "parallelism": "replicas (one independent solve per GPU)"}
     return d
 
 
@@ -192,18 +209,22 @@ def cpu_baseline(p, img, iters):
 
 
 def run_reference(args, world, rank):
-    import piks3d_b200 as pk
+    """The reference's algorithm on the host cores: the oracle (a line-by-line C++/OpenMP
+    restatement of the Fortran solver, which cannot be built here) on this workload, in
+    FP64. Loads only oracle/liboracle.so."""
     if rank != 0:
         return 0
     img = workload_image()
-    p = workload_params(pk)
+    p = workload_param_dict()
     iters = max(1, min(args.steps, 3))
     warm = 1
     cb = cpu_baseline(p, img, iters)
     line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": iters,
             "warmup": warm, "ms_per_step": cb["seconds_per_iteration"] * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": config_dict({"note": "each step is a bounded sample: the CPU run times %d iterations" % iters}),
+            "config": config_dict(),
+            "sample": "each step is a bounded sample: the CPU run times %d source iterations of the full "
+                      "workload after 1 warm-up" % iters,
             "impl": "reference", "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "gpu_launches": 0}
@@ -226,8 +247,9 @@ def swept_updates(s):
 
 
 def measure_iterations(pk, p, img, prec, args, world, local, device, clocks=None):
-    """K timed iterations (after W warm-up) of one precision with CUDA events on the
-    launching stream; per-kernel times from the library's own events."""
+    """K timed iterations (after W warm-up) of one precision, as a user runs them (iteration
+    graphs replayed), timed with CUDA events on the launching stream; then K more with the
+    library's per-kernel events for the breakdown and the sweep's own duration."""
     import torch
     s = pk.Solver(p, device=local)
     s.set_precision(prec)
@@ -241,8 +263,6 @@ def measure_iterations(pk, p, img, prec, args, world, local, device, clocks=None
     sweep_bytes = 2 * esz * nc8 * swept + 32 * nf     # f read + write per swept update, moments read once
     s.iterate(args.warmup)
     s.synchronize()
-    s.enable_timing(True)
-    s.kernel_times(reset=True)
     barrier(world, device)
     torch.cuda.synchronize()
     if clocks:
@@ -254,7 +274,13 @@ def measure_iterations(pk, p, img, prec, args, world, local, device, clocks=None
     ev1.record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop() if clocks else None
+    s.synchronize()
     ms_local = ev0.elapsed_time(ev1)
+    # per-kernel breakdown (plain launches with an event pair around each kernel group)
+    s.enable_timing(True)
+    s.kernel_times(reset=True)
+    s.iterate(args.steps)
+    s.synchronize()
     kt = s.kernel_times(reset=True)
     s.enable_timing(False)
     launches = s.launches_per_iteration() * args.steps
@@ -277,6 +303,16 @@ def traffic_per_update(precision):
         return None
 
 
+def roofline_of(m, hbm, peaks, tpu, nc8, kernel):
+    achieved = m["sweep_bytes"] / (m["sweep_ms"] * 1e-3) / 1e9
+    return {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+            "traffic": (tpu * m["swept"] * nc8) if tpu else None,
+            "kernel": kernel, "alg_bytes_per_iteration": m["sweep_bytes"],
+            "sweep_ms_per_iteration": m["sweep_ms"],
+            "peak_source": ("MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks
+                            else "fallback 6650 (of fallback)")}
+
+
 def run_ours(args, world, rank, local):
     import numpy as np
     import torch
@@ -288,15 +324,16 @@ def run_ours(args, world, rank, local):
     img = workload_image()
     p = workload_params(pk)
 
-    # --- device-resident iterations: value (refined solver's FP32 iteration), fp64, roofline
+    # --- device-resident iterations: value (plain FP64 iteration, the reference's arithmetic),
+    #     fp32 (the refined solver's FP32 iteration), rooflines of both sweeps
     clocks = ClockSampler(local)
-    m32 = measure_iterations(pk, p, img, pk.PREC_FP32, args, world, local, device, clocks)
-    m64 = measure_iterations(pk, p, img, pk.PREC_FP64, args, world, local, device)
-    info = m32["info"]
+    m64 = measure_iterations(pk, p, img, pk.PREC_FP64, args, world, local, device, clocks)
+    m32 = measure_iterations(pk, p, img, pk.PREC_FP32, args, world, local, device)
+    info = m64["info"]
     nf, nc8 = info["Nfluid"], info["Nc8"]
     nv = 8 * nc8
 
-    # --- full solves through the public API (image upload to field download) ------------------
+    # --- full solves through the public API (host image in, fields out) ------------------------
     solve = None
     e2e = None
     if not args.no_solve:
@@ -317,16 +354,23 @@ def run_ours(args, world, rank, local):
             "fp64": {**r64, "seconds": t64, "solves_per_s": world / t64},
             "refined": {**rrf, "seconds": trf, "solves_per_s": world / trf},
             "speedup_solves_per_s": t64 / trf,
+            "errors_measured_against": "the plain FP64 GPU solve of the same image and parameters, whose "
+                                       "iterations are bit-identical to the oracle's on this workload "
+                                       "(tests/test_gpu_parity.py::test_bench_workload_fp64_iterations_equal_oracle)",
             "perm_rel_diff_refined_vs_fp64": abs(rrf["permeability"] - r64["permeability"]) / abs(r64["permeability"]),
             "velocity_rel_l2_diff_refined_vs_fp64": (num / den) ** 0.5,
         }
         box = info["Nx"] * info["Ny"] * info["Nz"]
-        steps = rrf["steps"]
-        e2e = {"value": nf * nv * steps * world / trf / 1e9, "unit": UNIT,
-               "h2d_bytes_per_step": img.nbytes / steps,
-               "d2h_bytes_per_step": (8 * steps / p.chkConvergeStep + 4 * box * 8) / steps, "seconds": trf,
-               "what": "refined solve through the public API: create + setup_physical_grid(host image) + "
-                       "%d iterations with a check every %d + get_macro, wall clock" % (steps, p.chkConvergeStep)}
+
+        def e2e_of(r, t, what):
+            st = r["steps"]
+            return {"value": nf * nv * st * world / t / 1e9, "unit": UNIT,
+                    "h2d_bytes_per_step": img.nbytes / st,
+                    "d2h_bytes_per_step": (8 * st / p.chkConvergeStep + 4 * box * 8) / st, "seconds": t,
+                    "what": what + " solve through the public API: create + setup_physical_grid(host image) + "
+                            "%d iterations with a check every %d + get_macro, wall clock" % (st, p.chkConvergeStep)}
+        e2e = e2e_of(r64, t64, "plain FP64")
+        solve["e2e_refined"] = e2e_of(rrf, trf, "refined (FP32 sweep, FP64 refinement)")
 
     if rank != 0:
         return 0
@@ -336,32 +380,29 @@ def run_ours(args, world, rank, local):
     except Exception:
         pass
     hbm = peaks.get("hbm_gbs", 6650.0)
-    achieved = m32["sweep_bytes"] / (m32["sweep_ms"] * 1e-3) / 1e9
-    tpu = traffic_per_update("fp32")
+    per_it = lambda m: {k: v[0] / max(1, args.steps) for k, v in m["kt"].items()}
     line = {
-        "metric": METRIC, "value": m32["gupd"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": m32["ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32 sweep; f64 moments, wall densities, flux, convergence test",
-        "data": "synthetic",
-        "config": config_dict({"Nfluid": nf, "nWall": info["nWall"], "parallelism": "replicas x%d" % world,
-                               "schedule": m32["schedule"]}),
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": (tpu * m32["swept"] * nc8) if tpu else None,
-                     "kernel": "k_tile_sweep<float> (all launches of one iteration's sweep)",
-                     "alg_bytes_per_iteration": m32["sweep_bytes"],
-                     "peak_source": ("MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks
-                                     else "fallback 6650 (of fallback)")},
-        "kernel_ms_per_iteration": {k: v[0] / max(1, args.steps) for k, v in m32["kt"].items()},
-        "fp64": {"value": m64["gupd"], "unit": UNIT, "ms_per_step": m64["ms"] / args.steps,
-                 "kernel_ms_per_iteration": {k: v[0] / max(1, args.steps) for k, v in m64["kt"].items()},
-                 "sweep_frac_of_hbm": m64["sweep_bytes"] / (m64["sweep_ms"] * 1e-3) / 1e9 / hbm},
+        "metric": METRIC, "value": m64["gupd"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": m64["ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config_dict(),
+        "workload_info": {"Nfluid": nf, "nWall": info["nWall"], "replicas": world, "schedule_fp64": m64["schedule"],
+                          "schedule_fp32": m32["schedule"]},
+        "roofline": roofline_of(m64, hbm, peaks, traffic_per_update("fp64"), nc8,
+                                "FP64 octant sweep (all launches of one iteration's sweep)"),
+        "kernel_ms_per_iteration": per_it(m64),
+        "fp32": {"value": m32["gupd"], "unit": UNIT, "ms_per_step": m32["ms"] / args.steps,
+                 "what": "the refined solver's iteration: FP32 sweep, FP64 moments, wall densities and flux",
+                 "kernel_ms_per_iteration": per_it(m32),
+                 "roofline": roofline_of(m32, hbm, peaks, traffic_per_update("fp32"), nc8,
+                                         "FP32 octant sweep (all launches of one iteration's sweep)")},
         "solve": solve,
         "e2e": e2e,
-        "gpu_launches": m32["launches"],
-        "clocks": m32["clocks"],
+        "gpu_launches": m64["launches"],
+        "clocks": m64["clocks"],
     }
     if not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(p, img, args.cpu_iters)
+        line["cpu_baseline"] = cpu_baseline(workload_param_dict(), img, args.cpu_iters)
     print(json.dumps(line))
     return 0
 

@@ -105,6 +105,10 @@ piks_status piks_get_info(piks_ctx *ctx, int64_t *info, int32_t n);
  * voxels within two cells of fluid along an axis) are filled, the rest are 0. And fw. */
 piks_status piks_get_f(piks_ctx *ctx, double *f_ref, double *fw);
 
+/* f of n nodes (compact node indices, see the "node_g" geometry array for their voxels) as
+ * out[n][8][Nc8] (octant, then velocity), for sampled comparisons of large cases. */
+piks_status piks_get_f_nodes(piks_ctx *ctx, const int32_t *nodes, int32_t n, double *out);
+
 /* Host-side arrays of the preprocessed geometry by name ("label", "nodemap", "roles",
  * "commit", "wall_nb", ...), for inspection and tests; *count receives the element count,
  * out (capacity bytes) the data when not NULL. */
@@ -131,12 +135,16 @@ piks_status piks_selftest_division(int32_t device, int64_t samples, uint64_t see
  * it: a program that runs under a fixed device-memory budget, or that hands every device
  * allocation to its own pool and does not allow other allocators, can still check the
  * division. This entry point calls no allocator: its scratch is a static device buffer
- * compiled into the library (8 KB of per-block counts and a total, held on every GPU
- * that loads the library until the process exits). It accepts at most 16,777,216
- * samples and returns PIKS_ERR_ARG with a message above that. The first call on a device
- * looks up the buffer's device address, so make it before any stream capture. All calls
- * share the buffer: calls that overlap on the GPU race, so do not run two at once. Runs on
- * the default stream and returns after the result is on the host.
+ * compiled into the library (8 KB of per-block counts, a total and a count of the samples
+ * tested; held on every GPU that loads the library until the process exits). It accepts
+ * at most 16,777,216 samples and returns PIKS_ERR_ARG with a message above that. Each call
+ * looks up the buffer's device address on `device` (a lookup, not an allocation); the
+ * first lookup on a device can load the library's device code, so make the first call
+ * before any stream capture. All calls share the buffer: calls that overlap on the GPU
+ * race, so do not run two at once. The call clears the total first and returns
+ * PIKS_ERR_CUDA when a kernel failed to launch or did not test every sample, so a result
+ * always comes from this call. Runs on the default stream, returns after the result is on
+ * the host, and leaves the caller's current device as it found it.
  * Has no counterpart in the reference, which has no device code. */
 piks_status piks_selftest_division_noalloc(int32_t device, int64_t samples, uint64_t seed, int64_t *mismatches);
 

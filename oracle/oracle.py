@@ -55,6 +55,7 @@ def load():
         for name in ("oracle_get_extcoef", "oracle_get_f", "oracle_get_fw"):
             getattr(lib, name).argtypes = [ctypes.c_void_p, P(d)]
         lib.oracle_set_f.argtypes = [ctypes.c_void_p, P(d)]
+        lib.oracle_get_f_at.argtypes = [ctypes.c_void_p, P(i64), i32, P(d)]
         lib.oracle_get_macro.argtypes = [ctypes.c_void_p, P(d), P(d), P(d), P(d)]
         lib.oracle_get_dir.argtypes = [ctypes.c_void_p, ctypes.c_int, P(i32)]
         lib.oracle_get_coef.argtypes = [ctypes.c_void_p, ctypes.c_int, P(d)]
@@ -148,6 +149,14 @@ class Oracle:
         a = np.zeros(d["Ntotal"] * d["Nc8"] * 8)
         self.lib.oracle_get_f(self.h, _d(a))
         return a
+
+    def f_at(self, gidx):
+        """f of the voxels at 0-based ghosted linear indices gidx, as (n, 8, Nc8)."""
+        g = np.ascontiguousarray(gidx, dtype=np.int64)
+        n8 = self.dims()["Nc8"]
+        out = np.zeros((len(g), 8, n8))
+        self.lib.oracle_get_f_at(self.h, g.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), len(g), _d(out))
+        return out
 
     def set_f(self, a):
         a = np.ascontiguousarray(a, dtype=np.float64)

@@ -929,6 +929,16 @@ void oracle_get_mapf(void *h, int32_t *out) { auto *s = static_cast<Oracle *>(h)
 void oracle_get_extcoef(void *h, double *out) { auto *s = static_cast<Oracle *>(h); std::copy(s->extCoef.begin(), s->extCoef.end(), out); }
 void oracle_get_f(void *h, double *out) { auto *s = static_cast<Oracle *>(h); std::copy(s->f.begin(), s->f.end(), out); }
 void oracle_set_f(void *h, const double *in) { auto *s = static_cast<Oracle *>(h); std::copy(in, in + s->f.size(), s->f.begin()); }
+// f of n voxels (ghosted linear indices gidx) as out[n][8][Nc8]: rows of the reference layout
+// f(Ntotal, Nc8, 8) for sampled comparisons of large cases.
+void oracle_get_f_at(void *h, const int64_t *gidx, int32_t n, double *out) {
+  auto *s = static_cast<Oracle *>(h);
+  const size_t Ntot = s->f.size() / ((size_t)s->Nc8 * 8);
+  for (int32_t q = 0; q < n; ++q)
+    for (int o = 0; o < 8; ++o)
+      for (int l = 0; l < s->Nc8; ++l)
+        out[((size_t)q * 8 + o) * s->Nc8 + l] = s->f[(size_t)gidx[q] + (size_t)l * Ntot + (size_t)o * Ntot * s->Nc8];
+}
 void oracle_get_fw(void *h, double *out) { auto *s = static_cast<Oracle *>(h); std::copy(s->fw.begin(), s->fw.end(), out); }
 void oracle_get_macro(void *h, double *rho, double *ux, double *uy, double *uz) {
   auto *s = static_cast<Oracle *>(h);

@@ -73,6 +73,7 @@ void oracle_get_mapf(void *h, int32_t *out);         /* Nfluid local ids (1-base
 void oracle_get_extcoef(void *h, double *out);       /* nWall x 2, column-major */
 void oracle_get_f(void *h, double *out);             /* Ntotal x Nc8 x 8, column-major */
 void oracle_set_f(void *h, const double *in);
+void oracle_get_f_at(void *h, const int64_t *gidx, int32_t n, double *out); /* n x 8 x Nc8 rows at ghosted indices */
 void oracle_get_fw(void *h, double *out);            /* nCorner x Nc8 x 8 */
 void oracle_get_macro(void *h, double *rho, double *ux, double *uy, double *uz); /* Ntotal */
 void oracle_get_dir(void *h, int octant, int32_t *out);   /* 3 x Nstencil */

@@ -77,6 +77,7 @@ def load_library(path=LIB_PATH):
         "piks_get_labels": (i32, [c_void_p, P(i32)]),
         "piks_get_info": (i32, [c_void_p, P(i64), i32]),
         "piks_get_f": (i32, [c_void_p, P(dbl), P(dbl)]),
+        "piks_get_f_nodes": (i32, [c_void_p, P(i32), i32, P(dbl)]),
         "piks_geometry_array": (i32, [c_void_p, ctypes.c_char_p, c_void_p, i64, P(i64)]),
         "piks_set_stream": (i32, [c_void_p, c_void_p]),
         "piks_kernel_times": (i32, [c_void_p, P(dbl), i32, i32]),
@@ -290,6 +291,21 @@ class Solver:
         fw = np.zeros(max(1, inf["nCorner"]) * inf["Nc8"] * 8, dtype=np.float64)
         _check(self.lib.piks_get_f(self._ctx, _dptr(f), _dptr(fw)))
         return f, fw[: inf["nCorner"] * inf["Nc8"] * 8]
+
+    def get_fw(self):
+        """fw(nCorner, Nc8, 8) column-major, without the full-box f."""
+        inf = self.info()
+        fw = np.zeros(max(1, inf["nCorner"]) * inf["Nc8"] * 8, dtype=np.float64)
+        _check(self.lib.piks_get_f(self._ctx, None, _dptr(fw)))
+        return fw[: inf["nCorner"] * inf["Nc8"] * 8]
+
+    def get_f_nodes(self, nodes):
+        """f of the given compact nodes as (n, 8, Nc8) float64 (octant, then velocity)."""
+        nd = np.ascontiguousarray(nodes, dtype=np.int32)
+        out = np.zeros((len(nd), 8, self.info()["Nc8"]), dtype=np.float64)
+        _check(self.lib.piks_get_f_nodes(self._ctx, nd.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), len(nd),
+                                         _dptr(out)))
+        return out
 
     _GEO_DTYPES = {"label": np.uint8, "sym_flag": np.uint8, "roles": np.uint16, "wall_e": np.float64,
                    "hyper_start": np.int64, "tile_row_begin": np.int64, "tile_task_begin": np.int64,

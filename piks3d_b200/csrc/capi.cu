@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -699,6 +700,31 @@ piks_status piks_get_f(piks_ctx *c, double *f_ref, double *fw) {
   return PIKS_OK;
 }
 
+piks_status piks_get_f_nodes(piks_ctx *c, const int32_t *nodes, int32_t n, double *out) {
+  if (!c || !c->have_geometry) return fail(PIKS_ERR_STATE, "no geometry");
+  if (n < 0 || (n > 0 && (!nodes || !out))) return fail(PIKS_ERR_ARG, "bad node list");
+  cudaSetDevice(c->device);
+  const Geometry &g = c->geo;
+  const size_t row = (size_t)8 * c->vel.Nc8;
+  const bool f32 = c->prec == PIKS_PREC_FP32;
+  std::vector<float> t32(f32 ? row : 0);
+  for (int32_t q = 0; q < n; ++q) {
+    if (nodes[q] < 0 || (int64_t)nodes[q] >= (int64_t)g.NF + g.NB) return fail(PIKS_ERR_ARG, "node index out of range");
+    piks_status st;
+    if (f32) {
+      st = cuda_check(cudaMemcpyAsync(t32.data(), c->ds.h32 + (size_t)nodes[q] * row, row * sizeof(float),
+                                      cudaMemcpyDeviceToHost, c->stream), "f rows D2H");
+      if (!st) st = cuda_check(cudaStreamSynchronize(c->stream), "f rows sync");
+      if (!st) std::copy(t32.begin(), t32.end(), out + (size_t)q * row);
+    } else {
+      st = cuda_check(cudaMemcpyAsync(out + (size_t)q * row, c->ds.h + (size_t)nodes[q] * row, row * sizeof(double),
+                                      cudaMemcpyDeviceToHost, c->stream), "f rows D2H");
+    }
+    if (st) return st;
+  }
+  return cuda_check(cudaStreamSynchronize(c->stream), "f rows sync");
+}
+
 piks_status piks_save_fields(piks_ctx *c, const char *dir, int32_t format) {
   if (!c || !c->have_geometry) return fail(PIKS_ERR_STATE, "no geometry");
   const Geometry &g = c->geo;
@@ -1025,16 +1051,23 @@ piks_status piks_geometry_array(piks_ctx *c, const char *name, void *out, int64_
 
 piks_status piks_selftest_division(int32_t device, int64_t samples, uint64_t seed, int64_t *mismatches) {
   if (!mismatches || samples <= 0) return fail(PIKS_ERR_ARG, "bad argument");
+  int prev = -1;
+  if (cudaGetDevice(&prev) != cudaSuccess) { cudaGetLastError(); prev = -1; }
   piks_status st = cuda_check(cudaSetDevice(device), "cudaSetDevice");
   if (st) return st;
   unsigned long long *d = nullptr;
-  if ((st = cuda_check(cudaMalloc(&d, sizeof(unsigned long long)), "cudaMalloc"))) return st;
-  cudaMemset(d, 0, sizeof(unsigned long long));
-  launch_division_selftest(samples, seed, d);
-  unsigned long long h = 0;
-  st = cuda_check(cudaMemcpy(&h, d, sizeof h, cudaMemcpyDeviceToHost), "selftest");
-  cudaFree(d);
-  *mismatches = (int64_t)h;
+  if (!(st = cuda_check(cudaMalloc(&d, sizeof(unsigned long long)), "cudaMalloc"))) {
+    st = cuda_check(cudaMemset(d, 0, sizeof(unsigned long long)), "selftest memset");
+    if (!st) {
+      launch_division_selftest(samples, seed, d);
+      st = cuda_check(cudaGetLastError(), "selftest launch");
+    }
+    unsigned long long h = 0;
+    if (!st) st = cuda_check(cudaMemcpy(&h, d, sizeof h, cudaMemcpyDeviceToHost), "selftest");
+    cudaFree(d);
+    if (!st) *mismatches = (int64_t)h;
+  }
+  if (prev >= 0) cudaSetDevice(prev);
   return st;
 }
 
@@ -1101,7 +1134,7 @@ piks_status piks_selftest_wait_timeout(piks_ctx *c, double *seconds) {
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   // a negative epoch: no flag of an earlier sweep holds it, and no later iteration uses it
-  static int calls = 0;
+  static std::atomic<int> calls{0};
   const int epoch = -(++calls);
   const bool f32 = c->prec == PIKS_PREC_FP32;
   cudaEventRecord(e0, c->stream);

@@ -5,6 +5,11 @@
 // contracted and each value is rounded exactly as the CPU restatement rounds it.
 #include <cuda_runtime.h>
 
+#include <map>
+#include <mutex>
+#include <set>
+#include <tuple>
+
 #include "kernels.h"
 #include "piks_internal.h"
 
@@ -716,13 +721,14 @@ __global__ void k_division_selftest(int64_t samples, uint64_t seed, unsigned lon
 
 // ---------------------------------------------------------------------------------------
 // Allocation-free variant of the division self-test (piks_selftest_division_noalloc).
-// Its scratch is this file-scope device array: one mismatch count per block of the test
-// grid and a final total. Every GPU that loads the library holds it (8 KB + 8 bytes) until
-// the process exits; all calls share it and it keeps the last call's contents.
+// Its scratch is this file-scope device array: one count per block of the test grid, then
+// the total and the number of samples tested. Every GPU that loads the library holds it
+// (8 KB + 16 bytes) until the process exits; all calls share it and it keeps the last
+// call's contents.
 constexpr int kNoAllocBlocks = 1024;
 constexpr int kNoAllocThreads = 256;
 constexpr int64_t kNoAllocPerBlock = (int64_t)kNoAllocThreads * 64;   // samples per block
-static __device__ __align__(256) unsigned long long g_noalloc_scratch[kNoAllocBlocks + 1];
+static __device__ __align__(256) unsigned long long g_noalloc_scratch[kNoAllocBlocks + 2];
 
 __device__ __forceinline__ bool division_sample_differs(int64_t i, uint64_t seed) {
   const uint64_t r1 = splitmix64(seed ^ (uint64_t)(2 * i)), r2 = splitmix64(seed ^ (uint64_t)(2 * i + 1));
@@ -733,64 +739,129 @@ __device__ __forceinline__ bool division_sample_differs(int64_t i, uint64_t seed
   return __double_as_longlong(markstein_div(num, den, y)) != __double_as_longlong(__ddiv_rn(num, den));
 }
 
-// Each block counts the mismatches of its own sample range and writes its slot; no slot
-// is read before this launch writes it, so nothing has to be cleared between calls.
+// Each block counts the mismatches of its own sample range and writes its slot: the low 32
+// bits hold the mismatches, the high 32 bits the number of samples the block tested (at
+// most kNoAllocPerBlock each). The sum of the high halves is the call's completion count.
 __global__ void __launch_bounds__(kNoAllocThreads)
 k_division_selftest_blocks(int64_t samples, uint64_t seed, unsigned long long *partial) {
   __shared__ unsigned int warp_bad[kNoAllocThreads / 32];
+  __shared__ unsigned int warp_done[kNoAllocThreads / 32];
   const int64_t lo = (int64_t)blockIdx.x * kNoAllocPerBlock;
   const int64_t hi = min(samples, lo + kNoAllocPerBlock);
-  unsigned int bad = 0;
-  for (int64_t i = lo + threadIdx.x; i < hi; i += kNoAllocThreads) bad += division_sample_differs(i, seed) ? 1u : 0u;
-  for (int off = 16; off > 0; off >>= 1) bad += __shfl_down_sync(0xffffffffu, bad, off);
-  if ((threadIdx.x & 31) == 0) warp_bad[threadIdx.x >> 5] = bad;
+  unsigned int bad = 0, done = 0;
+  for (int64_t i = lo + threadIdx.x; i < hi; i += kNoAllocThreads) {
+    bad += division_sample_differs(i, seed) ? 1u : 0u;
+    ++done;
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    bad += __shfl_down_sync(0xffffffffu, bad, off);
+    done += __shfl_down_sync(0xffffffffu, done, off);
+  }
+  if ((threadIdx.x & 31) == 0) { warp_bad[threadIdx.x >> 5] = bad; warp_done[threadIdx.x >> 5] = done; }
   __syncthreads();
   if (threadIdx.x == 0) {
-    unsigned long long t = 0;
-    for (int w = 0; w < kNoAllocThreads / 32; ++w) t += warp_bad[w];
-    partial[blockIdx.x] = t;
+    unsigned long long b = 0, d = 0;
+    for (int w = 0; w < kNoAllocThreads / 32; ++w) { b += warp_bad[w]; d += warp_done[w]; }
+    partial[blockIdx.x] = b | (d << 32);
   }
 }
 
+// total = (sum of mismatches, sum of tested samples); both fit 32 bits at the sample limit.
 __global__ void k_sum_partials(const unsigned long long *partial, int n, unsigned long long *total) {
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    unsigned long long t = 0;
-    for (int b = 0; b < n; ++b) t += partial[b];
-    *total = t;
+    unsigned long long b = 0, d = 0;
+    for (int k = 0; k < n; ++k) { b += partial[k] & 0xffffffffull; d += partial[k] >> 32; }
+    total[0] = b;
+    total[1] = d;
   }
 }
 
+namespace {
+// Makes `device` current for the guard's lifetime and restores the caller's device after.
+struct DeviceGuard {
+  int prev = -1;
+  bool ok = false;
+  explicit DeviceGuard(int device) {
+    if (cudaGetDevice(&prev) != cudaSuccess) { cudaGetLastError(); prev = -1; }
+    ok = cudaSetDevice(device) == cudaSuccess;
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+}  // namespace
+
 int division_selftest_noalloc(int device, int64_t samples, uint64_t seed, int64_t *mismatches, const char **err) {
-  static unsigned long long *scratch_of_device[64] = {nullptr};
-  if (device < 0 || device >= 64) { *err = "device index out of range"; return 1; }
+  if (device < 0) { *err = "device index out of range"; return 1; }
   if (samples <= 0) { *err = "samples must be positive"; return 1; }
   const int64_t max_samples = (int64_t)kNoAllocBlocks * kNoAllocPerBlock;
   if (samples > max_samples) {
     *err = "samples exceeds 16777216, the most this allocation-free self-test runs with its static scratch";
     return 1;
   }
-  if (cudaSetDevice(device) != cudaSuccess) { *err = "cudaSetDevice failed"; return 4; }
-  if (!scratch_of_device[device]) {
-    // the host-side symbol is not a device address: look the device address up once per
-    // device, with that device current
-    void *ptr = nullptr;
-    if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) {
-      *err = "cudaGetSymbolAddress of the self-test scratch failed";
-      return 4;
-    }
-    scratch_of_device[device] = static_cast<unsigned long long *>(ptr);
-  }
-  unsigned long long *scratch = scratch_of_device[device];
-  const int blocks = (int)((samples + kNoAllocPerBlock - 1) / kNoAllocPerBlock);
-  k_division_selftest_blocks<<<blocks, kNoAllocThreads>>>(samples, seed, scratch);
-  k_sum_partials<<<1, 32>>>(scratch, blocks, scratch + kNoAllocBlocks);
-  unsigned long long total = 0;
-  if (cudaMemcpy(&total, scratch + kNoAllocBlocks, sizeof total, cudaMemcpyDeviceToHost) != cudaSuccess) {
-    *err = "self-test launch or copy failed";
+  DeviceGuard guard(device);
+  if (!guard.ok) { cudaGetLastError(); *err = "cudaSetDevice failed"; return 4; }
+  // The host-side name of the array is not a device address: look the address up on the
+  // current device on every call (a lookup, which allocates nothing). The first lookup on a
+  // device can load the library's device code, so make the first call before any capture.
+  void *ptr = nullptr;
+  if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) {
+    cudaGetLastError();
+    *err = "cudaGetSymbolAddress of the self-test scratch failed";
     return 4;
   }
-  *mismatches = (int64_t)total;
+  unsigned long long *scratch = static_cast<unsigned long long *>(ptr);
+  // the total and the completion count start at zero, so a stale total never comes back
+  if (cudaMemsetAsync(scratch + kNoAllocBlocks, 0, 2 * sizeof(unsigned long long), 0) != cudaSuccess) {
+    cudaGetLastError();
+    *err = "clearing the self-test total failed";
+    return 4;
+  }
+  const int blocks = (int)((samples + kNoAllocPerBlock - 1) / kNoAllocPerBlock);
+  k_division_selftest_blocks<<<blocks, kNoAllocThreads>>>(samples, seed, scratch);
+  if (cudaGetLastError() != cudaSuccess) { *err = "self-test kernel launch failed"; return 4; }
+  k_sum_partials<<<1, 32>>>(scratch, blocks, scratch + kNoAllocBlocks);
+  if (cudaGetLastError() != cudaSuccess) { *err = "self-test sum launch failed"; return 4; }
+  unsigned long long total[2] = {0, 0};
+  if (cudaMemcpy(total, scratch + kNoAllocBlocks, sizeof total, cudaMemcpyDeviceToHost) != cudaSuccess) {
+    cudaGetLastError();
+    *err = "self-test copy failed";
+    return 4;
+  }
+  if (total[1] != (unsigned long long)samples) {
+    *err = "self-test kernels did not test every sample";
+    return 4;
+  }
+  *mismatches = (int64_t)total[0];
   return 0;
+}
+
+namespace {
+std::mutex g_config_mu;
+std::set<std::pair<const void *, int>> g_configured;
+std::map<std::tuple<const void *, int, int, size_t>, long> g_resident;
+}  // namespace
+
+void once_per_device(const void *key, void (*configure)(int device)) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(g_config_mu);
+  if (g_configured.insert({key, dev}).second) configure(dev);
+}
+
+long resident_blocks(const void *fn, int threads, size_t smem) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(g_config_mu);
+  const auto key = std::make_tuple(fn, dev, threads, smem);
+  auto it = g_resident.find(key);
+  if (it != g_resident.end()) return it->second;
+  int nb = 0, nsm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, threads, smem) != cudaSuccess) { cudaGetLastError(); nb = 1; }
+  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) { cudaGetLastError(); nsm = 148; }
+  const long r = (long)(nb < 1 ? 1 : nb) * (nsm < 1 ? 1 : nsm);
+  g_resident[key] = r;
+  return r;
 }
 
 void launch_division_selftest(int64_t samples, uint64_t seed, unsigned long long *mismatches) {
@@ -863,14 +934,10 @@ void launch_symmetry(const DevState &s, cudaStream_t st) {
 
 void launch_moments(const DevState &s, cudaStream_t st) {
   if (s.NF == 0) return;
-  static unsigned long long configured = 0;  // one bit per device
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (!(configured >> (dev & 63) & 1ull)) {
+  once_per_device(reinterpret_cast<const void *>(k_moments), [](int) {
     cudaFuncSetAttribute(k_moments, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MomSmem));
     cudaFuncSetAttribute(k_moments_wide, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MomWSmem));
-    configured |= 1ull << (dev & 63);
-  }
+  });
   if (s.Nc8 % kMomWL == 0) {
     k_moments_wide<<<blocks_for((size_t)s.NF, kMomWWarps * 32), kMomWWarps * 32, sizeof(MomWSmem), st>>>(s);
     return;
@@ -881,15 +948,11 @@ void launch_moments(const DevState &s, cudaStream_t st) {
 void launch_walls(const DevState &s, int begin, int end, int gbuf, cudaStream_t st) {
   if (end <= begin) return;
   if (g_plan_ok && s.Nc8 <= 64 && (s.Nc8 <= 32 || s.Nc8 % 2 == 0)) {
-    static unsigned long long configured = 0;  // one bit per device
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (!(configured >> (dev & 63) & 1ull)) {
+    once_per_device(reinterpret_cast<const void *>(k_walls_onchip<1>), [](int) {
       const int most = kWallWarps * 13 * 64 * (int)sizeof(double);
       cudaFuncSetAttribute(k_walls_onchip<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
       cudaFuncSetAttribute(k_walls_onchip<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
-      configured |= 1ull << (dev & 63);
-    }
+    });
     const size_t smem = (size_t)kWallWarps * 13 * s.Nc8 * sizeof(double);
     const unsigned grid = blocks_for((size_t)(end - begin), kWallWarps);
     if (s.Nc8 > 32) k_walls_onchip<2><<<grid, kWallWarps * 32, smem, st>>>(s, begin, end, gbuf);

@@ -66,6 +66,13 @@ struct DevState {
   TileView tv;                  // tile-wavefront sweep schedule (when built)
 };
 
+// Runs configure() once per (key, current device) for the whole process, under a mutex:
+// launchers set kernel attributes this way from any host thread.
+void once_per_device(const void *key, void (*configure)(int device));
+// Resident blocks of kernel `fn` on the whole current device (blocks per SM x SMs) for
+// `threads` threads and `smem` dynamic shared memory; cached per (fn, device, smem).
+long resident_blocks(const void *fn, int threads, size_t smem);
+
 // Per-velocity sweep constants: cx cy cz w, then c*C products (x: 2/ds, 1/ds, -0.5/ds;
 // y: same; z: same), the 8 denominators by first-order class and their reciprocals.
 constexpr int kVtab = 29;

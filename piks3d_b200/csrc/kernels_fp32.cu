@@ -489,13 +489,9 @@ void launch_walls32(const DevState &s, int begin, int end, int gbuf, cudaStream_
   if (end <= begin) return;
   const size_t walls = (size_t)(end - begin);
   if (g32_plan_ok && (s.Nc8 == 64 || s.Nc8 <= 32)) {
-    static unsigned long long configured = 0;  // one bit per device
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (!(configured >> (dev & 63) & 1ull)) {
+    once_per_device(reinterpret_cast<const void *>(k_walls32_onchip<4, 16>), [](int) {
       cudaFuncSetAttribute(k_walls32_onchip<4, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 16 * 12 * 64 * 4);
-      configured |= 1ull << (dev & 63);
-    }
+    });
     const size_t smem_per_wall = (size_t)12 * s.Nc8 * sizeof(float);
     if (s.Nc8 == 64)
       k_walls32_onchip<4, 16><<<nblocks(walls * 16, 256), 256, 16 * smem_per_wall, st>>>(s, begin, end, gbuf);

@@ -350,19 +350,10 @@ k_tile_sweep_batch(const DevState *states, const int2 *items, int nitems, int sl
 template <typename T, int V>
 void launch_batch(const DevState *states, const int2 *items, int nitems, int slots, int tasks, int stride,
                   int *counter, int *err, cudaStream_t st) {
-  static unsigned long long configured = 0;  // one bit per device
-  int dev = 0;
-  cudaGetDevice(&dev);
-  dev &= 63;
-  if (!(configured >> dev & 1ull)) {
-    allow_dynamic_smem(reinterpret_cast<const void *>(k_tile_sweep_batch<T, V>), dev);
-    configured |= 1ull << dev;
-  }
+  const void *fn = reinterpret_cast<const void *>(k_tile_sweep_batch<T, V>);
+  once_per_device(fn, [](int dev) { allow_dynamic_smem(reinterpret_cast<const void *>(k_tile_sweep_batch<T, V>), dev); });
   const size_t smem = tile_smem_bytes(slots, tasks, stride, V * (int)sizeof(T));
-  int nb = 1, nsm = 148;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_tile_sweep_batch<T, V>, threads_of<T, V>(), smem);
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  long grid = (long)(nb < 1 ? 1 : nb) * nsm;
+  long grid = resident_blocks(fn, threads_of<T, V>(), smem);
   if (grid > nitems) grid = nitems;
   if (grid < 1) return;
   cudaMemsetAsync(counter, 0, sizeof(int), st);
@@ -372,28 +363,11 @@ void launch_batch(const DevState *states, const int2 *items, int nitems, int slo
 
 template <typename T, int V>
 void launch_dataflow(const DevState &s, int epoch, int slots, int tasks, cudaStream_t st) {
-  static unsigned long long configured = 0;  // one bit per device
-  static int per_sm[64][2];                  // resident CTAs per SM for the last smem size
-  static size_t per_sm_smem[64];
-  int dev = 0;
-  cudaGetDevice(&dev);
-  dev &= 63;
-  if (!(configured >> dev & 1ull)) {
-    allow_dynamic_smem(reinterpret_cast<const void *>(k_tile_sweep_dataflow<T, V>), dev);
-    configured |= 1ull << dev;
-    per_sm_smem[dev] = 0;
-  }
+  const void *fn = reinterpret_cast<const void *>(k_tile_sweep_dataflow<T, V>);
+  once_per_device(fn, [](int dev) { allow_dynamic_smem(reinterpret_cast<const void *>(k_tile_sweep_dataflow<T, V>), dev); });
   const size_t smem = tile_smem_bytes(slots, tasks, s.tv.steps_stride, V * (int)sizeof(T));
-  if (per_sm_smem[dev] != smem) {
-    int nb = 1, nsm = 148;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_tile_sweep_dataflow<T, V>, threads_of<T, V>(), smem);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    per_sm[dev][0] = nb < 1 ? 1 : nb;
-    per_sm[dev][1] = nsm;
-    per_sm_smem[dev] = smem;
-  }
   const long items = (long)s.tv.njobs * (s.Nc8 / V);
-  long grid = (long)per_sm[dev][0] * per_sm[dev][1];
+  long grid = resident_blocks(fn, threads_of<T, V>(), smem);
   if (grid > items) grid = items;
   if (grid < 1) return;
   cudaMemsetAsync(s.tv.counter, 0, sizeof(int), st);
@@ -402,13 +376,8 @@ void launch_dataflow(const DevState &s, int epoch, int slots, int tasks, cudaStr
 
 template <typename T, int V>
 void launch_one(const DevState &s, int job0, int njobs, int slots, int tasks, bool pdl, cudaStream_t st) {
-  static unsigned long long configured = 0;  // one bit per device
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (!(configured >> (dev & 63) & 1ull)) {
-    allow_dynamic_smem(reinterpret_cast<const void *>(k_tile_sweep<T, V>), dev);
-    configured |= 1ull << (dev & 63);
-  }
+  once_per_device(reinterpret_cast<const void *>(k_tile_sweep<T, V>),
+                  [](int dev) { allow_dynamic_smem(reinterpret_cast<const void *>(k_tile_sweep<T, V>), dev); });
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)((size_t)njobs * (s.Nc8 / V)));
   cfg.blockDim = dim3(threads_of<T, V>());

@@ -1,8 +1,11 @@
 """Generates the golden fixtures in this directory (run in a tree where the PIKS3D
 reference is mounted; the fixtures are committed so the tests never read it).
 
-  python tests/golden/make_golden.py tables   # parse the reference Fortran sources
-  python tests/golden/make_golden.py traces   # run the oracle on the shipped tutorial case
+  python tests/golden/make_golden.py --reference DIR tables   # parse the reference Fortran sources
+  python tests/golden/make_golden.py --reference DIR traces   # run the oracle on the shipped tutorial case
+
+DIR is the root of a PIKS3D source tree (src/, tutorials/); it can also be given in the
+environment as PIKS3D_REFERENCE.
 
 tables -> reference_tables.json:
   gauss_hermite : every xi*/wi*/hxi*/hwi* array of src/gaussHermite.F90 as decimal text
@@ -21,7 +24,7 @@ import re
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("PIKS3D_REFERENCE", "/root/reference")
+REF = os.environ.get("PIKS3D_REFERENCE")
 ROOT = os.path.dirname(os.path.dirname(HERE))
 
 
@@ -181,7 +184,14 @@ def _trace(o, p, what):
 
 
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["tables"]
+    argv = sys.argv[1:]
+    if "--reference" in argv:
+        i = argv.index("--reference")
+        REF = argv[i + 1]
+        del argv[i:i + 2]
+    if not REF or not os.path.isdir(REF):
+        sys.exit("make_golden.py: give the PIKS3D source tree with --reference DIR or PIKS3D_REFERENCE")
+    which = argv or ["tables"]
     if "tables" in which:
         tables()
     if "traces" in which:

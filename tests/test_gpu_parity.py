@@ -214,3 +214,78 @@ def test_larger_velocity_sets_bit_exact(nf):
         err = np.abs(fs - fo).max() / np.abs(fo).max()
         print("Nc_fundamental %d: FP32 after 3 iterations max |f32 - f64| / max |f64| = %.3e" % (nf, err))
         assert err <= 1e-5 and abs(m32 - mo[0]) / abs(mo[0]) <= 1e-5
+
+
+def test_bench_workload_fp64_iterations_equal_oracle():
+    """The benchmark's own configuration (128^3 sphere pack, porosity 0.40, radii 4-8, seed
+    12345, 512 velocities, Kn = 0.5, wallExtOrder 1), two FP64 iterations through the C ABI
+    against two oracle iterations: the chkConverge triple and the full-box Rho and U equal
+    bit for bit, and so do f at 4096 seeded nodes (fluid and wall rows, all octants and
+    velocities) and every 3-fold corner slot. The refined solver's errors in the bench are
+    stated against this FP64 path."""
+    import os
+    import bench
+    img = bench.workload_image()
+    p = bench.workload_params(pk)
+    o = Oracle(p, img.tobytes(), nthreads=os.cpu_count() or 8)
+    s = pk.Solver(p, device=0)
+    s.setup_physical_grid(img)
+    assert np.array_equal(o.labels(), s.get_labels())
+    o.iterate(2)
+    s.iterate(2)
+    assert o.chk_converge() == s.chk_converge()
+    mo = o.macro()
+    for a, b in zip(mo, s.get_macro()):
+        assert np.array_equal(a[2:-2, 2:-2, 2:-2], b)
+    inf = s.info()
+    rng = np.random.default_rng(20261203)
+    nodes = np.sort(rng.choice(inf["nNodes"], size=4096, replace=False)).astype(np.int32)
+    gidx = s.geometry_array("node_g")[nodes]
+    fs = s.get_f_nodes(nodes)
+    fo = o.f_at(gidx)
+    assert np.array_equal(fo, fs), "f differs: max %g" % np.abs(fo - fs).max()
+    assert np.array_equal(o.fw(), s.get_fw())
+    s.close()
+    o.close()
+
+
+@pytest.mark.parametrize("nf", [12, 16])
+def test_velocity_sets_beyond_512_bit_exact(nf):
+    """12 and 16 abscissae per axis (1728 and 4096 velocities per octant, 13,824 and 32,768
+    in all; velocityGrid.F90:130-154), as CPC Table 3 uses at Kn >= 1, on a 6^3 pack: every
+    kernel loops over 108 / 256 FP64 chunks; FP64 bit for bit against the oracle after two
+    iterations, for the tile and the per-node schedules."""
+    img = images.sphere_pack(6, 0.6, 1.0, 1.8, seed=21)
+    p = base_params(6, Nc_fundamental=nf, Kn=2.0, pressDrop=0.1)
+    o = Oracle(p, img.tobytes(), nthreads=8)
+    o.iterate(2)
+    mo = o.chk_converge()
+    for tiles in ((2, 2, 2), (0, 0, 0)):
+        with pk.Solver(p, device=0) as s:
+            s.set_tiles(*tiles)
+            s.setup_physical_grid(img)
+            assert s.info()["Nc8"] == nf ** 3
+            s.iterate(2)
+            _compare_state(o, s, s.geometry_array("node_g"))
+            assert s.chk_converge() == mo
+
+
+@pytest.mark.parametrize("nf", [2, 4, 8])
+def test_full_range_gauss_hermite_bit_exact(nf):
+    """halfRange = F: the full-range Gauss-Hermite abscissae and weights
+    (velocityGrid.F90:102-127) drive the sweep, walls and moments; FP64 bit for bit
+    against the oracle after three iterations on a pack with every wall type."""
+    img = images.sphere_pack(12, 0.5, 1.5, 3.0, seed=23)
+    p = base_params(12, Nc_fundamental=nf, halfRange=0, Kn=0.8, pressDrop=0.5)
+    o = Oracle(p, img.tobytes(), nthreads=8)
+    s = pk.Solver(p, device=0)
+    s.setup_physical_grid(img)
+    cx = s.geometry_array("cx")
+    assert np.array_equal(cx, o.velocity()[0])
+    nodes = s.geometry_array("node_g")
+    for _ in range(3):
+        o.iterate(1)
+        s.iterate(1)
+        _compare_state(o, s, nodes)
+        assert o.chk_converge() == s.chk_converge()
+    s.close()
