@@ -181,8 +181,17 @@ piks_status piks_set_tiles(piks_ctx *ctx, int32_t tx, int32_t ty, int32_t tz);
  * diagonal separately; PIKS_SCHED_TILE_DATAFLOW runs all jobs of an iteration in one
  * launch, each job waiting for its upwind neighbour tiles through device flags (waits give
  * up after about a second: piks_synchronize / piks_chk_converge then return
- * PIKS_ERR_CUDA). */
-enum { PIKS_SCHED_TILE_DATAFLOW = 0, PIKS_SCHED_TILE_DIAGONALS = 1 };
+ * PIKS_ERR_CUDA); PIKS_SCHED_TILE_COLUMNS runs one persistent launch in which each CTA
+ * marches down columns of tiles (one octant, one (x, y) tile position, the octant's z
+ * order): a producer warp stages the next tile with bulk asynchronous copies while the
+ * other warps sweep the current one, and the tile's last two z layers stay on chip for the
+ * next (waits give up after about two seconds, reported as for the dataflow launch);
+ * PIKS_SCHED_TILE_PIPELINED runs the same producer / consumer kernel over single jobs taken
+ * in diagonal order, each job's upwind rows staged from HBM once their jobs are done, the
+ * producer up to three jobs ahead. A change between launch schedules that read different
+ * forms of the tile jobs rebuilds them. All give identical values. */
+enum { PIKS_SCHED_TILE_DATAFLOW = 0, PIKS_SCHED_TILE_DIAGONALS = 1, PIKS_SCHED_TILE_COLUMNS = 2,
+       PIKS_SCHED_TILE_PIPELINED = 3 };
 piks_status piks_set_schedule(piks_ctx *ctx, int32_t schedule);
 /* Autotuner of the sweep schedule: right after piks_setup_physical_grid (before the first
  * iteration) times `sweeps` sweeps of each candidate (4 int32 each: TX, TY, TZ, launch

@@ -142,7 +142,7 @@ def _dptr(a):
 
 
 PREC_FP64, PREC_FP32 = 0, 1
-SCHED_TILE_DATAFLOW, SCHED_TILE_DIAGONALS = 0, 1
+SCHED_TILE_DATAFLOW, SCHED_TILE_DIAGONALS, SCHED_TILE_COLUMNS, SCHED_TILE_PIPELINED = 0, 1, 2, 3
 
 KERNEL_NAMES = ("sweep", "commit", "capture", "walls", "inlet_outlet", "symmetry", "moments", "flux")
 
@@ -309,6 +309,7 @@ class Solver:
 
     _GEO_DTYPES = {"label": np.uint8, "sym_flag": np.uint8, "roles": np.uint16, "wall_e": np.float64,
                    "hyper_start": np.int64, "tile_row_begin": np.int64, "tile_task_begin": np.int64,
+                   "tile_carry_begin": np.int64,
                    "tile_steps": np.uint16,
                    "cx": np.float64, "cy": np.float64, "cz": np.float64, "w": np.float64}
 

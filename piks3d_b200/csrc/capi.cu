@@ -212,7 +212,11 @@ void enqueue_sweep(piks_ctx *c, cudaStream_t st, int n) {
   const bool f32 = c->prec == PIKS_PREC_FP32;
   {
     Timed t(c, KT_SWEEP);
-    if (c->use_tiles && c->schedule == PIKS_SCHED_TILE_DATAFLOW) {
+    if (c->use_tiles && c->tiles.split) {
+      c->dataflow_used = true;
+      if (c->tiles.columns) launch_tile_sweep_columns(s, f32, 1, st);
+      else launch_tile_sweep_pipelined(s, f32, 1, st);
+    } else if (c->use_tiles && c->schedule == PIKS_SCHED_TILE_DATAFLOW) {
       c->dataflow_used = true;
       launch_tile_sweep_dataflow(s, f32, n, c->tiles.max_rows, c->tiles.max_tasks, st);
     } else if (c->use_tiles) {
@@ -270,13 +274,44 @@ void drop_tiles_next(piks_ctx *c) {
   c->tiles_next_dims[0] = c->tiles_next_dims[1] = c->tiles_next_dims[2] = 0;
 }
 
+// TileView fields of the column form that size the column kernel's shared memory.
+TileView column_sizes(const TileJobs &tj) {
+  TileView tv{};
+  tv.max_tasks = tj.max_tasks;
+  tv.max_nrows = tj.max_rows - 1;
+  tv.steps_stride = tj.steps_stride;
+  tv.max_carry = tj.max_carry;
+  tv.ncells = tj.ncells;
+  tv.max_region = tj.max_region;
+  tv.mean_region = tj.row_count.empty() ? 0.f : (float)((double)tj.sum_region / (double)tj.row_count.size());
+  return tv;
+}
+
+// Form of the tile jobs a launch schedule reads.
+int tile_form(int schedule) {
+  return schedule == PIKS_SCHED_TILE_COLUMNS ? TILE_FORM_COLUMNS
+         : schedule == PIKS_SCHED_TILE_PIPELINED ? TILE_FORM_SPLIT
+                                                  : TILE_FORM_SLOTS;
+}
+
+// Tile jobs for a tile shape in the given form (the split forms fall back to the slot form
+// when the producer / consumer kernel cannot hold the largest job in shared memory).
+bool build_tiles_for(const piks_ctx *c, const int *dims, int form, TileJobs &tj) {
+  tj = TileJobs{};
+  if (dims[0] <= 0) return false;
+  if (form != TILE_FORM_SLOTS) {
+    if (build_tile_jobs(c->geo, dims[0], dims[1], dims[2], 65535, tj, form) &&
+        column_sweep_fits(column_sizes(tj), c->vel.Nc8, false) && column_sweep_fits(column_sizes(tj), c->vel.Nc8, true))
+      return true;
+    tj = TileJobs{};
+  }
+  const bool ok = build_tile_jobs(c->geo, dims[0], dims[1], dims[2], tile_slots(c, dims), tj);
+  if (!ok) tj = TileJobs{};
+  return ok;
+}
+
 bool build_tiles(piks_ctx *c) {
-  c->use_tiles = false;
-  c->tiles = TileJobs{};
-  if (c->tile_dims[0] <= 0) return false;
-  const int slots = tile_slots(c, c->tile_dims);
-  c->use_tiles = build_tile_jobs(c->geo, c->tile_dims[0], c->tile_dims[1], c->tile_dims[2], slots, c->tiles);
-  if (!c->use_tiles) c->tiles = TileJobs{};
+  c->use_tiles = build_tiles_for(c, c->tile_dims, tile_form(c->schedule), c->tiles);
   return c->use_tiles;
 }
 
@@ -287,7 +322,8 @@ piks_status upload_tiles(piks_ctx *c) {
   for (const void *p : {(const void *)tv.rows, (const void *)tv.row_begin, (const void *)tv.row_count,
                         (const void *)tv.tasks, (const void *)tv.task_begin, (const void *)tv.steps,
                         (const void *)tv.job_list, (const void *)tv.up, (const void *)tv.flags,
-                        (const void *)tv.counter})
+                        (const void *)tv.counter, (const void *)tv.hdr, (const void *)tv.carry,
+                        (const void *)tv.col_jobs, (const void *)tv.col_begin, (const void *)tv.col_list})
     if (p) release(c, const_cast<void *>(p));
   tv = TileView{};
   piks_status st;
@@ -325,6 +361,19 @@ piks_status upload_tiles(piks_ctx *c) {
   tv.err = pw + 1;
   tv.nsteps = tj.nsteps;
   tv.steps_stride = tj.steps_stride;
+  if (tj.split) {
+    const TileView sz = column_sizes(tj);
+    tv.max_tasks = sz.max_tasks; tv.max_nrows = sz.max_nrows; tv.max_carry = sz.max_carry;
+    tv.ncells = sz.ncells; tv.max_region = sz.max_region; tv.mean_region = sz.mean_region;
+#define UPC(vec, field) do { if ((st = upload(c, vec, &pi))) return st; tv.field = pi; } while (0)
+    UPC(tj.hdr, hdr);
+    UPC(tj.carry, carry);
+    UPC(tj.col_jobs, col_jobs);
+    UPC(tj.col_begin, col_begin);
+    UPC(tj.col_list, col_list);
+#undef UPC
+    tv.ncols = (int)tj.col_list.size();
+  }
   return PIKS_OK;
 }
 
@@ -529,9 +578,10 @@ piks_status piks_setup_physical_grid(piks_ctx *c, const uint8_t *raw, int64_t nb
     // a refined solve switches to FP64 later: its schedule is built meanwhile
     default_tile_dims(PIKS_PREC_FP64, c->tiles_next_dims);
     const int slots = tile_slots(c, c->tiles_next_dims);
-    c->tiles_next_ready = std::async(std::launch::async, [c, slots] {
-      return build_tile_jobs(c->geo, c->tiles_next_dims[0], c->tiles_next_dims[1], c->tiles_next_dims[2], slots,
-                             c->tiles_next);
+    (void)slots;
+    const int form = tile_form(c->schedule);
+    c->tiles_next_ready = std::async(std::launch::async, [c, form] {
+      return build_tiles_for(c, c->tiles_next_dims, form, c->tiles_next);
     });
   }
   c->mass = 1.0;  // flow.F90:97
@@ -835,7 +885,7 @@ static piks_status retile_for_precision(piks_ctx *c) {
     ok = c->tiles_next_ready.get();
     if (ok) tj = std::move(c->tiles_next);
   } else {
-    ok = build_tile_jobs(c->geo, d[0], d[1], d[2], tile_slots(c, d), tj);
+    ok = build_tiles_for(c, d, tile_form(c->schedule), tj);
   }
   drop_tiles_next(c);
   if (!ok) return PIKS_OK;  // keep the current schedule
@@ -892,9 +942,25 @@ piks_status piks_set_tiles(piks_ctx *c, int32_t tx, int32_t ty, int32_t tz) {
 
 piks_status piks_set_schedule(piks_ctx *c, int32_t schedule) {
   if (!c) return fail(PIKS_ERR_ARG, "null context");
-  if (schedule != PIKS_SCHED_TILE_DATAFLOW && schedule != PIKS_SCHED_TILE_DIAGONALS)
+  if (schedule < PIKS_SCHED_TILE_DATAFLOW || schedule > PIKS_SCHED_TILE_PIPELINED)
     return fail(PIKS_ERR_ARG, "unknown schedule");
+  const int old_form = tile_form(c->schedule);
   c->schedule = schedule;
+  if (old_form == tile_form(schedule) || !c->have_host_geometry) return PIKS_OK;
+  // the new launch schedule reads another form of the tile jobs: rebuild them
+  drop_tiles_next(c);
+  if (c->device >= 0 && c->have_geometry) {
+    cudaSetDevice(c->device);
+    piks_status st = cuda_check(cudaStreamSynchronize(c->stream), "schedule sync");
+    if (st) return st;
+  }
+  build_tiles(c);
+  if (c->device >= 0 && c->have_geometry) {
+    piks_status st = upload_tiles(c);
+    if (!st) st = cuda_check(cudaStreamSynchronize(c->stream), "schedule upload");
+    if (st) return st;
+    c->version += 1;
+  }
   return PIKS_OK;
 }
 
@@ -930,11 +996,11 @@ piks_status piks_autotune(piks_ctx *c, const int32_t *cand, int32_t ncand, int32
     const int32_t *k = cand + 4 * i;
     if (ms_out) ms_out[i] = -1.0;
     if (k[0] < 2 || k[1] < 2 || k[2] < 2 || (int64_t)k[0] * k[1] * k[2] > 65535) continue;
-    if (k[3] != PIKS_SCHED_TILE_DIAGONALS && k[3] != PIKS_SCHED_TILE_DATAFLOW) continue;
+    if (k[3] < PIKS_SCHED_TILE_DATAFLOW || k[3] > PIKS_SCHED_TILE_PIPELINED) continue;
     c->tile_dims[0] = k[0]; c->tile_dims[1] = k[1]; c->tile_dims[2] = k[2];
+    c->schedule = k[3];
     if (!build_tiles(c)) continue;
     if ((st = upload_tiles(c))) break;
-    c->schedule = k[3];
     enqueue_sweep(c, c->stream, epoch++);  // warm-up
     cudaEventRecord(e0, c->stream);
     for (int r = 0; r < sweeps; ++r) enqueue_sweep(c, c->stream, epoch++);
@@ -953,9 +1019,9 @@ piks_status piks_autotune(piks_ctx *c, const int32_t *cand, int32_t ncand, int32
   if (bi < 0) return fail(PIKS_ERR_ARG, "no usable tile candidate");
   const int32_t *k = cand + 4 * bi;
   c->tile_dims[0] = k[0]; c->tile_dims[1] = k[1]; c->tile_dims[2] = k[2];
+  c->schedule = k[3];
   build_tiles(c);
   if ((st = upload_tiles(c))) return st;
-  c->schedule = k[3];
   c->tiles_tuned = true;
   // the trial sweeps changed f: back to the state of setupFlow (all zero)
   const StateSizes z = state_sizes(c);
@@ -1037,9 +1103,12 @@ piks_status piks_geometry_array(piks_ctx *c, const char *name, void *out, int64_
   ARR("tile_tasks", tj.tasks)
   ARR("tile_task_begin", tj.task_begin) ARR("tile_steps", tj.steps) ARR("tile_diag_begin", tj.diag_begin)
   ARR("tile_diag_rows", tj.diag_rows) ARR("tile_job_list", tj.job_list) ARR("tile_launches", tj.launches)
-  ARR("tile_up", tj.up)
+  ARR("tile_up", tj.up) ARR("tile_hdr", tj.hdr) ARR("tile_carry", tj.carry) ARR("tile_carry_begin", tj.carry_begin)
+  ARR("tile_col_jobs", tj.col_jobs) ARR("tile_col_begin", tj.col_begin) ARR("tile_col_list", tj.col_list)
 #undef ARR
   if (nm == "flux_groups") { src = g.flux_groups; n = 10; esz = sizeof(int32_t); }
+  int32_t colinfo[5] = {tj.columns ? 1 : tj.split ? 2 : 0, tj.ncells, tj.max_region, tj.max_carry, tj.max_tasks};
+  if (nm == "tile_column_info") { src = colinfo; n = 5; esz = sizeof(int32_t); }
   if (!esz) return fail(PIKS_ERR_ARG, "unknown geometry array " + nm);
   if (count) *count = (int64_t)n;
   if (out) {
@@ -1106,7 +1175,7 @@ piks_status piks_launches_per_iteration(piks_ctx *c, int64_t *n) {
   const DevState &s = c->ds;
   int64_t k = 0;
   if (c->use_tiles) {
-    k += c->schedule == PIKS_SCHED_TILE_DATAFLOW ? 1 : (int64_t)(c->tiles.launches.size() / 4);
+    k += (c->schedule == PIKS_SCHED_TILE_DATAFLOW || c->tiles.split) ? 1 : (int64_t)(c->tiles.launches.size() / 4);
   } else {
     for (size_t h = 0; h + 1 < c->geo.hyper_start.size(); ++h) k += c->geo.hyper_start[h + 1] > c->geo.hyper_start[h];
   }
@@ -1118,8 +1187,8 @@ piks_status piks_launches_per_iteration(piks_ctx *c, int64_t *n) {
 
 piks_status piks_selftest_wait_timeout(piks_ctx *c, double *seconds) {
   if (!c || !seconds) return fail(PIKS_ERR_ARG, "null argument");
-  if (c->device < 0 || !c->have_geometry || !c->use_tiles || c->ds.tv.njobs < 1)
-    return fail(PIKS_ERR_STATE, "the wait self-test needs a device state with a tile schedule");
+  if (c->device < 0 || !c->have_geometry || !c->use_tiles || c->ds.tv.njobs < 1 || c->tiles.split)
+    return fail(PIKS_ERR_STATE, "the wait self-test needs a device state with a dataflow or diagonal tile schedule");
   cudaSetDevice(c->device);
   DevState &s = c->ds;
   TileView &tv = s.tv;

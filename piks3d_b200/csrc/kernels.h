@@ -20,6 +20,12 @@ struct TileView {
   int *err;                     // set when a dependency wait gave up
   int njobs;
   int nsteps, steps_stride;
+  // column form (TileJobs::columns): per-job headers, carry lists, columns in dependency order
+  const int32_t *hdr;           // [njobs][8]
+  const int32_t *carry;
+  const int32_t *col_jobs, *col_begin, *col_list;
+  int ncols, ncells, max_region, max_carry, max_tasks, max_nrows;
+  float mean_region;
 };
 
 // Everything the kernels read, as device pointers (one struct passed by value).
@@ -113,6 +119,14 @@ void launch_tile_sweep_dataflow(const DevState &s, bool fp32, int epoch, int slo
 // members' flags must be zero.
 void launch_tile_sweep_batch(const DevState *states, const int2 *items, int nitems, bool fp32, int V, int slots,
                              int tasks, int stride, int *counter, int *err, cudaStream_t st);
+// Column-march sweep over the column form: one persistent launch per sweep (flags cleared
+// on the stream first, so the launch sequence can be captured in a graph).
+void launch_tile_sweep_columns(const DevState &s, bool fp32, int epoch, cudaStream_t st);
+// Pipelined dataflow sweep over the split form: the same persistent producer / consumer
+// kernel, with single jobs in the diagonal launch order as its work items.
+void launch_tile_sweep_pipelined(const DevState &s, bool fp32, int epoch, cudaStream_t st);
+// Whether the column-march kernel's shared memory holds the schedule's largest job.
+bool column_sweep_fits(const TileView &tv, int Nc8, bool fp32);
 void launch_widen(const float *src, double *dst, size_t n, cudaStream_t st);
 void launch_narrow(const double *src, float *dst, size_t n, cudaStream_t st);
 void launch_division_selftest(int64_t samples, uint64_t seed, unsigned long long *mismatches);

@@ -158,11 +158,41 @@ struct TileJobs {
   std::vector<int32_t> up;           // [njobs][4]: jobs of the upwind x, y, z neighbour tiles (same octant) or -1
   int32_t max_rows = 0;              // largest slot count of a job
   int32_t max_tasks = 0;             // largest task count of a job
+  // Column form (built with columns = true; only the column-march sweep reads it). A column
+  // is one octant's tiles at one (x, y) tile position, in the octant's z sweep order; one CTA
+  // runs a column's jobs one after another and keeps the last two z layers of each tile on
+  // chip for the next. A job's rows are then its own rows, the static rows (solid, corner
+  // and inflow-plane rows, which the sweep never writes) and the dependent rows (own rows of
+  // the x- and y-upwind tiles, read once their jobs are done); the rows it reads from the
+  // previous tile of its column come from the carried layers instead. Slots: 0 a zero row,
+  // 1 .. ncin the carried rows, then the job's rows in that order.
+  bool columns = false;
+  // Split form (built with form TILE_FORM_SPLIT or TILE_FORM_COLUMNS): rows ordered own,
+  // static, dependent, with the per-job headers; without the carried layers (columns false)
+  // the rows of the z-upwind tile are dependent rows like the x and y ones. Read by the
+  // pipelined dataflow sweep.
+  bool split = false;
+  std::vector<int32_t> hdr;          // [njobs][8]: row_begin, task_begin, carry_begin, nrows, ntask,
+                                     // first dependent row, ncin, ncout
+  BigVec<int32_t> carry;             // per job: ncin entries cell | slot << 16, then ncout entries
+                                     // own index | cell << 16 (padded to a multiple of 4)
+  std::vector<int64_t> carry_begin;  // njobs + 1
+  std::vector<int32_t> col_jobs;     // jobs of every column in sweep order
+  std::vector<int32_t> col_begin;    // ncols + 1
+  std::vector<int32_t> col_list;     // columns in dependency order (x+y tile diagonal of the octant)
+  int32_t ncells = 0;                // carried cells: 2 * TX * TY
+  int32_t max_region = 0;            // largest 1 + ncin + nrows of a job
+  int32_t max_carry = 0;             // largest ncin + ncout of a job, rounded up to 4
+  int64_t sum_region = 0;            // sum of 1 + ncin + nrows over the jobs
 };
 
 // Builds the tile jobs from g.tasks; returns false when a job needs more than max_slots
 // shared-memory rows (the caller then keeps the hyperplane schedule).
-bool build_tile_jobs(const Geometry &g, int TX, int TY, int TZ, int max_slots, TileJobs &tj);
+// Forms of the tile jobs: slots in first-read order (diagonal, dataflow and batch sweeps),
+// split rows (pipelined dataflow sweep), split rows with carried z layers (column march).
+enum { TILE_FORM_SLOTS = 0, TILE_FORM_SPLIT = 1, TILE_FORM_COLUMNS = 2 };
+bool build_tile_jobs(const Geometry &g, int TX, int TY, int TZ, int max_slots, TileJobs &tj,
+                     int form = TILE_FORM_SLOTS);
 // (Re)builds the launch plan with at most max_classes size classes per diagonal; a class
 // holds the jobs whose slot count is above `ratio` times its largest.
 void plan_tile_launches(TileJobs &tj, int max_classes, double ratio);

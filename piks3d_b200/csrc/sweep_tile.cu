@@ -17,12 +17,14 @@
 #include <cuda_runtime.h>
 
 #include "kernels.h"
+#include "sweep_core.cuh"
 
 namespace piks {
 
 namespace {
 
-constexpr int kFwBit = 1 << 30;
+using namespace sweep;
+
 // Task groups per CTA (tasks of one local hyperplane in flight): 16 for FP64, 6 for FP32,
 // whose groups have twice the lanes (V = 32 velocities); both measured fastest on B200
 // (FP32 sweep of a 128^3 pack per iteration: 4 groups 2.76 ms, 6: 2.69, 8: 2.74, 12: 3.39).
@@ -34,27 +36,6 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
-
-__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
-__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
-__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
-// RN(num/den) from y = RN(1/den) with Markstein's correction step (see kernels.cu).
-__device__ __forceinline__ double markstein_div(double num, double den, double y) {
-  const double q0 = __dmul_rn(num, y);
-  const double r = __fma_rn(-q0, den, num);
-  return __fma_rn(r, y, q0);
-}
-
-template <typename T> struct Pair;
-template <> struct Pair<double> { using type = double2; };
-template <> struct Pair<float> { using type = float2; };
-
-template <typename T> __device__ __forceinline__ const T *state_h(const DevState &a);
-template <> __device__ __forceinline__ const double *state_h<double>(const DevState &a) { return a.h; }
-template <> __device__ __forceinline__ const float *state_h<float>(const DevState &a) { return a.h32; }
-template <typename T> __device__ __forceinline__ const T *state_fw(const DevState &a);
-template <> __device__ __forceinline__ const double *state_fw<double>(const DevState &a) { return a.fw; }
-template <> __device__ __forceinline__ const float *state_fw<float>(const DevState &a) { return a.fw32; }
 
 // Shared-memory layout of one CTA: [slots][V] rows, the job's task records (int4), the
 // moments of each task's node (two double2), the row codes (int32) and the step offsets.
@@ -119,111 +100,23 @@ __device__ __forceinline__ void tile_job(const DevState &a, int job, int chunk, 
   const int grp = threadIdx.x / LPT, sub = threadIdx.x % LPT;
   const int lp = l0 + 2 * sub;
   const int o = Codes[0] & 7;                       // own row code = node * 8 + octant
-  const bool nx_ = !(o == 0 || o == 3 || o == 4 || o == 7);
-  const bool ny_ = !(o == 0 || o == 1 || o == 4 || o == 5);
-  const bool nz_ = o >= 4;
+  const bool nx_ = neg_x(o), ny_ = neg_y(o), nz_ = neg_z(o);
   T K[13][2];
-  if constexpr (sizeof(T) == 8) {
-    const double2 *vt = a.vtab2 + (size_t)(lp >> 1) * kVtab;
-#pragma unroll
-    for (int k = 0; k < 13; ++k) { const double2 t = __ldg(vt + k); K[k][0] = t.x; K[k][1] = t.y; }
-  } else {
-#pragma unroll
-    for (int k = 0; k < 13; ++k) {
-      K[k][0] = __ldg(a.vtab32 + (size_t)lp * kVtab + k);
-      K[k][1] = __ldg(a.vtab32 + (size_t)(lp + 1) * kVtab + k);
-    }
-  }
+  load_lane_consts<T>(a, lp, K);
 
   cp_async_wait_all();
   __syncthreads();
 
   // 2. the part of every update that does not depend on this sweep's values,
   //    mu * (fEq - f_old / 2) (solver.F90:205-214), replaces f_old in the task's own slot
-  for (int t = grp; t < ntask; t += GROUPS) {
-    const double2 m01 = Mom[2 * t], m23 = Mom[2 * t + 1];
-    T2 *own = reinterpret_cast<T2 *>(S + (size_t)(1 + t) * V + 2 * sub);
-    const T2 fold = *own;
-    const T fo[2] = {fold.x, fold.y};
-    T base[2];
-    if constexpr (sizeof(T) == 8) {
-      const double rho = m01.x, ux = m01.y, uy = m23.x, uz = m23.y;
-#pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        const double cx = K[0][q], cy = K[1][q], cz = K[2][q], wl = K[3][q];
-        const double ex = dmul(nx_ ? -cx : cx, ux), ey = dmul(ny_ ? -cy : cy, uy), ez = dmul(nz_ ? -cz : cz, uz);
-        const double feq = dmul(wl, dadd(rho, dadd(dadd(ex, ey), ez)));
-        base[q] = dmul(a.mu, dsub(feq, dmul(0.5, fo[q])));
-      }
-    } else {
-      const float rho = (float)m01.x, ux = (float)m01.y, uy = (float)m23.x, uz = (float)m23.y;
-      const float mu = (float)a.mu;
-#pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        const float cx = K[0][q], cy = K[1][q], cz = K[2][q], wl = K[3][q];
-        const float feq = wl * (rho + ((nx_ ? -cx : cx) * ux + (ny_ ? -cy : cy) * uy + (nz_ ? -cz : cz) * uz));
-        base[q] = mu * (feq - 0.5f * fo[q]);
-      }
-    }
-    T2 bv;
-    bv.x = base[0];
-    bv.y = base[1];
-    *own = bv;
-  }
+  base_pass<T, V, GROUPS>(a, Mom, S, 1, ntask, grp, sub, K, nx_, ny_, nz_);
   __syncthreads();
 
   // 3. local hyperplanes: the upwind terms in the reference's order, then the division
   for (int s = 0; s < nsteps; ++s) {
     const int t0 = Steps[s], t1 = Steps[s + 1];
     if (t0 == t1) continue;
-    for (int t = t0 + grp; t < t1; t += GROUPS) {
-      const int4 rec = Trec[t];
-      const bool fx = (rec.x >> 27) & 1, fy = (rec.x >> 28) & 1, fz = (rec.x >> 29) & 1;
-      const int cls = (fx ? 1 : 0) | (fy ? 2 : 0) | (fz ? 4 : 0);
-      auto ld = [&](int slot) { return *reinterpret_cast<const T2 *>(S + (size_t)slot * V + 2 * sub); };
-      const T2 b2 = ld(1 + t);
-      const T2 x1 = ld(rec.y & 0xffff), y1 = ld(rec.z & 0xffff), z1 = ld(rec.w & 0xffff);
-      T2 x2{}, y2{}, z2{};
-      if (!fx) x2 = ld((unsigned)rec.y >> 16);
-      if (!fy) y2 = ld((unsigned)rec.z >> 16);
-      if (!fz) z2 = ld((unsigned)rec.w >> 16);
-      const T bs[2] = {b2.x, b2.y}, vx1[2] = {x1.x, x1.y}, vx2[2] = {x2.x, x2.y}, vy1[2] = {y1.x, y1.y},
-              vy2[2] = {y2.x, y2.y}, vz1[2] = {z1.x, z1.y}, vz2[2] = {z2.x, z2.y};
-      T out[2];
-      if constexpr (sizeof(T) == 8) {
-        const double2 dn = __ldg(a.vtab2 + (size_t)(lp >> 1) * kVtab + 13 + cls);
-        const double2 rc = __ldg(a.vtab2 + (size_t)(lp >> 1) * kVtab + 21 + cls);
-        const double den[2] = {dn.x, dn.y}, rcp[2] = {rc.x, rc.y};
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-          double num = bs[q];
-          num = dadd(num, dmul(fx ? K[5][q] : K[4][q], vx1[q]));
-          if (!fx) num = dadd(num, dmul(K[6][q], vx2[q]));
-          num = dadd(num, dmul(fy ? K[8][q] : K[7][q], vy1[q]));
-          if (!fy) num = dadd(num, dmul(K[9][q], vy2[q]));
-          num = dadd(num, dmul(fz ? K[11][q] : K[10][q], vz1[q]));
-          if (!fz) num = dadd(num, dmul(K[12][q], vz2[q]));
-          out[q] = markstein_div(num, den[q], rcp[q]);
-        }
-      } else {
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-          const float rcp = __ldg(a.vtab32 + (size_t)(lp + q) * kVtab + 21 + cls);
-          float num = bs[q];
-          num += (fx ? K[5][q] : K[4][q]) * vx1[q];
-          if (!fx) num += K[6][q] * vx2[q];
-          num += (fy ? K[8][q] : K[7][q]) * vy1[q];
-          if (!fy) num += K[9][q] * vy2[q];
-          num += (fz ? K[11][q] : K[10][q]) * vz1[q];
-          if (!fz) num += K[12][q] * vz2[q];
-          out[q] = num * rcp;
-        }
-      }
-      T2 res;
-      res.x = out[0];
-      res.y = out[1];
-      *reinterpret_cast<T2 *>(S + (size_t)(1 + t) * V + 2 * sub) = res;
-    }
+    for (int t = t0 + grp; t < t1; t += GROUPS) update_task<T, V>(a, S, Trec[t], 1 + t, sub, lp, K);
     __syncthreads();
   }
 

@@ -45,9 +45,214 @@ struct RowSet {
   }
 };
 
+// Rows, task records, steps, carried layers and column lists of the column form (see
+// TileJobs). Returns false when a job reads a row of a tile that is not its own or one of
+// its three upwind neighbours, or needs more shared-memory rows than `max_slots`.
+bool build_column_rows(const Geometry &g, TileJobs &tj, const BigVec<int64_t> &order, int32_t njobs,
+                       const std::vector<int64_t> &job_pair, int64_t ntiles, int nTx, int nTy, int nTz, int max_slots,
+                       unsigned cap, const BigVec<uint16_t> &step, bool carry_z) {
+  const int TX = tj.TX, TY = tj.TY, TZ = tj.TZ;
+  const int64_t GX = g.GX, GXY = (int64_t)g.GX * g.GY;
+  const int64_t nrows_h = ((int64_t)g.NF + g.NB) * 8;
+  tj.columns = carry_z;
+  tj.split = true;
+  tj.ncells = carry_z ? 2 * TX * TY : 0;
+  // owner job and own index of every swept h row
+  BigVec<int32_t> job_of_row((size_t)nrows_h);
+  BigVec<uint16_t> own_of_row((size_t)nrows_h);
+  parallel_chunks(nrows_h, [&](int64_t b, int64_t e) { std::fill(job_of_row.begin() + b, job_of_row.begin() + e, -1); });
+  parallel_chunks(njobs, [&](int64_t jb, int64_t je) {
+    for (int64_t j = jb; j < je; ++j)
+      for (int64_t p = tj.task_begin[(size_t)j]; p < tj.task_begin[(size_t)j + 1]; ++p) {
+        const int32_t *r = &g.tasks[(size_t)order[(size_t)p] * 8];
+        const int64_t row = (int64_t)r[0] * 8 + (r[1] & 7);
+        job_of_row[(size_t)row] = (int32_t)j;
+        own_of_row[(size_t)row] = (uint16_t)(p - tj.task_begin[(size_t)j]);
+      }
+  });
+  // carried cell of a node in the two z layers of tile-z index c nearest to the next tile in
+  // the octant's sweep order (-1 when the node is not in them)
+  auto cell_of = [&](int32_t node, int o, int c) -> int {
+    if (!carry_z) return -1;
+    const int64_t gi = g.node_g[(size_t)node];
+    const int x = (int)(gi % GX) - 2, y = (int)((gi / GX) % g.GY) - 2, z = (int)(gi / GXY) - 2;
+    if (z / TZ != c) return -1;
+    const int layer = oct_sz(o) > 0 ? z - (c * TZ + TZ - 2) : (c * TZ + 1) - z;
+    if (layer < 0 || layer > 1) return -1;
+    return layer * TX * TY + (y % TY) * TX + (x % TX);
+  };
+  auto row_index = [&](int32_t code) -> int64_t {
+    return (code & (1 << 30)) ? nrows_h + (code & ~(1 << 30)) : (int64_t)code;
+  };
+  std::vector<int32_t> ncin((size_t)njobs), ncout((size_t)njobs), nstat((size_t)njobs), ndep((size_t)njobs);
+  std::vector<char> bad((size_t)njobs, 0);
+  // pass 1: counts
+  unsigned ccap = 64;
+  while (ccap < (unsigned)(4 * TX * TY)) ccap <<= 1;
+  parallel_chunks(njobs, [&](int64_t jb, int64_t je) {
+    RowSet cin(ccap), stat(cap), dep(cap);
+    for (int64_t j = jb; j < je; ++j) {
+      cin.clear(); stat.clear(); dep.clear();
+      const int64_t pr = job_pair[(size_t)j];
+      const int o = (int)(pr / ntiles);
+      const int c = (int)((pr % ntiles) / ((int64_t)nTx * nTy));
+      const int32_t ux = tj.up[(size_t)j * 4], uy = tj.up[(size_t)j * 4 + 1], uz = tj.up[(size_t)j * 4 + 2];
+      int32_t ni = 0, ns = 0, nd = 0, no = 0;
+      bool added;
+      for (int64_t p = tj.task_begin[(size_t)j]; p < tj.task_begin[(size_t)j + 1]; ++p) {
+        const int32_t *r = &g.tasks[(size_t)order[(size_t)p] * 8];
+        if (cell_of(r[0], o, c) >= 0) ++no;
+        for (int k = 0; k < 6; ++k) {
+          const int32_t code = r[2 + k];
+          if (code < 0) continue;
+          const int32_t jq = (code & (1 << 30)) ? -1 : job_of_row[(size_t)code];
+          if (jq < 0) { stat.find_or_add(row_index(code), ns, &added); ns += added; continue; }
+          if (jq == (int32_t)j) continue;
+          if (carry_z && jq == uz && k >= 4) {
+            const int cell = cell_of(code >> 3, o, c - oct_sz(o));
+            if (cell < 0) { bad[(size_t)j] = 1; break; }
+            cin.find_or_add(cell, ni, &added); ni += added;
+          } else if (jq == ux || jq == uy || (!carry_z && jq == uz && k >= 4)) {
+            dep.find_or_add(row_index(code), nd, &added); nd += added;
+          } else {
+            bad[(size_t)j] = 1;
+            break;
+          }
+        }
+      }
+      const int32_t nt = (int32_t)(tj.task_begin[(size_t)j + 1] - tj.task_begin[(size_t)j]);
+      ncin[(size_t)j] = ni; ncout[(size_t)j] = no; nstat[(size_t)j] = ns; ndep[(size_t)j] = nd;
+      if (1 + ni + nt + ns + nd > max_slots) bad[(size_t)j] = 1;
+    }
+  });
+  for (int32_t j = 0; j < njobs; ++j)
+    if (bad[(size_t)j]) return false;
+  tj.row_count.assign((size_t)njobs, 0);
+  tj.row_begin.assign((size_t)njobs + 1, 0);
+  tj.carry_begin.assign((size_t)njobs + 1, 0);
+  for (int32_t j = 0; j < njobs; ++j) {
+    const int32_t nt = (int32_t)(tj.task_begin[(size_t)j + 1] - tj.task_begin[(size_t)j]);
+    tj.row_count[(size_t)j] = nt + nstat[(size_t)j] + ndep[(size_t)j];
+    tj.row_begin[(size_t)j + 1] = tj.row_begin[(size_t)j] + (tj.row_count[(size_t)j] + 3) / 4 * 4;
+    tj.carry_begin[(size_t)j + 1] = tj.carry_begin[(size_t)j] + (ncin[(size_t)j] + ncout[(size_t)j] + 3) / 4 * 4;
+  }
+  // the device addresses these arrays with 32-bit offsets
+  if (tj.row_begin.back() + 4 > INT32_MAX || tj.task_begin.back() > INT32_MAX || tj.carry_begin.back() + 4 > INT32_MAX)
+    return false;
+  // (+4: bulk copies move whole 16-byte pieces past a job's last entry)
+  tj.rows.assign((size_t)tj.row_begin.back() + 4, 0);
+  tj.carry.assign((size_t)tj.carry_begin.back() + 4, 0);
+  tj.tasks.resize((size_t)tj.task_begin.back() * 4);
+  tj.steps.assign((size_t)njobs * tj.steps_stride, 0);
+  tj.hdr.assign((size_t)njobs * 8, 0);
+  // pass 2: slots and records
+  parallel_chunks(njobs, [&](int64_t jb, int64_t je) {
+    RowSet cin(ccap), stat(cap), dep(cap);
+    for (int64_t j = jb; j < je; ++j) {
+      cin.clear(); stat.clear(); dep.clear();
+      const int64_t pr = job_pair[(size_t)j];
+      const int o = (int)(pr / ntiles);
+      const int c = (int)((pr % ntiles) / ((int64_t)nTx * nTy));
+      const int32_t uz = tj.up[(size_t)j * 4 + 2];
+      const int64_t q = tj.task_begin[(size_t)j], e = tj.task_begin[(size_t)j + 1];
+      const int32_t nt = (int32_t)(e - q), ni = ncin[(size_t)j], ns = nstat[(size_t)j];
+      int32_t *rows = &tj.rows[(size_t)tj.row_begin[(size_t)j]];
+      int32_t *cl = &tj.carry[(size_t)tj.carry_begin[(size_t)j]];
+      const int32_t own0 = 1 + ni;
+      int32_t ci = 0, si = 0, di = 0, co = 0;
+      bool added;
+      for (int64_t p = q; p < e; ++p) {
+        const int32_t *r = &g.tasks[(size_t)order[(size_t)p] * 8];
+        rows[p - q] = r[0] * 8 + (r[1] & 7);
+        const int cell = cell_of(r[0], o, c);
+        if (cell >= 0) cl[ni + co++] = (int32_t)(p - q) | (cell << 16);
+      }
+      for (int64_t p = q; p < e; ++p) {
+        const int32_t *r = &g.tasks[(size_t)order[(size_t)p] * 8];
+        int32_t sl[6];
+        for (int k = 0; k < 6; ++k) {
+          const int32_t code = r[2 + k];
+          if (code < 0) { sl[k] = 0; continue; }
+          const int32_t jq = (code & (1 << 30)) ? -1 : job_of_row[(size_t)code];
+          if (jq < 0) {
+            const int32_t idx = stat.find_or_add(row_index(code), si, &added);
+            if (added) rows[nt + si++] = code;
+            sl[k] = own0 + nt + idx;
+          } else if (jq == (int32_t)j) {
+            sl[k] = own0 + own_of_row[(size_t)code];
+          } else if (carry_z && jq == uz && k >= 4) {
+            const int cell = cell_of(code >> 3, o, c - oct_sz(o));
+            const int32_t idx = cin.find_or_add(cell, ci, &added);
+            if (added) { cl[ci] = cell | ((1 + ci) << 16); ++ci; }
+            sl[k] = 1 + idx;
+          } else {
+            const int32_t idx = dep.find_or_add(row_index(code), di, &added);
+            if (added) rows[nt + ns + di++] = code;
+            sl[k] = own0 + nt + ns + idx;
+          }
+        }
+        const int fl = r[1];
+        int32_t *tr = &tj.tasks[(size_t)p * 4];
+        tr[0] = r[0] | ((fl & 8) ? 1 << 27 : 0) | ((fl & 16) ? 1 << 28 : 0) | ((fl & 32) ? 1 << 29 : 0);
+        tr[1] = sl[0] | (sl[1] << 16);
+        tr[2] = sl[2] | (sl[3] << 16);
+        tr[3] = sl[4] | (sl[5] << 16);
+      }
+      uint16_t *st = &tj.steps[(size_t)j * tj.steps_stride];
+      for (int64_t p = q; p < e; ++p) st[step[(size_t)order[(size_t)p]] + 1]++;
+      for (int s2 = 0; s2 < tj.nsteps; ++s2) st[s2 + 1] = (uint16_t)(st[s2 + 1] + st[s2]);
+      int32_t *h = &tj.hdr[(size_t)j * 8];
+      h[0] = (int32_t)tj.row_begin[(size_t)j];
+      h[1] = (int32_t)q;
+      h[2] = (int32_t)tj.carry_begin[(size_t)j];
+      h[3] = tj.row_count[(size_t)j];
+      h[4] = nt;
+      h[5] = nt + ns;
+      h[6] = ni;
+      h[7] = co;
+    }
+  });
+  tj.max_region = 0;
+  tj.max_carry = 0;
+  tj.sum_region = 0;
+  for (int32_t j = 0; j < njobs; ++j) {
+    const int32_t reg = 1 + ncin[(size_t)j] + tj.row_count[(size_t)j];
+    tj.max_region = std::max(tj.max_region, reg);
+    tj.sum_region += reg;
+    tj.max_carry = std::max(tj.max_carry, (ncin[(size_t)j] + ncout[(size_t)j] + 3) / 4 * 4);
+  }
+  // columns: (octant, x tile, y tile), their jobs in the octant's z order, listed by the
+  // x+y tile diagonal of the octant's frame (every upwind column comes first)
+  const int64_t ncol_all = (int64_t)8 * nTx * nTy;
+  std::vector<int32_t> job_at((size_t)ntiles * 8, -1);
+  for (int32_t j = 0; j < njobs; ++j) job_at[(size_t)job_pair[(size_t)j]] = j;
+  tj.col_begin.assign(1, 0);
+  tj.col_jobs.clear();
+  std::vector<std::pair<int, int32_t>> keyed;
+  for (int64_t col = 0; col < ncol_all; ++col) {
+    const int o = (int)(col / ((int64_t)nTx * nTy));
+    const int a = (int)(col % nTx), b = (int)((col / nTx) % nTy);
+    const size_t before = tj.col_jobs.size();
+    for (int k = 0; k < nTz; ++k) {
+      const int cz = oct_sz(o) > 0 ? k : nTz - 1 - k;
+      const int32_t j = job_at[(size_t)((int64_t)o * ntiles + a + (int64_t)nTx * (b + (int64_t)nTy * cz))];
+      if (j >= 0) tj.col_jobs.push_back(j);
+    }
+    if (tj.col_jobs.size() == before) continue;
+    const int d = (oct_sx(o) > 0 ? a : nTx - 1 - a) + (oct_sy(o) > 0 ? b : nTy - 1 - b);
+    keyed.push_back({d, (int32_t)(tj.col_begin.size() - 1)});
+    tj.col_begin.push_back((int32_t)tj.col_jobs.size());
+  }
+  std::stable_sort(keyed.begin(), keyed.end(),
+                   [](const std::pair<int, int32_t> &x, const std::pair<int, int32_t> &y) { return x.first < y.first; });
+  tj.col_list.resize(keyed.size());
+  for (size_t i = 0; i < keyed.size(); ++i) tj.col_list[i] = keyed[i].second;
+  return true;
+}
+
 }  // namespace
 
-bool build_tile_jobs(const Geometry &g, int TX, int TY, int TZ, int max_slots, TileJobs &tj) {
+bool build_tile_jobs(const Geometry &g, int TX, int TY, int TZ, int max_slots, TileJobs &tj, int form) {
   tj = TileJobs{};
   tj.TX = TX; tj.TY = TY; tj.TZ = TZ;
   tj.nsteps = TX + TY + TZ - 2;
@@ -148,12 +353,30 @@ bool build_tile_jobs(const Geometry &g, int TX, int TY, int TZ, int max_slots, T
   jstep.clear(); jstep.shrink_to_fit();
   pair_of.clear(); pair_of.shrink_to_fit();
 
+  // upstream jobs: the neighbour tiles on the upwind side of each axis, same octant
+  tj.up.assign((size_t)njobs * 4, -1);
+  for (int32_t j = 0; j < njobs; ++j) {
+    const int64_t pr = job_pair[(size_t)j];
+    const int o = (int)(pr / ntiles);
+    const int64_t t = pr % ntiles;
+    const int a = (int)(t % nTx), b = (int)((t / nTx) % nTy), c = (int)(t / ((int64_t)nTx * nTy));
+    const int na = a - oct_sx(o), nb = b - oct_sy(o), nc = c - oct_sz(o);
+    const int64_t base = (int64_t)o * ntiles;
+    if (na >= 0 && na < nTx) tj.up[(size_t)j * 4 + 0] = job_of_pair[(size_t)(base + na + (int64_t)nTx * (b + (int64_t)nTy * c))];
+    if (nb >= 0 && nb < nTy) tj.up[(size_t)j * 4 + 1] = job_of_pair[(size_t)(base + a + (int64_t)nTx * (nb + (int64_t)nTy * c))];
+    if (nc >= 0 && nc < nTz) tj.up[(size_t)j * 4 + 2] = job_of_pair[(size_t)(base + a + (int64_t)nTx * (b + (int64_t)nTy * nc))];
+  }
   const int64_t nrows_h = ((int64_t)g.NF + g.NB) * 8;
   auto row_index = [&](int32_t code) -> int64_t {
     return (code & (1 << 30)) ? nrows_h + (code & ~(1 << 30)) : (int64_t)code;
   };
   unsigned cap = 64;
   while (cap < (unsigned)std::max(2 * max_slots, 64)) cap <<= 1;
+  if (form != TILE_FORM_SLOTS) {
+    if (!build_column_rows(g, tj, order, njobs, job_pair, ntiles, nTx, nTy, nTz, max_slots, cap, step,
+                           form == TILE_FORM_COLUMNS))
+      return false;
+  } else {
   // pass 1: rows (slots - 1) of every job
   tj.row_count.assign((size_t)njobs, 0);
   parallel_chunks(njobs, [&](int64_t jb, int64_t je) {
@@ -226,6 +449,7 @@ bool build_tile_jobs(const Geometry &g, int TX, int TY, int TZ, int max_slots, T
       for (int s2 = 0; s2 < nsteps; ++s2) st[s2 + 1] = (uint16_t)(st[s2 + 1] + st[s2]);
     }
   });
+  }
   // per-diagonal bounds
   tj.diag_begin.assign((size_t)ndiag + 1, 0);
   tj.diag_rows.assign((size_t)ndiag, 0);
@@ -241,19 +465,6 @@ bool build_tile_jobs(const Geometry &g, int TX, int TY, int TZ, int max_slots, T
     tj.diag_begin[(size_t)diag + 1] = j + 1;
   }
   for (int d = 0; d < ndiag; ++d) tj.diag_begin[(size_t)d + 1] = std::max(tj.diag_begin[(size_t)d + 1], tj.diag_begin[(size_t)d]);
-  // upstream jobs: the neighbour tiles on the upwind side of each axis, same octant
-  tj.up.assign((size_t)njobs * 4, -1);
-  for (int32_t j = 0; j < njobs; ++j) {
-    const int64_t pr = job_pair[(size_t)j];
-    const int o = (int)(pr / ntiles);
-    const int64_t t = pr % ntiles;
-    const int a = (int)(t % nTx), b = (int)((t / nTx) % nTy), c = (int)(t / ((int64_t)nTx * nTy));
-    const int na = a - oct_sx(o), nb = b - oct_sy(o), nc = c - oct_sz(o);
-    const int64_t base = (int64_t)o * ntiles;
-    if (na >= 0 && na < nTx) tj.up[(size_t)j * 4 + 0] = job_of_pair[(size_t)(base + na + (int64_t)nTx * (b + (int64_t)nTy * c))];
-    if (nb >= 0 && nb < nTy) tj.up[(size_t)j * 4 + 1] = job_of_pair[(size_t)(base + a + (int64_t)nTx * (nb + (int64_t)nTy * c))];
-    if (nc >= 0 && nc < nTz) tj.up[(size_t)j * 4 + 2] = job_of_pair[(size_t)(base + a + (int64_t)nTx * (b + (int64_t)nTy * nc))];
-  }
   plan_tile_launches(tj, 1, 0.0);
   return true;
 }

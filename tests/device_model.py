@@ -264,6 +264,121 @@ class DeviceModel:
                     code = int(rows[rbeg[j] + q])
                     self.h[code // 8, code % 8] = S[1 + q]
 
+    def sweep_columns(self, solver, arena_rows=None):
+        """All eight octant sweeps as the column-march kernel runs them: columns in their
+        dependency order, each column's jobs in z order; a job's region holds a zero row,
+        the rows carried from the previous tile of the column (a dense buffer of two z layers
+        per column, written at the end of each job), its own rows (previous values), the
+        static rows and the dependent rows (written by the upwind columns' jobs, which come
+        earlier in the list). Checks every slot, cell and count against the bounds the kernel
+        sizes its shared memory by, and, when arena_rows is given, replays the producer's
+        region allocation in an arena of that many rows (the consumer releasing each job's
+        region one job later than it could)."""
+        g = solver.geometry_array
+        rows, rbeg = g("tile_rows"), g("tile_row_begin")
+        tasks, tbeg = g("tile_tasks").reshape(-1, 4), g("tile_task_begin")
+        steps = g("tile_steps")
+        hdr = g("tile_hdr").reshape(-1, 8)
+        carry, cbeg = g("tile_carry"), g("tile_carry_begin")
+        cjobs, cbegin, clist = g("tile_col_jobs"), g("tile_col_begin"), g("tile_col_list")
+        info = g("tile_column_info")
+        assert info[0] in (1, 2)
+        ncells, max_region, max_carry, max_tasks = int(info[1]), int(info[2]), int(info[3]), int(info[4])
+        njobs = len(rbeg) - 1
+        stride = len(steps) // njobs
+        sch = solver.schedule()
+        nst = int(sch["TX"] + sch["TY"] + sch["TZ"] - 2)
+        c15, c10 = 1.5 / self.ds, 1.0 / self.ds
+        P = {"x2": self.cx * (2.0 / self.ds), "x1": self.cx * c10, "xh": self.cx * (-0.5 / self.ds),
+             "y2": self.cy * (2.0 / self.ds), "y1": self.cy * c10, "yh": self.cy * (-0.5 / self.ds),
+             "z2": self.cz * (2.0 / self.ds), "z1": self.cz * c10, "zh": self.cz * (-0.5 / self.ds)}
+        dens = {}
+        for cls in range(8):
+            d = 0.5 * self.mu + self.cx * (c10 if cls & 1 else c15)
+            d = d + self.cy * (c10 if cls & 2 else c15)
+            dens[cls] = d + self.cz * (c10 if cls & 4 else c15)
+        assert sorted(cjobs.tolist()) == list(range(njobs))
+        done = np.zeros(njobs, dtype=bool)
+        up = g("tile_up").reshape(-1, 4)
+        live, tail = [], 0                       # arena replay: (base, n) of unreleased regions
+        for col in clist:
+            cbuf = [None] * ncells
+            for q in range(cbegin[col], cbegin[col + 1]):
+                j = int(cjobs[q])
+                rb, tb, cb, nrows, ntask, dep0, ncin, ncout = (int(v) for v in hdr[j])
+                assert rb == rbeg[j] and tb == tbeg[j] and cb == cbeg[j] and rb % 4 == 0 and cb % 4 == 0
+                assert ntask == tbeg[j + 1] - tbeg[j] <= max_tasks and ncin + ncout <= max_carry
+                n = 1 + ncin + nrows
+                assert n <= max_region
+                for u in up[j, :3]:
+                    assert u < 0 or done[u], "dependent rows read before their job ran"
+                if arena_rows is not None:
+                    assert n <= arena_rows
+                    while True:
+                        if not live:
+                            base = 0
+                            break
+                        head = live[0][0]
+                        if tail > head:
+                            if arena_rows - tail >= n:
+                                base = tail
+                                break
+                            if head >= n:
+                                base = 0
+                                break
+                        elif head - tail >= n:
+                            base = tail
+                            break
+                        live.pop(0)
+                    tail = base + n
+                    for b0, n0 in live:
+                        assert base + n <= b0 or b0 + n0 <= base, "regions overlap"
+                    live.append((base, n))
+                    if len(live) > 2:                # released one job after its successor ran
+                        live.pop(0)
+                S = [np.zeros(self.Nc8)]
+                for e in range(ncin):
+                    cell, slot = carry[cb + e] & 0xFFFF, carry[cb + e] >> 16
+                    assert slot == 1 + e and 0 <= cell < ncells and cbuf[cell] is not None
+                    S.append(cbuf[cell].copy())
+                for r in rows[rb:rb + nrows]:
+                    S.append(self._row(int(r)).copy())
+                o = int(rows[rb]) & 7
+                own0 = 1 + ncin
+                T = tasks[tb:tb + ntask]
+                st = steps[j * stride:(j + 1) * stride]
+                for s_ in range(nst):
+                    for t in range(st[s_], st[s_ + 1]):
+                        rec = [int(v) & 0xFFFFFFFF for v in T[t]]
+                        m = rec[0] & ((1 << 27) - 1)
+                        fx, fy, fz = bool(rec[0] >> 27 & 1), bool(rec[0] >> 28 & 1), bool(rec[0] >> 29 & 1)
+                        sl = [rec[1] & 0xFFFF, rec[1] >> 16, rec[2] & 0xFFFF, rec[2] >> 16, rec[3] & 0xFFFF, rec[3] >> 16]
+                        assert all(0 <= v < n for v in sl)
+                        ex = (-self.cx if SX[o] < 0 else self.cx) * self.mom[1, m]
+                        ey = (-self.cy if SY[o] < 0 else self.cy) * self.mom[2, m]
+                        ez = (-self.cz if SZ[o] < 0 else self.cz) * self.mom[3, m]
+                        feq = self.w * (self.mom[0, m] + ((ex + ey) + ez))
+                        num = self.mu * (feq - 0.5 * S[own0 + t])
+                        num = num + (P["x1"] if fx else P["x2"]) * S[sl[0]]
+                        if not fx:
+                            num = num + P["xh"] * S[sl[1]]
+                        num = num + (P["y1"] if fy else P["y2"]) * S[sl[2]]
+                        if not fy:
+                            num = num + P["yh"] * S[sl[3]]
+                        num = num + (P["z1"] if fz else P["z2"]) * S[sl[4]]
+                        if not fz:
+                            num = num + P["zh"] * S[sl[5]]
+                        cls = (1 if fx else 0) | (2 if fy else 0) | (4 if fz else 0)
+                        S[own0 + t] = num / dens[cls]
+                for t in range(ntask):
+                    code = int(rows[rb + t])
+                    self.h[code // 8, code % 8] = S[own0 + t]
+                for e in range(ncout):
+                    r, cell = carry[cb + ncin + e] & 0xFFFF, carry[cb + ncin + e] >> 16
+                    assert 0 <= r < ntask and 0 <= cell < ncells
+                    cbuf[cell] = S[own0 + r].copy()
+                done[j] = True
+
     # --- the rest of one iteration -------------------------------------------------------
     def _far(self, code, o, gbuf):
         if code >= 0:
@@ -313,7 +428,7 @@ class DeviceModel:
                     else:
                         self.fw[corner, dst_o - 1] = v
 
-    def iterate(self, n=1, schedule="tasks", solver=None):
+    def iterate(self, n=1, schedule="tasks", solver=None, arena_rows=None):
         for _ in range(n):
             it = self.iStep + 1
             cap, prev = it & 1, (it - 1) & 1
@@ -321,6 +436,8 @@ class DeviceModel:
                 self.sweep_tasks()
             elif schedule == "tiles":
                 self.sweep_tiles(solver)
+            elif schedule == "columns":
+                self.sweep_columns(solver, arena_rows)
             else:
                 for o in range(8):
                     self.sweep(o)

@@ -183,3 +183,23 @@ def test_fp32_dataflow_216_velocities_matches_diagonals():
             s.iterate(5)
             out.append((s.get_f()[0], s.chk_converge()))
     assert np.array_equal(out[0][0], out[1][0]) and out[0][1] == out[1][1]
+
+
+@pytest.mark.parametrize("nf", [2, 4, 6])
+def test_fp32_columns_match_diagonals(nf):
+    """The column-march and pipelined FP32 sweeps evaluate each update with the tile
+    kernel's operations, so their values equal the tile-diagonal sweep's bit for bit (64,
+    512 and 1728 velocities: rows of 8, 32 and 8 FP32 velocities per chunk)."""
+    img = images.sphere_pack(14, 0.5, 1.2, 3.0, seed=31)
+    p = base_params(14, Nc_fundamental=nf, Kn=0.5, fluidlayer=1)
+    out = []
+    for sched in (pk.SCHED_TILE_COLUMNS, pk.SCHED_TILE_PIPELINED, pk.SCHED_TILE_DIAGONALS):
+        with pk.Solver(p, device=0) as s:
+            s.set_tiles(4, 4, 4)
+            s.set_precision(pk.PREC_FP32)
+            s.set_schedule(sched)
+            s.setup_physical_grid(img)
+            s.iterate(6)
+            out.append((s.get_f()[0], s.chk_converge()))
+    for f, m in out[:2]:
+        assert np.array_equal(f, out[2][0]) and m == out[2][1]

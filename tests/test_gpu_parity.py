@@ -46,7 +46,11 @@ CASES = [
 SCHEDULES = {"tiles844_dataflow": ((8, 4, 4), pk.SCHED_TILE_DATAFLOW),
              "tiles435_dataflow": ((4, 3, 5), pk.SCHED_TILE_DATAFLOW),
              "tiles8_diagonals": ((8, 8, 8), pk.SCHED_TILE_DIAGONALS),
-             "hyperplanes": ((0, 0, 0), pk.SCHED_TILE_DATAFLOW)}
+             "hyperplanes": ((0, 0, 0), pk.SCHED_TILE_DATAFLOW),
+             "columns444": ((4, 4, 4), pk.SCHED_TILE_COLUMNS),
+             "columns523": ((5, 2, 3), pk.SCHED_TILE_COLUMNS),
+             "pipelined444": ((4, 4, 4), pk.SCHED_TILE_PIPELINED),
+             "pipelined523": ((5, 2, 3), pk.SCHED_TILE_PIPELINED)}
 
 
 @pytest.mark.parametrize("schedule", list(SCHEDULES))
