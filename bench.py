@@ -367,6 +367,10 @@ def run_ours(args, world, rank, local):
             return {"value": nf * nv * st * world / t / 1e9, "unit": UNIT,
                     "h2d_bytes_per_step": img.nbytes / st,
                     "d2h_bytes_per_step": (8 * st / p.chkConvergeStep + 4 * box * 8) / st, "seconds": t,
+                    "setup_seconds": {"box_and_drill_thin": r["setup_seconds"][0],
+                                      "voxel_classification_on_device": r["setup_seconds"][1],
+                                      "rest_of_geometry": r["setup_seconds"][2],
+                                      "whole_setup_call": r["setup_seconds"][3]},
                     "what": what + " solve through the public API: create + setup_physical_grid(host image) + "
                             "%d iterations with a check every %d + get_macro, wall clock" % (st, p.chkConvergeStep)}
         e2e = e2e_of(r64, t64, "plain FP64")

@@ -114,6 +114,19 @@ piks_status piks_get_f_nodes(piks_ctx *ctx, const int32_t *nodes, int32_t n, dou
  * out (capacity bytes) the data when not NULL. */
 piks_status piks_geometry_array(piks_ctx *ctx, const char *name, void *out, int64_t capacity, int64_t *count);
 
+/* Where piks_setup_physical_grid classifies the voxels (wall labels, the node map of the
+ * voxels the solver reads, 3-fold corner numbers and the wall list; physicalGrid.F90:546-936):
+ * PIKS_PREP_DEVICE (the default for a context with a device) runs it as CUDA kernels,
+ * PIKS_PREP_HOST on the host; both give identical arrays. The image read and the drill /
+ * thin passes (physicalGrid.F90:257-422, whose in-place raster order decides their result)
+ * and the sweep schedule stay on the host. No counterpart in the reference. */
+enum { PIKS_PREP_HOST = 0, PIKS_PREP_DEVICE = 1 };
+piks_status piks_set_preprocessing(piks_ctx *ctx, int32_t where);
+/* Wall-clock seconds of the last piks_setup_physical_grid (out[4]): image read, replication
+ * and drill / thin; voxel classification; the rest of the geometry and the sweep tasks; the
+ * whole call (tile schedule, uploads and allocation included). */
+piks_status piks_setup_seconds(piks_ctx *ctx, double *out);
+
 /* Makes the context enqueue on `stream` (a cudaStream_t); NULL restores its own stream. */
 piks_status piks_set_stream(piks_ctx *ctx, void *stream);
 

@@ -80,6 +80,8 @@ def load_library(path=LIB_PATH):
         "piks_get_f_nodes": (i32, [c_void_p, P(i32), i32, P(dbl)]),
         "piks_geometry_array": (i32, [c_void_p, ctypes.c_char_p, c_void_p, i64, P(i64)]),
         "piks_set_stream": (i32, [c_void_p, c_void_p]),
+        "piks_set_preprocessing": (i32, [c_void_p, i32]),
+        "piks_setup_seconds": (i32, [c_void_p, P(dbl)]),
         "piks_kernel_times": (i32, [c_void_p, P(dbl), i32, i32]),
         "piks_kernel_names": (ctypes.c_char_p, []),
         "piks_enable_timing": (i32, [c_void_p, i32]),
@@ -143,6 +145,7 @@ def _dptr(a):
 
 PREC_FP64, PREC_FP32 = 0, 1
 SCHED_TILE_DATAFLOW, SCHED_TILE_DIAGONALS, SCHED_TILE_COLUMNS, SCHED_TILE_PIPELINED = 0, 1, 2, 3
+PREP_HOST, PREP_DEVICE = 0, 1
 
 KERNEL_NAMES = ("sweep", "commit", "capture", "walls", "inlet_outlet", "symmetry", "moments", "flux")
 
@@ -212,6 +215,18 @@ class Solver:
         """PREC_FP64 (reference arithmetic) or PREC_FP32 (FP32 f and sweep, FP64 moments,
         wall densities and flux); converts a live state on the device."""
         _check(self.lib.piks_set_precision(self._ctx, int(precision)))
+
+    def set_preprocessing(self, where):
+        """PREP_DEVICE (default with a device) or PREP_HOST: where setup_physical_grid classifies
+        the voxels; both give identical geometry."""
+        _check(self.lib.piks_set_preprocessing(self._ctx, int(where)))
+
+    def setup_seconds(self):
+        """Seconds of the last setup: (box and drill / thin, classification, rest of the
+        geometry, the whole call)."""
+        a = (ctypes.c_double * 4)()
+        _check(self.lib.piks_setup_seconds(self._ctx, a))
+        return tuple(a)
 
     def set_tiles(self, tx, ty=None, tz=None):
         """Tile shape of the sweep schedule (0 = per-node hyperplanes); applies at the next

@@ -22,7 +22,7 @@ CU_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + CSRC
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-I" + CSRC,
              "-I" + os.path.join(ROOT, "include")]
 
-CU_SOURCES = ["kernels.cu", "kernels_fp32.cu", "sweep_tile.cu", "sweep_column.cu", "capi.cu", "batch.cu"]
+CU_SOURCES = ["kernels.cu", "kernels_fp32.cu", "sweep_tile.cu", "sweep_column.cu", "preprocess.cu", "capi.cu", "batch.cu"]
 CXX_SOURCES = ["host.cpp", "tiles.cpp", "output.cpp"]
 
 

@@ -479,17 +479,43 @@ piks_status piks_create(const piks_params *p, int32_t device, piks_ctx **out) {
 
 piks_status piks_setup_physical_grid(piks_ctx *c, const uint8_t *raw, int64_t nbytes) {
   if (!c) return fail(PIKS_ERR_ARG, "null context");
+  const auto t_setup = std::chrono::steady_clock::now();
   drop_tiles_next(c);
   if (c->device >= 0) { cudaSetDevice(c->device); free_device(c); }
   c->have_host_geometry = false;
   std::string err;
-  piks_status st = preprocess(c->setup, raw, nbytes, c->geo, err);
-  if (st) return fail(st, err);
+  piks_status st;
+  {
+    // the box on the host (its drill / thin passes depend on the raster order), the voxel
+    // classification on the device when the context has one, the rest on the host
+    using clk = std::chrono::steady_clock;
+    const auto t0 = clk::now();
+    std::vector<uint8_t> box;
+    st = preprocess_box(c->setup, raw, nbytes, box, err);
+    if (st) return fail(st, err);
+    const auto t1 = clk::now();
+    if (c->device >= 0 && c->prep == PIKS_PREP_DEVICE) {
+      st = classify_device(c->setup, box, c->geo, c->stream, err);
+      if (st) return fail(st, err);
+    } else {
+      classify_host(c->setup, box, c->geo);
+    }
+    const auto t2 = clk::now();
+    st = finish_geometry(c->setup, c->geo, err);
+    if (st) return fail(st, err);
+    const auto t3 = clk::now();
+    c->setup_seconds[0] = std::chrono::duration<double>(t1 - t0).count();
+    c->setup_seconds[1] = std::chrono::duration<double>(t2 - t1).count();
+    c->setup_seconds[2] = std::chrono::duration<double>(t3 - t2).count();
+  }
   c->have_host_geometry = true;
   c->tiles_tuned = false;
   if (!c->tiles_explicit) default_tile_dims(c->prec, c->tile_dims);
   build_tiles(c);
-  if (c->device < 0) return PIKS_OK;
+  if (c->device < 0) {
+    c->setup_seconds[3] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_setup).count();
+    return PIKS_OK;
+  }
   const Geometry &g = c->geo;
   const Velocity &v = c->vel;
   DevState &s = c->ds;
@@ -587,6 +613,7 @@ piks_status piks_setup_physical_grid(piks_ctx *c, const uint8_t *raw, int64_t nb
   c->mass = 1.0;  // flow.F90:97
   c->error = 1.0;
   c->permeability = 0.0;
+  c->setup_seconds[3] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_setup).count();
   return PIKS_OK;
 }
 
@@ -1146,6 +1173,19 @@ piks_status piks_selftest_division_noalloc(int32_t device, int64_t samples, uint
   const int rc = division_selftest_noalloc(device, samples, seed, mismatches, &err);
   if (rc == 1) return fail(PIKS_ERR_ARG, err);
   if (rc) return fail(PIKS_ERR_CUDA, err);
+  return PIKS_OK;
+}
+
+piks_status piks_set_preprocessing(piks_ctx *c, int32_t where) {
+  if (!c) return fail(PIKS_ERR_ARG, "null context");
+  if (where != PIKS_PREP_HOST && where != PIKS_PREP_DEVICE) return fail(PIKS_ERR_ARG, "unknown preprocessing place");
+  c->prep = where;
+  return PIKS_OK;
+}
+
+piks_status piks_setup_seconds(piks_ctx *c, double *out) {
+  if (!c || !out) return fail(PIKS_ERR_ARG, "null argument");
+  for (int i = 0; i < 4; ++i) out[i] = c->setup_seconds[i];
   return PIKS_OK;
 }
 

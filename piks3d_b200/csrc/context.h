@@ -40,6 +40,8 @@ struct piks_ctx {
   piks::TileJobs tiles;
   bool use_tiles = false;           // tile schedule built and uploaded
   int schedule = PIKS_SCHED_TILE_DIAGONALS;
+  int prep = PIKS_PREP_DEVICE;      // where voxels are classified (device contexts)
+  double setup_seconds[4] = {0, 0, 0, 0};  // last setup: box, classification, rest of the geometry, all
   int iStep = 0;
   int version = 0;                  // bumped whenever the device state is reallocated
   double mass = 1.0, error = 1.0, permeability = 0.0;

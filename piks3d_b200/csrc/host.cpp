@@ -368,7 +368,8 @@ int label_from_sides(uint8_t sides) {
 
 }  // namespace
 
-piks_status preprocess(const Setup &s, const uint8_t *raw, int64_t nbytes, Geometry &g, std::string &err) {
+piks_status preprocess_box(const Setup &s, const uint8_t *raw, int64_t nbytes, std::vector<uint8_t> &box,
+                           std::string &err) {
   const int Nx = s.Nx, Ny = s.Ny, Nz = s.Nz, fl = s.p.fluidlayer;
   const int64_t need = (int64_t)s.Nz_base * s.Ny_base * (s.Nx_base - 2 * fl);
   if (!raw || nbytes < need) { err = "image stream shorter than Nx*Ny*Nz bytes"; return PIKS_ERR_IMAGE; }
@@ -393,7 +394,16 @@ piks_status preprocess(const Setup &s, const uint8_t *raw, int64_t nbytes, Geome
                 b.at(i * s.Nx_base + ii, j * s.Ny_base + jj, k * s.Nz_base + kk) = b.at(ii, jj, kk);
   b.set_ghosts(L_GHOST);
   for (int round = 0; round < 2; ++round) { drill_pass(b); thin_pass(b); }
+  box.swap(b.v);
+  return PIKS_OK;
+}
 
+void classify_host(const Setup &s, const std::vector<uint8_t> &box, Geometry &g) {
+  const int Nx = s.Nx, Ny = s.Ny, Nz = s.Nz;
+  const int BGX = Nx + 4, BGY = Ny + 4;
+  auto B = [&](int i, int j, int k) -> uint8_t {
+    return box[(size_t)(i + 1) + (size_t)(j + 1) * BGX + (size_t)(k + 1) * BGX * BGY];
+  };
   g.Nx = Nx; g.Ny = Ny; g.Nz = Nz; g.GX = Nx + 4; g.GY = Ny + 4; g.GZ = Nz + 4;
   const size_t NG = (size_t)g.GX * g.GY * g.GZ;
   g.label.assign(NG, L_GHOST);
@@ -401,16 +411,16 @@ piks_status preprocess(const Setup &s, const uint8_t *raw, int64_t nbytes, Geome
   for (int k = 1; k <= Nz; ++k)
     for (int j = 1; j <= Ny; ++j)
       for (int i = 1; i <= Nx; ++i) {
-        uint8_t c = b.at(i, j, k);
+        uint8_t c = B(i, j, k);
         int lab = c;
         if (c == L_SOLID) {
           uint8_t sides = 0;
-          if (b.at(i + 1, j, k) == L_FLUID) sides |= FACE_E;
-          if (b.at(i - 1, j, k) == L_FLUID) sides |= FACE_W;
-          if (b.at(i, j + 1, k) == L_FLUID) sides |= FACE_N;
-          if (b.at(i, j - 1, k) == L_FLUID) sides |= FACE_S;
-          if (b.at(i, j, k + 1) == L_FLUID) sides |= FACE_F;
-          if (b.at(i, j, k - 1) == L_FLUID) sides |= FACE_B;
+          if (B(i + 1, j, k) == L_FLUID) sides |= FACE_E;
+          if (B(i - 1, j, k) == L_FLUID) sides |= FACE_W;
+          if (B(i, j + 1, k) == L_FLUID) sides |= FACE_N;
+          if (B(i, j - 1, k) == L_FLUID) sides |= FACE_S;
+          if (B(i, j, k + 1) == L_FLUID) sides |= FACE_F;
+          if (B(i, j, k - 1) == L_FLUID) sides |= FACE_B;
           lab = label_from_sides(sides);
         }
         g.label[g.ghost_index(i, j, k)] = (uint8_t)lab;
@@ -451,16 +461,11 @@ piks_status preprocess(const Setup &s, const uint8_t *raw, int64_t nbytes, Geome
   g.NF = 0;
   for (int32_t gi : g.node_g) if (g.label[gi] == L_FLUID) g.NF++;
   g.NB = (int32_t)g.node_g.size() - g.NF;
-  // node*8 + slot codes of the sweep must stay below 2^30
-  if ((int64_t)g.node_g.size() * 8 >= (int64_t)1 << 30) { err = "image too large (more than 2^27 nodes read by the solver)"; return PIKS_ERR_ARG; }
 
   // walls in raster (vecWall) order, 3-fold corners numbered in the same order
   g.wall_node.clear(); g.wall_label.clear(); g.wall_corner.clear(); g.wall_e.clear(); g.wall_nb.clear();
   g.bcorner.assign(g.NB, -1);
   g.nCorner = 0;
-  const int GX = g.GX, GXY = g.GX * g.GY;
-  // reference local id (1-based) and its decode, used by wallExtOrder == 3 (physicalGrid.F90:895-936)
-  const int64_t NXT = Nx + 4, NXYT = (int64_t)(Nx + 4) * (Ny + 4);
   for (int k = 1; k <= Nz; ++k)
     for (int j = 1; j <= Ny; ++j)
       for (int i = 1; i <= Nx; ++i) {
@@ -470,40 +475,11 @@ piks_status preprocess(const Setup &s, const uint8_t *raw, int64_t nbytes, Geome
         int corner = -1;
         if (is_corner3_label(lab)) corner = g.nCorner++;
         if (node >= g.NF) g.bcorner[node - g.NF] = corner;
-        double e1 = 2.0, e2 = -1.0;
-        if (s.p.wallExtOrder == 1) { e1 = 1.0; e2 = 0.0; }
-        else if (s.p.wallExtOrder != 2) {
-          int64_t localid = (int64_t)(i + 2) + (int64_t)(j + 1) * NXT + (int64_t)(k + 1) * NXYT;
-          int kd = -1 + (int)(localid / NXYT);
-          int jd = -1 + (int)((localid - (int64_t)(kd + 1) * NXYT) / NXT);
-          int id = -1 + (int)(localid - (int64_t)(kd + 1) * NXYT - (int64_t)(jd + 1) * NXT);
-          int v = LAB(id, jd, kd);
-          uint8_t fm = face_mask(v);
-          bool first = false;
-          if ((fm & FACE_W) && id == 2 && LAB(1, jd, kd) == L_FLUID) first = true;
-          if ((fm & FACE_E) && id == Nx - 1 && LAB(Nx, jd, kd) == L_FLUID) first = true;
-          if ((fm & FACE_S) && jd == 2 && LAB(id, 1, kd) == L_FLUID) first = true;
-          if ((fm & FACE_N) && jd == Ny - 1 && LAB(id, Ny, kd) == L_FLUID) first = true;
-          if ((fm & FACE_B) && kd == 2 && LAB(id, jd, 1) == L_FLUID) first = true;
-          if ((fm & FACE_F) && kd == Nz - 1 && LAB(id, jd, Nz) == L_FLUID) first = true;
-          if (first) { e1 = 1.0; e2 = 0.0; }
-        }
+        double e1, e2;
+        wall_extrapolation(s, g, i, j, k, e1, e2);
         const WProg *P = wall_program(lab);
-        int32_t nb[6] = {-1, -1, -1, -1, -1, -1};
-        for (int fi = 0; fi < P->nface; ++fi) {
-          int dir = P->face[fi].dir;
-          int dx = dir == DIR_PX ? 1 : dir == DIR_MX ? -1 : 0;
-          int dy = dir == DIR_PY ? 1 : dir == DIR_MY ? -1 : 0;
-          int dz = dir == DIR_PZ ? 1 : dir == DIR_MZ ? -1 : 0;
-          nb[2 * fi] = g.nodemap[g.ghost_index(i + dx, j + dy, k + dz)];
-          int i2 = i + 2 * dx, j2 = j + 2 * dy, k2 = k + 2 * dz;
-          int32_t code;
-          if (real(i2, j2, k2)) code = g.nodemap[g.ghost_index(i2, j2, k2)];  // node, or -1
-          else if (i2 == 0 && j2 >= 1 && j2 <= Ny && k2 >= 1 && k2 <= Nz) code = -(2 + 2 * ((k2 - 1) * Ny + (j2 - 1)));
-          else if (i2 == Nx + 1 && j2 >= 1 && j2 <= Ny && k2 >= 1 && k2 <= Nz) code = -(3 + 2 * ((k2 - 1) * Ny + (j2 - 1)));
-          else code = -1;  // y/z ghost layers hold zeros on one rank
-          nb[2 * fi + 1] = code;
-        }
+        int32_t nb[6];
+        wall_neighbours(g, P, i, j, k, nb);
         g.wall_node.push_back(node);
         g.wall_label.push_back(lab);
         g.wall_corner.push_back(corner);
@@ -511,6 +487,63 @@ piks_status preprocess(const Setup &s, const uint8_t *raw, int64_t nbytes, Geome
         for (int t = 0; t < 6; ++t) g.wall_nb.push_back(nb[t]);
       }
   g.nWall = (int32_t)g.wall_node.size();
+}
+
+// wallExtOrder's extrapolation coefficients of the wall at (i, j, k) (physicalGrid.F90:889-936).
+void wall_extrapolation(const Setup &s, const Geometry &g, int i, int j, int k, double &e1, double &e2) {
+  const int Nx = s.Nx, Ny = s.Ny, Nz = s.Nz;
+  auto LAB = [&](int ii, int jj, int kk) -> int { return g.label[g.ghost_index(ii, jj, kk)]; };
+  // reference local id (1-based) and its decode, used by wallExtOrder == 3 (physicalGrid.F90:895-936)
+  const int64_t NXT = Nx + 4, NXYT = (int64_t)(Nx + 4) * (Ny + 4);
+  e1 = 2.0; e2 = -1.0;
+  if (s.p.wallExtOrder == 1) { e1 = 1.0; e2 = 0.0; }
+  else if (s.p.wallExtOrder != 2) {
+    int64_t localid = (int64_t)(i + 2) + (int64_t)(j + 1) * NXT + (int64_t)(k + 1) * NXYT;
+    int kd = -1 + (int)(localid / NXYT);
+    int jd = -1 + (int)((localid - (int64_t)(kd + 1) * NXYT) / NXT);
+    int id = -1 + (int)(localid - (int64_t)(kd + 1) * NXYT - (int64_t)(jd + 1) * NXT);
+    int v = LAB(id, jd, kd);
+    uint8_t fm = face_mask(v);
+    bool first = false;
+    if ((fm & FACE_W) && id == 2 && LAB(1, jd, kd) == L_FLUID) first = true;
+    if ((fm & FACE_E) && id == Nx - 1 && LAB(Nx, jd, kd) == L_FLUID) first = true;
+    if ((fm & FACE_S) && jd == 2 && LAB(id, 1, kd) == L_FLUID) first = true;
+    if ((fm & FACE_N) && jd == Ny - 1 && LAB(id, Ny, kd) == L_FLUID) first = true;
+    if ((fm & FACE_B) && kd == 2 && LAB(id, jd, 1) == L_FLUID) first = true;
+    if ((fm & FACE_F) && kd == Nz - 1 && LAB(id, jd, Nz) == L_FLUID) first = true;
+    if (first) { e1 = 1.0; e2 = 0.0; }
+  }
+}
+
+// Node at +d and code at +2d along each face direction of wall program P at (i, j, k)
+// (see Geometry::wall_nb).
+void wall_neighbours(const Geometry &g, const WProg *P, int i, int j, int k, int32_t *nb) {
+  const int Nx = g.Nx, Ny = g.Ny, Nz = g.Nz;
+  auto real = [&](int ii, int jj, int kk) { return ii >= 1 && ii <= Nx && jj >= 1 && jj <= Ny && kk >= 1 && kk <= Nz; };
+  for (int t = 0; t < 6; ++t) nb[t] = -1;
+  for (int fi = 0; fi < P->nface; ++fi) {
+    int dir = P->face[fi].dir;
+    int dx = dir == DIR_PX ? 1 : dir == DIR_MX ? -1 : 0;
+    int dy = dir == DIR_PY ? 1 : dir == DIR_MY ? -1 : 0;
+    int dz = dir == DIR_PZ ? 1 : dir == DIR_MZ ? -1 : 0;
+    nb[2 * fi] = g.nodemap[g.ghost_index(i + dx, j + dy, k + dz)];
+    int i2 = i + 2 * dx, j2 = j + 2 * dy, k2 = k + 2 * dz;
+    int32_t code;
+    if (real(i2, j2, k2)) code = g.nodemap[g.ghost_index(i2, j2, k2)];  // node, or -1
+    else if (i2 == 0 && j2 >= 1 && j2 <= Ny && k2 >= 1 && k2 <= Nz) code = -(2 + 2 * ((k2 - 1) * Ny + (j2 - 1)));
+    else if (i2 == Nx + 1 && j2 >= 1 && j2 <= Ny && k2 >= 1 && k2 <= Nz) code = -(3 + 2 * ((k2 - 1) * Ny + (j2 - 1)));
+    else code = -1;  // y/z ghost layers hold zeros on one rank
+    nb[2 * fi + 1] = code;
+  }
+}
+
+piks_status finish_geometry(const Setup &s, Geometry &g, std::string &err) {
+  const int Nx = s.Nx, Ny = s.Ny, Nz = s.Nz;
+  // node*8 + slot codes of the sweep must stay below 2^30
+  if ((int64_t)g.node_g.size() * 8 >= (int64_t)1 << 30) { err = "image too large (more than 2^27 nodes read by the solver)"; return PIKS_ERR_ARG; }
+  auto LAB = [&](int i, int j, int k) -> int { return g.label[g.ghost_index(i, j, k)]; };
+  auto real = [&](int i, int j, int k) { return i >= 1 && i <= Nx && j >= 1 && j <= Ny && k >= 1 && k <= Nz; };
+  const int GX = g.GX, GXY = g.GX * g.GY;
 
   // Dependency levels: a wall whose extrapolation reads another wall's slots must see
   // that wall's new values if it comes earlier in vecWall order and its old values if it
@@ -691,6 +724,14 @@ piks_status preprocess(const Setup &s, const uint8_t *raw, int64_t nbytes, Geome
   g.flux_list.push_back(fnode(Ny, Nz)); // NF
   g.flux_groups[gi++] = (int32_t)g.flux_list.size();
   return PIKS_OK;
+}
+
+piks_status preprocess(const Setup &s, const uint8_t *raw, int64_t nbytes, Geometry &g, std::string &err) {
+  std::vector<uint8_t> box;
+  piks_status st = preprocess_box(s, raw, nbytes, box, err);
+  if (st) return st;
+  classify_host(s, box, g);
+  return finish_geometry(s, g, err);
 }
 
 }  // namespace piks

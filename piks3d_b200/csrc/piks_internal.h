@@ -200,6 +200,23 @@ void plan_tile_launches(TileJobs &tj, int max_classes, double ratio);
 piks_status make_setup(const piks_params &p, Setup &s, std::string &err);
 piks_status make_velocity(const piks_params &p, Velocity &v, std::string &err);
 piks_status preprocess(const Setup &s, const uint8_t *raw, int64_t nbytes, Geometry &g, std::string &err);
+// The stages of preprocess: the ghosted working box after the stream read, block replication
+// and the two drill / thin rounds (raster-order passes, physicalGrid.F90:257-422); the
+// classification of its voxels into labels, the node map (fluid nodes, then the solid
+// nodes the solver reads, both in raster order), the 3-fold corner numbers and the wall
+// list (physicalGrid.F90:546-936), on the host or on the device (classify_device,
+// preprocess.cu); the rest of the geometry from those (wall levels, switch roles,
+// commits, sweep tasks, planes, flux list).
+piks_status preprocess_box(const Setup &s, const uint8_t *raw, int64_t nbytes, std::vector<uint8_t> &box,
+                           std::string &err);
+void classify_host(const Setup &s, const std::vector<uint8_t> &box, Geometry &g);
+// classify_host on the current CUDA device (preprocess.cu), identical results; synchronous on
+// `stream` (a cudaStream_t).
+piks_status classify_device(const Setup &s, const std::vector<uint8_t> &box, Geometry &g, void *stream,
+                            std::string &err);
+piks_status finish_geometry(const Setup &s, Geometry &g, std::string &err);
+void wall_extrapolation(const Setup &s, const Geometry &g, int i, int j, int k, double &e1, double &e2);
+void wall_neighbours(const Geometry &g, const WProg *P, int i, int j, int k, int32_t *nb);
 piks_status read_namelist(const char *path, piks_params &p, std::string &image_file, std::string &err);
 std::string fortran_es15_6(double v);
 

@@ -338,6 +338,7 @@ def solve_one(image, params, device=0, precision="fp64", tol=None, eps=None, swi
     if precision in ("fp32", "refined"):
         s.set_precision(PREC_FP32)
     s.setup_physical_grid(image)
+    setup_seconds = list(s.setup_seconds())
     chk = params.chkConvergeStep
     phase = "fp64" if precision == "fp64" else "fp32"
     base_eps = eps if eps is not None else params.eps
@@ -359,7 +360,8 @@ def solve_one(image, params, device=0, precision="fp64", tol=None, eps=None, swi
             continue
         if ok or conv.diverged or steps >= params.maxStep:
             res = {"steps": steps, "steps32": steps32, "mass": m, "permeability": k, "error": e,
-                   "converged": bool(ok), "diverged": conv.diverged, "estimate": conv.estimate}
+                   "converged": bool(ok), "diverged": conv.diverged, "estimate": conv.estimate,
+                   "setup_seconds": setup_seconds}
             if keep_fields:
                 res["macro"] = s.get_macro()
             s.close()
