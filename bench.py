@@ -376,6 +376,10 @@ def run_ours(args, world, rank, local):
         e2e = e2e_of(r64, t64, "plain FP64")
         solve["e2e_refined"] = e2e_of(rrf, trf, "refined (FP32 sweep, FP64 refinement)")
 
+    batch = None
+    if args.batch_images > 0:
+        batch = small_batch(args, world, rank, local, device)
+
     if rank != 0:
         return 0
     peaks = {}
@@ -401,6 +405,7 @@ def run_ours(args, world, rank, local):
                  "roofline": roofline_of(m32, hbm, peaks, traffic_per_update("fp32"), nc8,
                                          "FP32 octant sweep (all launches of one iteration's sweep)")},
         "solve": solve,
+        "batch": batch,
         "e2e": e2e,
         "gpu_launches": m64["launches"],
         "clocks": m64["clocks"],
@@ -411,7 +416,7 @@ def run_ours(args, world, rank, local):
     return 0
 
 
-def batch_jobs(pk, count, seed, max_step):
+def batch_jobs(pk, count, seed, max_step, edges=(32, 48, 64, 80, 96), kn_range=(0.01, 10.0)):
     """The batching workload: seeded sphere packs, edges from {32, 48, 64, 80, 96}, porosity
     U[0.3, 0.6], Kn log-uniform in [0.01, 10], 64 or 512 velocities per sample."""
     import numpy as np
@@ -420,15 +425,54 @@ def batch_jobs(pk, count, seed, max_step):
     rng = np.random.default_rng(seed)
     jobs = []
     for i in range(count):
-        n = int(rng.choice([32, 48, 64, 80, 96]))
+        n = int(rng.choice(list(edges)))
         por = float(rng.uniform(0.3, 0.6))
-        kn = float(np.exp(rng.uniform(np.log(0.01), np.log(10.0))))
+        kn = float(np.exp(rng.uniform(np.log(kn_range[0]), np.log(kn_range[1]))))
         ncf = int(rng.choice([2, 4]))
         img = images.sphere_pack(n, por, 4.0, 8.0, seed=seed * 1000 + i)
         p = pk.default_params(Nx=n, Ny=n, Nz=n, Nc_fundamental=ncf, Kn=kn, pressDrop=1.0, wallExtOrder=1,
                               maxStep=max_step, chkConvergeStep=10, eps=1e-8)
         jobs.append(Job(img, p, name="img%d" % i))
     return jobs
+
+
+SMALL_BATCH = dict(edges=(32, 48, 64), kn_range=(0.3, 10.0), seed=77)
+
+
+def small_batch(args, world, rank, local, device):
+    """The reduced batching workload of the default line: `--batch-images` seeded sphere
+    packs (edges 32-64, porosity U[0.3, 0.6], Kn log-uniform in [0.3, 10], 64 or 512
+    velocities) solved to the 1e-4 permeability tolerance, plain FP64 one after another
+    against the refined solver's batch runner (all images in flight together)."""
+    import numpy as np
+    import piks3d_b200 as pk
+    from piks3d_b200.solve import BatchRunner, solve_one
+    sb = SMALL_BATCH
+    jobs = batch_jobs(pk, args.batch_images, sb["seed"] + rank, args.max_step, sb["edges"], sb["kn_range"])
+    barrier(world, device)
+    t0 = time.perf_counter()
+    plain = [solve_one(j.image, j.params, device=local, precision="fp64", tol=TOL) for j in jobs]
+    t_plain = reduce_max(time.perf_counter() - t0, world, device)
+    runner = BatchRunner(device=local, precision="refined", tol=TOL, max_members=args.batch_images)
+    barrier(world, device)
+    t0 = time.perf_counter()
+    done = runner.run(batch_jobs(pk, args.batch_images, sb["seed"] + rank, args.max_step, sb["edges"],
+                                 sb["kn_range"]))
+    t_batch = reduce_max(time.perf_counter() - t0, world, device)
+    runner.close()
+    by = {j.name: j.result for j in done}
+    diffs = [abs(by[j.name]["permeability"] - p["permeability"]) / abs(p["permeability"]) for j, p in zip(jobs, plain)]
+    return {"workload": "%d seeded sphere packs, edges %s, porosity U[0.3,0.6], Kn log-U[%g,%g], 64 or 512 velocities, "
+                        "wallExtOrder 1, tolerance %g on k" % (args.batch_images, list(sb["edges"]), sb["kn_range"][0],
+                                                              sb["kn_range"][1], TOL),
+            "plain_fp64_sequential": {"seconds": t_plain, "solves_per_s": args.batch_images * world / t_plain,
+                                      "iterations": sum(p["steps"] for p in plain)},
+            "refined_batched": {"seconds": t_batch, "solves_per_s": args.batch_images * world / t_batch,
+                                "iterations": sum(r["steps"] for r in by.values()),
+                                "converged": sum(1 for r in by.values() if r["converged"])},
+            "speedup_solves_per_s": t_plain / t_batch,
+            "perm_rel_diff_refined_vs_fp64": {"max": max(diffs), "median": float(np.median(diffs))},
+            "autotuned_tiles": sorted({str(r.get("tiles")) for r in by.values()})}
 
 
 def run_batch_workload(args, world, rank, local):
@@ -520,6 +564,8 @@ def main():
     ap.add_argument("--cpu-iters", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-solve", action="store_true", help="skip the full solves (solve / e2e blocks)")
+    ap.add_argument("--batch-images", type=int, default=12,
+                    help="images of the reduced batching workload in the default line (0: skip)")
     ap.add_argument("--workload", default="precision", choices=["precision", "batch", "serve", "large"],
                     help="precision: the 128^3 pack (default); batch: many images; serve: request stream; "
                          "large: the 256^3 Gaussian random field (add --solve-large for the full solves)")
@@ -540,6 +586,8 @@ def main():
         WORKLOAD.update(LARGE)
         args.no_solve = args.no_solve or not args.solve_large
         args.workload = "precision"
+    if args.no_solve:
+        args.batch_images = 0
     if args.n:
         WORKLOAD["n"] = args.n
     world, rank, local = dist_setup(args)

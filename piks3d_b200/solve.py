@@ -21,7 +21,7 @@ import time
 
 import numpy as np
 
-from . import Batch, PREC_FP32, PREC_FP64, Solver
+from . import Batch, PREC_FP32, PREC_FP64, SCHED_TILE_DATAFLOW, Solver
 
 
 class Convergence:
@@ -128,6 +128,7 @@ class Job:
         self.image, self.params, self.name, self.arrival = image, params, name, arrival
         self.make_image, self.porosity = make_image, porosity
         self.solver = None
+        self.tuned = None             # (TX, TY, TZ, schedule) chosen by the batch runner's autotuner
         self.conv = None
         self.phase = None             # "fp32" / "fp64"
         self.steps32 = 0
@@ -162,7 +163,12 @@ def footprint_bytes(image, params, precision="refined"):
     return f32 + f64 + moments + tables
 
 
-def _prepare(job, device, precision):
+# Tile shapes the batch runner's autotuner times on each job (the batch sweeps every member
+# with its own tile jobs in one dataflow launch, so candidates use the dataflow schedule).
+TUNE_CANDIDATES = ((4, 4, 4, SCHED_TILE_DATAFLOW), (8, 4, 4, SCHED_TILE_DATAFLOW), (4, 4, 8, SCHED_TILE_DATAFLOW))
+
+
+def _prepare(job, device, precision, autotune=False):
     if job.image is None:
         job.image = job.make_image()
     s = Solver(job.params, device=device)
@@ -170,6 +176,10 @@ def _prepare(job, device, precision):
         if precision in ("fp32", "refined"):
             s.set_precision(PREC_FP32)
         s.setup_physical_grid(job.image)
+        if autotune:
+            # times one sweep of each candidate on this image (its own stream: the batch's
+            # iterations may run meanwhile), keeps the fastest, resets the state
+            job.tuned = s.autotune(TUNE_CANDIDATES, sweeps=1)[0]
     except Exception:
         s.close()
         raise
@@ -179,16 +189,18 @@ def _prepare(job, device, precision):
 class BatchRunner:
     """Solves many jobs on one GPU as a continuously refilled batch: jobs are admitted while
     their estimated footprint fits the HBM budget and the batch has a free slot, preprocessed
-    on host threads while the GPU iterates, iterated together (piks_batch_*), checked every
+    (and, with `autotune`, their tile shape timed on the image) on host threads while the GPU
+    iterates, iterated together (piks_batch_*), checked every
     chkConvergeStep iterations, switched from FP32 to FP64 when their FP32 phase ends, and
     retired (state freed) as soon as they converge."""
 
     def __init__(self, device=0, precision="refined", tol=1e-4, eps=None, switch_eps=1e-6, switch_change=1e-6,
-                 max_members=64, hbm_budget=None, prep_threads=4, keep_fields=False):
+                 max_members=64, hbm_budget=None, prep_threads=4, keep_fields=False, autotune=True):
         import torch  # noqa: F401  (device memory query only)
         self.device, self.precision, self.tol, self.eps = device, precision, tol, eps
         self.switch_eps, self.max_members, self.keep_fields = switch_eps, max_members, keep_fields
         self.switch_change = switch_change
+        self.autotune = autotune
         if hbm_budget is None:
             import torch
             free, _total = torch.cuda.mem_get_info(device)
@@ -239,7 +251,7 @@ class BatchRunner:
         job.footprint = fp
         job.admitted = now
         self.reserved += fp
-        self.preparing.append((job, self.pool.submit(_prepare, job, self.device, self.precision)))
+        self.preparing.append((job, self.pool.submit(_prepare, job, self.device, self.precision, self.autotune)))
         return True
 
     def _join_ready(self, block=False):
@@ -300,7 +312,7 @@ class BatchRunner:
                 job.result = {"steps": job.steps, "steps32": job.steps32, "mass": float(mass[i]),
                               "permeability": float(perm[i]), "error": float(err[i]),
                               "converged": bool(conv), "diverged": job.conv.diverged,
-                              "estimate": job.conv.estimate}
+                              "estimate": job.conv.estimate, "tiles": job.tuned}
                 if self.keep_fields:
                     job.result["macro"] = job.solver.get_macro()
                 done.append(job)
