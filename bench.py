@@ -447,7 +447,22 @@ def small_batch(args, world, rank, local, device):
     import numpy as np
     import piks3d_b200 as pk
     from piks3d_b200.solve import BatchRunner, solve_one
+    from piks3d_b200 import images
+    from piks3d_b200.solve import Job
     sb = SMALL_BATCH
+    # untimed warm-up of both arms: 20 iterations of a small pack per velocity set, plain and
+    # batched in both precisions, so that neither timed arm pays the first use of a kernel
+    warm = []
+    for ncf in (2, 4):
+        p = pk.default_params(Nx=24, Ny=24, Nz=24, Nc_fundamental=ncf, Kn=1.0, pressDrop=1.0, wallExtOrder=1,
+                              maxStep=20, chkConvergeStep=10, eps=1e-8)
+        warm.append((images.sphere_pack(24, 0.45, 4.0, 8.0, seed=4242 + ncf), p))
+    for img, p in warm:
+        solve_one(img, p, device=local, precision="fp64", tol=TOL)
+    for prec in ("fp64", "fp32"):
+        wr = BatchRunner(device=local, precision=prec, tol=TOL, max_members=2, autotune=False)
+        wr.run([Job(img, p, name="warm%d" % i) for i, (img, p) in enumerate(warm)])
+        wr.close()
     jobs = batch_jobs(pk, args.batch_images, sb["seed"] + rank, args.max_step, sb["edges"], sb["kn_range"])
     barrier(world, device)
     t0 = time.perf_counter()

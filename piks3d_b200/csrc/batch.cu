@@ -1,7 +1,10 @@
 // Batches of solves (piks_batch_*, include/piks3d_gpu.h): several contexts on one device
 // iterated together. One iteration of a batch is, per precision class of its members, one
 // dataflow launch that sweeps every member's tile jobs, followed by each member's boundary
-// kernels; the sequence is captured once as a CUDA graph per iteration parity and replayed
+// kernels. The members' boundary chains are independent of one another, so they fork onto
+// side streams after the sweep and join before the next iteration: in the captured graph they
+// are parallel branches, and small members' launches overlap instead of running one after
+// another. The sequence is captured once as a CUDA graph per iteration parity and replayed
 // while the membership stays the same.
 #include <cuda_runtime.h>
 
@@ -34,11 +37,39 @@ struct piks_batch {
   int warm = 0;                  // iterations run since the last rebuild
   double *h_mass = nullptr;      // pinned, one per member
   size_t h_cap = 0;
+  // fork / join of the members' boundary chains: member m runs on side[m % side.size()]
+  std::vector<cudaStream_t> side;
+  std::vector<cudaEvent_t> joined;  // one per side stream
+  cudaEvent_t swept = nullptr;      // recorded on the batch stream after the sweeps
 };
 
 namespace {
 
 constexpr int kMaxClasses = 8;
+// Side streams for the members' boundary chains (more gives the graph no further overlap:
+// a boundary chain is a handful of dependent launches of a few microseconds each).
+constexpr int kMaxSide = 16;
+
+piks_status make_side_streams(piks_batch *b, size_t want) {
+  want = std::min<size_t>(want, kMaxSide);
+  if (!b->swept) {
+    piks_status st = cuda_check(cudaEventCreateWithFlags(&b->swept, cudaEventDisableTiming), "batch event");
+    if (st) return st;
+  }
+  while (b->side.size() < want) {
+    cudaStream_t s = nullptr;
+    cudaEvent_t e = nullptr;
+    piks_status st = cuda_check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "batch side stream");
+    if (!st) st = cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "batch event");
+    if (st) {
+      if (s) cudaStreamDestroy(s);
+      return st;
+    }
+    b->side.push_back(s);
+    b->joined.push_back(e);
+  }
+  return PIKS_OK;
+}
 
 void drop_graphs(piks_batch *b) {
   for (auto &g : b->graph)
@@ -121,6 +152,8 @@ piks_status rebuild(piks_batch *b) {
   for (auto &oc : b->classes)
     if (oc.d_items) cudaFree(oc.d_items);
   b->classes.swap(cls);
+  piks_status sst = make_side_streams(b, nm);
+  if (sst) return sst;
   b->versions.resize(nm);
   for (size_t m = 0; m < nm; ++m) b->versions[m] = b->members[m]->version;
   b->dirty = false;
@@ -139,7 +172,19 @@ void enqueue_batch_iteration(piks_batch *b, int parity) {
     launch_tile_sweep_batch(b->d_states, cl.d_items, (int)cl.items.size(), cl.fp32, cl.V, cl.slots, cl.tasks,
                             cl.stride, b->d_ctl + k, b->d_ctl + kMaxClasses, b->stream);
   }
-  for (piks_ctx *c : b->members) enqueue_boundaries(c, b->stream, c->iStep + 1 + parity);
+  const size_t ns = std::min(b->side.size(), b->members.size());
+  if (ns < 2) {
+    for (piks_ctx *c : b->members) enqueue_boundaries(c, b->stream, c->iStep + 1 + parity);
+    return;
+  }
+  cudaEventRecord(b->swept, b->stream);
+  for (size_t k = 0; k < ns; ++k) cudaStreamWaitEvent(b->side[k], b->swept, 0);
+  for (size_t m = 0; m < b->members.size(); ++m)
+    enqueue_boundaries(b->members[m], b->side[m % ns], b->members[m]->iStep + 1 + parity);
+  for (size_t k = 0; k < ns; ++k) {
+    cudaEventRecord(b->joined[k], b->side[k]);
+    cudaStreamWaitEvent(b->stream, b->joined[k], 0);
+  }
 }
 
 }  // namespace
@@ -281,6 +326,11 @@ piks_status piks_batch_destroy(piks_batch *b) {
   if (b->d_states) cudaFree(b->d_states);
   if (b->d_ctl) cudaFree(b->d_ctl);
   if (b->h_mass) cudaFreeHost(b->h_mass);
+  for (size_t k = 0; k < b->side.size(); ++k) {
+    cudaStreamDestroy(b->side[k]);
+    cudaEventDestroy(b->joined[k]);
+  }
+  if (b->swept) cudaEventDestroy(b->swept);
   cudaStreamDestroy(b->stream);
   delete b;
   return PIKS_OK;

@@ -1033,6 +1033,7 @@ piks_status piks_autotune(piks_ctx *c, const int32_t *cand, int32_t ncand, int32
     for (int r = 0; r < sweeps; ++r) enqueue_sweep(c, c->stream, epoch++);
     cudaEventRecord(e1, c->stream);
     if ((st = cuda_check(cudaEventSynchronize(e1), "autotune"))) break;
+    if ((st = check_sweep_error(c))) break;
     float ms = 0.f;
     cudaEventElapsedTime(&ms, e0, e1);
     const double per = ms / sweeps;
