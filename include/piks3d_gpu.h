@@ -127,6 +127,29 @@ piks_status piks_set_preprocessing(piks_ctx *ctx, int32_t where);
  * whole call (tile schedule, uploads and allocation included). */
 piks_status piks_setup_seconds(piks_ctx *ctx, double *out);
 
+/* ---- One box over several GPUs: x slabs (setupVirtualProcessGrid, mpiParams.F90:120-240,
+ * with mpi_xdim = nranks, mpi_ydim = mpi_zdim = 1; the halo exchange of solver.F90:146-170
+ * and :535-612). Each rank's context owns the x planes [xl, xu] of the reference's
+ * partition and reads two planes of each neighbour (periodic in x: the last rank's east
+ * neighbour is rank 0), one iteration behind, as the reference's MPI ranks do.
+ *
+ * piks_set_decomposition: before piks_setup_physical_grid (every rank passes the whole
+ * image); fails when a rank would own fewer than two planes. A slab context iterates one
+ * step per piks_iterate call; before each call the host moves, for each side, `send` of
+ * this rank to the neighbour's `recv` on the opposite side (NCCL send / recv, a peer copy,
+ * or a device copy when the ranks share a GPU), on the context's stream or ordered before
+ * it. piks_chk_converge computes the check on rank 0 (the plane x = 2, output.F90:89) and
+ * returns the others' stored values: the host broadcasts rank 0's triple. piks_run and
+ * batches refuse slab contexts. Replaces: the MPI calls of the reference; no counterpart
+ * in its call sequence. */
+piks_status piks_set_decomposition(piks_ctx *ctx, int32_t nranks, int32_t rank);
+/* out[4] = xl, xu (global 1-based x), nranks, rank. */
+piks_status piks_get_slab(piks_ctx *ctx, int32_t *out);
+/* Device buffers of the exchange that precedes the next iteration on `side` (0 west, 1 east):
+ * `send` (bytes[0] bytes) goes to the neighbour on that side, `recv` (bytes[1]) receives what
+ * that neighbour sends; valid until that iteration runs. One rank: NULL / 0 (no exchange). */
+piks_status piks_halo_buffers(piks_ctx *ctx, int32_t side, void **send, void **recv, int64_t *bytes);
+
 /* Makes the context enqueue on `stream` (a cudaStream_t); NULL restores its own stream. */
 piks_status piks_set_stream(piks_ctx *ctx, void *stream);
 

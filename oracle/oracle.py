@@ -61,6 +61,14 @@ def load():
         lib.oracle_get_coef.argtypes = [ctypes.c_void_p, ctypes.c_int, P(d)]
         lib.oracle_save.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int]
         lib.oracle_save.restype = ctypes.c_int
+        lib.oracle_create_rank.restype = ctypes.c_void_p
+        lib.oracle_create_rank.argtypes = [P(OracleParams), ctypes.c_char_p, i64, ctypes.c_int, i32, i32,
+                                           ctypes.c_char_p, ctypes.c_int]
+        lib.oracle_slab.argtypes = [ctypes.c_void_p, P(i32)]
+        lib.oracle_halo_size.restype = i64
+        lib.oracle_halo_size.argtypes = [ctypes.c_void_p]
+        lib.oracle_halo_send.argtypes = [ctypes.c_void_p, P(d), P(d)]
+        lib.oracle_halo_recv.argtypes = [ctypes.c_void_p, P(d), P(d)]
         _lib = lib
     return _lib
 
@@ -78,16 +86,18 @@ DIM_KEYS = ("Nx", "Ny", "Nz", "Nxtotal", "Nytotal", "Nztotal", "Ntotal", "Nc8", 
 
 
 class Oracle:
-    """Single-rank CPU restatement of PIKS3D (reference layout f(Ntotal, Nc8, 8))."""
+    """CPU restatement of PIKS3D for one rank (reference layout f(Ntotal, Nc8, 8) over the
+    rank's ghosted box); `nranks` > 1 makes it rank `rank` of an x-only process grid."""
 
-    def __init__(self, params, raw, nthreads=0):
+    def __init__(self, params, raw, nthreads=0, nranks=1, rank=0):
         lib = load()
         op = OracleParams()
         for name, _ in OracleParams._fields_:
             setattr(op, name, getattr(params, name) if not isinstance(params, dict) else params[name])
         data = bytes(np.ascontiguousarray(raw, dtype=np.uint8).reshape(-1)) if not isinstance(raw, (bytes, bytearray)) else bytes(raw)
         err = ctypes.create_string_buffer(256)
-        self.h = lib.oracle_create(ctypes.byref(op), data, len(data), int(nthreads), err, 256)
+        self.h = lib.oracle_create_rank(ctypes.byref(op), data, len(data), int(nthreads), int(nranks), int(rank),
+                                        err, 256)
         if not self.h:
             raise ValueError(err.value.decode())
         self.lib = lib
@@ -189,3 +199,78 @@ class Oracle:
 
     def save(self, out_dir, fmt):
         return self.lib.oracle_save(self.h, os.fsencode(out_dir), int(fmt))
+
+    def slab(self):
+        """{'xl', 'xu', 'xlg', 'nranks', 'rank'} (global 1-based x)."""
+        a = np.zeros(5, dtype=np.int32)
+        self.lib.oracle_slab(self.h, _i(a))
+        return dict(zip(("xl", "xu", "xlg", "nranks", "rank"), a.tolist()))
+
+    def halo_send(self):
+        """(west, east): the x messages the last iteration packed (solver.F90:535-612)."""
+        n = self.lib.oracle_halo_size(self.h)
+        w, e = np.zeros(n), np.zeros(n)
+        self.lib.oracle_halo_send(self.h, _d(w), _d(e))
+        return w, e
+
+    def halo_recv(self, west, east):
+        """Sets the messages received from the west / east neighbour for the next iteration."""
+        w = np.ascontiguousarray(west, dtype=np.float64)
+        e = np.ascontiguousarray(east, dtype=np.float64)
+        self.lib.oracle_halo_recv(self.h, _d(w), _d(e))
+
+
+class SlabOracle:
+    """`nranks` oracle ranks along x in one process, iterated together with the x messages
+    moved between them before every iteration as MPI moves them in solver.F90:146-170
+    (rank r receives its west message from rank r-1's east buffer and its east message from
+    rank r+1's west buffer, periodic in x)."""
+
+    def __init__(self, params, raw, nranks, nthreads=0):
+        self.ranks = [Oracle(params, raw, nthreads, nranks, r) for r in range(nranks)]
+
+    def close(self):
+        for o in self.ranks:
+            o.close()
+
+    def exchange(self):
+        n = len(self.ranks)
+        if n == 1:
+            return
+        sent = [o.halo_send() for o in self.ranks]
+        for r, o in enumerate(self.ranks):
+            o.halo_recv(sent[(r - 1) % n][1], sent[(r + 1) % n][0])
+
+    def iterate(self, n=1):
+        for _ in range(n):
+            self.exchange()
+            for o in self.ranks:
+                o.iterate(1)
+
+    def chk_converge(self):
+        """The west-most rank's (mass, k, error) (output.F90:89-162)."""
+        return self.ranks[0].chk_converge()
+
+    def macro(self):
+        """Rho, Ux, Uy, Uz over the whole box's interior, (Nz, Ny, Nx), from the owning ranks."""
+        parts = []
+        for o in self.ranks:
+            sl = o.slab()
+            a = o.macro()
+            lo = sl["xl"] - sl["xlg"]
+            parts.append([m[2:-2, 2:-2, lo:lo + sl["xu"] - sl["xl"] + 1] for m in a])
+        return [np.concatenate([p[q] for p in parts], axis=2) for q in range(4)]
+
+    def f_at_global(self, i, j, k):
+        """f rows (n, 8, Nc8) at global 1-based voxels from their owning ranks."""
+        i, j, k = (np.asarray(v, dtype=np.int64) for v in (i, j, k))
+        d0 = self.ranks[0].dims()
+        out = np.zeros((len(i), 8, d0["Nc8"]))
+        for o in self.ranks:
+            sl, d = o.slab(), o.dims()
+            sel = (i >= sl["xl"]) & (i <= sl["xu"])
+            if not sel.any():
+                continue
+            g = (i[sel] - sl["xlg"]) + (j[sel] + 1) * d["Nxtotal"] + (k[sel] + 1) * d["Nxtotal"] * d["Nytotal"]
+            out[sel] = o.f_at(g)
+        return out

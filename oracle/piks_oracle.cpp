@@ -104,7 +104,8 @@ struct Oracle {
   double Kn, pressDrop, accom;
   int Nx_base, Ny_base, Nz_base;
   int xmin, xmax, ymin, ymax, zmin, zmax;
-  // mpiParams (single rank)
+  // mpiParams: an x-only Cartesian grid of mpi_xdim ranks (mpi_ydim = mpi_zdim = 1)
+  int mpi_xdim = 1, rank = 0;
   int xl, xu, yl, yu, zl, zu, xlg, xug, ylg, yug, zlg, zug;
   int Nxtotal, Nytotal, Nztotal, Nxytotal, Nxsub, Nysub, Nzsub;
   size_t Ntotal;
@@ -175,10 +176,20 @@ bool setup_velocity_grid(Oracle &s, std::string &err) {
 }
 
 // ---------------------------------------------------------------------------------
-// mpiParams.F90 setupVirtualProcessGrid for dims = (1,1,1)
+// mpiParams.F90:150-191 setupVirtualProcessGrid for dims = (mpi_xdim, 1, 1); the rank's
+// Cartesian coordinate is its rank (x-only grid).
 void setup_process_grid(Oracle &s) {
-  int complete = (s.xmax - s.xmin) / 1;
-  s.xl = s.xmin; s.xu = s.xmin + complete - 1 + 1;
+  const int dims = s.mpi_xdim, c = s.rank;
+  int complete = (s.xmax - s.xmin) / dims;
+  int partial = (s.xmax - s.xmin) - complete * dims;
+  if (c + 1 <= partial) {
+    s.xl = s.xmin + (complete + 1) * c;
+    s.xu = s.xmin + (complete + 1) * (c + 1) - 1;
+  } else {
+    s.xl = s.xmin + complete * c + partial;
+    s.xu = s.xmin + complete * (c + 1) + partial - 1;
+  }
+  if ((c + 1) % dims == 0) s.xu = s.xu + 1;
   complete = (s.ymax - s.ymin) / 1;
   s.yl = s.ymin; s.yu = s.ymin + complete - 1 + 1;
   complete = (s.zmax - s.zmin) / 1;
@@ -313,11 +324,13 @@ bool setup_physical_grid(Oracle &s, const uint8_t *raw, int64_t nbytes, std::str
         bool gh = i < s.xmin || i > s.xmax || j < s.ymin || j > s.ymax || k < s.zmin || k > s.zmax;
         s.IMG(i, j, k) = gh ? GHOST : s.array3Dg[s.a3g(i, j, k)];
       }
-  // :546-671 wall labels from the product of fluid-neighbour primes
+  // :546-671 wall labels from the product of fluid-neighbour primes, over :512-523's
+  // bounds: the rank's own planes plus its ghost planes where a neighbour rank owns them
   s.nWall = 0;
+  const int lxl = s.xl == s.xmin ? s.xl : s.xlg, lxu = s.xu == s.xmax ? s.xu : s.xug;
   for (int k = s.zl; k <= s.zu; ++k)
     for (int j = s.yl; j <= s.yu; ++j)
-      for (int i = s.xl; i <= s.xu; ++i) {
+      for (int i = lxl; i <= lxu; ++i) {
         if (s.array3D[s.a3(i, j, k)] != SOLID) continue;
         int p = 1;
         const auto &g = s.array3Dg;
@@ -381,7 +394,8 @@ bool setup_physical_grid(Oracle &s, const uint8_t *raw, int64_t nbytes, std::str
   for (int o = 0; o < 8; ++o) {
     int sx = kSx[o], sy = kSy[o], sz = kSz[o];
     int bxl = s.xl, bxu = s.xu, byl = s.yl, byu = s.yu, bzl = s.zl, bzu = s.zu;
-    if (sx > 0) bxl = s.xl + 1; else bxu = s.xu - 1;
+    // :976-985: the first plane along the sweep is an inflow plane only at the box's edge
+    if (sx > 0) { if (s.xl == s.xmin) bxl = s.xl + 1; } else { if (s.xu == s.xmax) bxu = s.xu - 1; }
     if (sy > 0) byl = s.yl + 1; else byu = s.yu - 1;
     if (sz > 0) bzl = s.zl + 1; else bzu = s.zu - 1;
     auto &d = s.dir[o];
@@ -556,13 +570,20 @@ void wall_bc(Oracle &s, int q, std::vector<double> &fwZ) {
 
 // solver.F90:111-1940
 void iterate(Oracle &s) {
-  // :146-170 (single rank): the west/east messages are the buffers packed during the
-  // previous iteration; y/z neighbours are MPI_PROC_NULL. The 3-fold-corner part of the
-  // x message has no receiving map on one rank (map3CorWrcv/ErcvE are empty), so it is
-  // dropped here. (The reference's MPI receive count excludes it: with 3-fold corners in
-  // the planes x = 1, 2, Nx-1, Nx its MPI_WAITALL would report a truncated message.)
-  s.east_rcv = s.west_snd;
-  s.west_rcv = s.east_snd;
+  // :146-170: the west/east messages are the buffers packed during the previous
+  // iteration; y/z neighbours are MPI_PROC_NULL. On one rank the x neighbours are the rank
+  // itself; with several ranks the caller moves the messages before the call
+  // (oracle_halo_send / oracle_halo_recv). The 3-fold-corner part of the x message is not
+  // carried: on one rank it has no receiving map (map3CorWrcv/Ercv are empty), and with
+  // several ranks it fills fw slots of corners in the ghost planes, which no statement
+  // reads (the sweep's switch reads fw of a corner in the swept voxel's own x plane, the
+  // wall loop only its own walls' slots). (The reference's MPI receive count on one rank
+  // excludes it: with 3-fold corners in the planes x = 1, 2, Nx-1, Nx its MPI_WAITALL would
+  // report a truncated message.)
+  if (s.mpi_xdim == 1) {
+    s.east_rcv = s.west_snd;
+    s.west_rcv = s.east_snd;
+  }
   const int Nc8 = s.Nc8;
 #pragma omp parallel num_threads(s.nthreads)
   {
@@ -619,19 +640,21 @@ void iterate(Oracle &s) {
       for (int q = 0; q < s.nWall; ++q) wall_bc(s, q, fwZ);
     }
   }
-  // :1832-1862 inlet / outlet (whole ghosted y-z extent)
-  for (int k = s.zlg; k <= s.zug; ++k)
-    for (int j = s.ylg; j <= s.yug; ++j) {
-      long l = s.lid(s.xl, j, k);
-      for (int o : {1, 4, 5, 8})
-        for (int v = 1; v <= Nc8; ++v) s.F(l, v, o) = s.F(l - 1, v, o) + s.w[v - 1] * s.pressDrop;
-    }
-  for (int k = s.zlg; k <= s.zug; ++k)
-    for (int j = s.ylg; j <= s.yug; ++j) {
-      long l = s.lid(s.xu, j, k);
-      for (int o : {2, 3, 6, 7})
-        for (int v = 1; v <= Nc8; ++v) s.F(l, v, o) = s.F(l + 1, v, o) - s.w[v - 1] * s.pressDrop;
-    }
+  // :1832-1862 inlet on the west-most rank, outlet on the east-most (whole ghosted y-z extent)
+  if (s.xl == s.xmin)
+    for (int k = s.zlg; k <= s.zug; ++k)
+      for (int j = s.ylg; j <= s.yug; ++j) {
+        long l = s.lid(s.xl, j, k);
+        for (int o : {1, 4, 5, 8})
+          for (int v = 1; v <= Nc8; ++v) s.F(l, v, o) = s.F(l - 1, v, o) + s.w[v - 1] * s.pressDrop;
+      }
+  if (s.xu == s.xmax)
+    for (int k = s.zlg; k <= s.zug; ++k)
+      for (int j = s.ylg; j <= s.yug; ++j) {
+        long l = s.lid(s.xu, j, k);
+        for (int o : {2, 3, 6, 7})
+          for (int v = 1; v <= Nc8; ++v) s.F(l, v, o) = s.F(l + 1, v, o) - s.w[v - 1] * s.pressDrop;
+      }
   // :1867-1918 symmetry planes
   auto copy = [&](long l, int dst, int src) {
     for (int v = 1; v <= Nc8; ++v) s.F(l, v, dst) = s.F(l, v, src);
@@ -694,6 +717,10 @@ std::string es15_6(double v) {
 
 // output.F90:60-164
 void chk_converge(Oracle &s, const char *results_path, int verbose) {
+  // :89: only the west-most rank holds the plane x = 2 (its caller broadcasts the result,
+  // :162); with x-only ranks the inlet communicator has that one rank, so the reduction of
+  // :144-145 is the rank's own value
+  if (s.xl != s.xmin) return;
   int byl = s.yl + 1, byu = s.yu - 1, bzl = s.zl + 1, bzu = s.zu - 1;
   const long NX = s.Nxtotal, NXY = s.Nxytotal;
   const int col = 2 + 2;  // column + ghostLayers
@@ -836,8 +863,20 @@ extern "C" {
 
 void *oracle_create(const oracle_params *p, const uint8_t *raw, int64_t nbytes, int nthreads,
                     char *err, int errlen) {
+  return oracle_create_rank(p, raw, nbytes, nthreads, 1, 0, err, errlen);
+}
+
+void *oracle_create_rank(const oracle_params *p, const uint8_t *raw, int64_t nbytes, int nthreads,
+                         int32_t mpi_xdim, int32_t rank, char *err, int errlen) {
   auto *s = new Oracle();
   std::string e;
+  if (mpi_xdim < 1 || rank < 0 || rank >= mpi_xdim) {
+    if (err && errlen > 0) { std::strncpy(err, "bad rank / mpi_xdim", errlen - 1); err[errlen - 1] = 0; }
+    delete s;
+    return nullptr;
+  }
+  s->mpi_xdim = mpi_xdim;
+  s->rank = rank;
   // parameters.F90:87-136
   s->Nx = p->Nx; s->Ny = p->Ny; s->Nz = p->Nz;
   s->wallExtOrder = p->wallExtOrder; s->fluidlayer = p->fluidlayer; s->Ref_L = p->Ref_L;
@@ -852,7 +891,12 @@ void *oracle_create(const oracle_params *p, const uint8_t *raw, int64_t nbytes, 
   s->Nx = s->block_repx * s->Nx; s->Ny = s->block_repy * s->Ny; s->Nz = s->block_repz * s->Nz;
   s->xmin = 1; s->xmax = s->Nx; s->ymin = 1; s->ymax = s->Ny; s->zmin = 1; s->zmax = s->Nz;
   bool ok = setup_velocity_grid(*s, e);
-  if (ok) { setup_process_grid(*s); ok = setup_physical_grid(*s, raw, nbytes, e); }
+  if (ok) {
+    setup_process_grid(*s);
+    // two ghost planes come from each neighbour rank: every rank owns at least two planes
+    if (s->xu - s->xl + 1 < 2) { e = "fewer than two x planes per rank"; ok = false; }
+  }
+  if (ok) ok = setup_physical_grid(*s, raw, nbytes, e);
   if (ok) setup_flow(*s);
   if (!ok) {
     if (err && errlen > 0) { std::strncpy(err, e.c_str(), errlen - 1); err[errlen - 1] = 0; }
@@ -954,5 +998,21 @@ void oracle_get_coef(void *h, int octant, double *out) {
   std::copy(s->coef[octant - 1].begin(), s->coef[octant - 1].end(), out);
 }
 int oracle_save(void *h, const char *dir, int format) { return save_fields(*static_cast<Oracle *>(h), dir, format); }
+
+void oracle_slab(void *h, int32_t *out) {
+  auto *s = static_cast<Oracle *>(h);
+  out[0] = s->xl; out[1] = s->xu; out[2] = s->xlg; out[3] = s->mpi_xdim; out[4] = s->rank;
+}
+int64_t oracle_halo_size(void *h) { return (int64_t)static_cast<Oracle *>(h)->west_snd.size(); }
+void oracle_halo_send(void *h, double *west, double *east) {
+  auto *s = static_cast<Oracle *>(h);
+  std::copy(s->west_snd.begin(), s->west_snd.end(), west);
+  std::copy(s->east_snd.begin(), s->east_snd.end(), east);
+}
+void oracle_halo_recv(void *h, const double *west, const double *east) {
+  auto *s = static_cast<Oracle *>(h);
+  std::copy(west, west + s->west_rcv.size(), s->west_rcv.begin());
+  std::copy(east, east + s->east_rcv.size(), s->east_rcv.begin());
+}
 
 }  // extern "C"

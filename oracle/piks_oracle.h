@@ -6,8 +6,9 @@
  * reference leg of bench.py load this library, and only as the checker or as the timed
  * CPU baseline. The product (piks3d_b200/, libpiks3d_b200.so) never links or calls it.
  *
- * It restates, for one MPI rank (mpi_xdim = mpi_ydim = mpi_zdim = 1) and in the
- * reference's own full-box layout f(Ntotal, Nc8, 8), the arithmetic of
+ * It restates, for one MPI rank of an x-only process grid (mpi_xdim ranks, mpi_ydim =
+ * mpi_zdim = 1; one rank is the whole box) and in the reference's own layout f(Ntotal, Nc8,
+ * 8) over the rank's ghosted box, the arithmetic of
  *   src/parameters.F90  initParams                 (:87-136)
  *   src/gaussHermite.F90 + src/velocityGrid.F90    (:90-192)
  *   src/physicalGrid.F90 setupPhysicalGrid         (:217-1625)
@@ -49,6 +50,10 @@ typedef struct oracle_params {
  * err on failure (invalid voxel byte, unsupported Nc_fundamental, short image). */
 void *oracle_create(const oracle_params *p, const uint8_t *raw, int64_t nbytes,
                     int nthreads, char *err, int errlen);
+/* The same for rank `rank` of mpi_xdim ranks along x (mpiParams.F90:150-191 with dims =
+ * (mpi_xdim, 1, 1)); every rank owns at least two x planes. */
+void *oracle_create_rank(const oracle_params *p, const uint8_t *raw, int64_t nbytes,
+                         int nthreads, int32_t mpi_xdim, int32_t rank, char *err, int errlen);
 void oracle_destroy(void *h);
 
 /* `nsteps` calls of iterate; iStep advances by one per call. */
@@ -81,6 +86,17 @@ void oracle_get_coef(void *h, int octant, double *out);   /* Nstencil x 9 */
 
 /* Field writers of output.F90 (VTI/VTK/Tecplot, proc 000) into directory `dir`. */
 int oracle_save(void *h, const char *dir, int format);
+
+/* [xl, xu, xlg, mpi_xdim, rank] of the rank's slab (global 1-based x). */
+void oracle_slab(void *h, int32_t *out);
+/* x messages of solver.F90:146-170 / :535-612 (the face part, oracle_halo_size doubles
+ * each): oracle_halo_send copies out the buffers the last iteration packed (what the rank
+ * sends west / east at the start of the next one); oracle_halo_recv sets what it receives
+ * from its west / east neighbour for the next iteration. With mpi_xdim = 1 iterate moves
+ * them itself. */
+int64_t oracle_halo_size(void *h);
+void oracle_halo_send(void *h, double *west, double *east);
+void oracle_halo_recv(void *h, const double *west, const double *east);
 
 #ifdef __cplusplus
 }

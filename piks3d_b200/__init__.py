@@ -82,6 +82,9 @@ def load_library(path=LIB_PATH):
         "piks_set_stream": (i32, [c_void_p, c_void_p]),
         "piks_set_preprocessing": (i32, [c_void_p, i32]),
         "piks_setup_seconds": (i32, [c_void_p, P(dbl)]),
+        "piks_set_decomposition": (i32, [c_void_p, i32, i32]),
+        "piks_get_slab": (i32, [c_void_p, P(i32)]),
+        "piks_halo_buffers": (i32, [c_void_p, i32, P(c_void_p), P(c_void_p), P(i64)]),
         "piks_kernel_times": (i32, [c_void_p, P(dbl), i32, i32]),
         "piks_kernel_names": (ctypes.c_char_p, []),
         "piks_enable_timing": (i32, [c_void_p, i32]),
@@ -227,6 +230,25 @@ class Solver:
         a = (ctypes.c_double * 4)()
         _check(self.lib.piks_setup_seconds(self._ctx, a))
         return tuple(a)
+
+    def set_decomposition(self, nranks, rank):
+        """Makes this context rank `rank` of `nranks` x slabs of the box (before
+        setup_physical_grid, which then takes the whole image on every rank)."""
+        _check(self.lib.piks_set_decomposition(self._ctx, int(nranks), int(rank)))
+
+    def slab(self):
+        """{'xl', 'xu', 'nranks', 'rank'}: the owned x planes (global, 1-based)."""
+        a = (ctypes.c_int32 * 4)()
+        _check(self.lib.piks_get_slab(self._ctx, a))
+        return dict(zip(("xl", "xu", "nranks", "rank"), list(a)))
+
+    def halo_buffers(self, side):
+        """(send_ptr, recv_ptr, send_bytes, recv_bytes) of the exchange on `side` (0 west,
+        1 east) that precedes the next iteration; device pointers (0 for one rank)."""
+        snd, rcv = ctypes.c_void_p(), ctypes.c_void_p()
+        b = (ctypes.c_int64 * 2)()
+        _check(self.lib.piks_halo_buffers(self._ctx, int(side), ctypes.byref(snd), ctypes.byref(rcv), b))
+        return snd.value or 0, rcv.value or 0, b[0], b[1]
 
     def set_tiles(self, tx, ty=None, tz=None):
         """Tile shape of the sweep schedule (0 = per-node hyperplanes); applies at the next

@@ -217,6 +217,7 @@ piks_status piks_batch_add(piks_batch *b, piks_ctx *c) {
   if (!c->have_geometry) return fail(PIKS_ERR_STATE, "batch member has no device state");
   if (c->device != b->device) return fail(PIKS_ERR_ARG, "batch member lives on another device");
   if (!c->use_tiles) return fail(PIKS_ERR_ARG, "batch members need the tile schedule");
+  if (c->setup.nranks > 1) return fail(PIKS_ERR_ARG, "a slab of a decomposed box cannot join a batch");
   if (b->members.size() >= 4096) return fail(PIKS_ERR_ARG, "batch holds at most 4096 members");
   if (std::find(b->members.begin(), b->members.end(), c) != b->members.end()) return PIKS_OK;
   cudaSetDevice(b->device);

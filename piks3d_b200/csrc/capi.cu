@@ -95,11 +95,13 @@ void release(piks_ctx *c, void *p) {
 }
 
 // Sizes of the precision-dependent state: f, fw and one ghost plane (in elements).
-struct StateSizes { size_t h, fw, plane; };
+struct StateSizes { size_t h, fw, plane, hsend[2], hrecv[2]; };
 StateSizes state_sizes(const piks_ctx *c) {
   const Geometry &g = c->geo;
   const size_t Nc8 = (size_t)c->vel.Nc8;
-  return {((size_t)g.NF + g.NB) * 8 * Nc8, (size_t)g.nCorner * 8 * Nc8, (size_t)g.Ny * g.Nz * 4 * Nc8};
+  return {((size_t)g.NF + g.NB) * 8 * Nc8, (size_t)g.nCorner * 8 * Nc8, (size_t)g.Ny * g.Nz * 4 * Nc8,
+          {g.halo_send[0].size() * 4 * Nc8, g.halo_send[1].size() * 4 * Nc8},
+          {g.halo_recv[0].size() * 4 * Nc8, g.halo_recv[1].size() * 4 * Nc8}};
 }
 
 // Allocates (zeroed) f, fw and the two pairs of ghost planes in precision `prec`
@@ -123,6 +125,15 @@ piks_status alloc_state(piks_ctx *c, int prec) {
       if ((st = zeros(c, z.plane, &s.ghostE32[b]))) return st;
     }
   }
+  // the x messages of a slab start as zeros (flow.F90:115-163 allocate the buffers zeroed)
+  for (int side = 0; side < 2; ++side) {
+    if (!z.hsend[side] && !z.hrecv[side]) continue;
+    for (int b = 0; b < 2; ++b)
+      if ((st = prec == PIKS_PREC_FP64 ? zeros(c, z.hsend[side], &s.hsend[side][b])
+                                       : zeros(c, z.hsend[side], &s.hsend32[side][b]))) return st;
+    if ((st = prec == PIKS_PREC_FP64 ? zeros(c, z.hrecv[side], &s.hrecv[side]) : zeros(c, z.hrecv[side], &s.hrecv32[side])))
+      return st;
+  }
   return PIKS_OK;
 }
 
@@ -132,10 +143,20 @@ void free_state(piks_ctx *c, int prec) {
     release(c, s.h); release(c, s.fw);
     for (int b = 0; b < 2; ++b) { release(c, s.ghostW[b]); release(c, s.ghostE[b]); s.ghostW[b] = s.ghostE[b] = nullptr; }
     s.h = s.fw = nullptr;
+    for (int side = 0; side < 2; ++side) {
+      for (int b = 0; b < 2; ++b) { release(c, s.hsend[side][b]); s.hsend[side][b] = nullptr; }
+      release(c, s.hrecv[side]);
+      s.hrecv[side] = nullptr;
+    }
   } else {
     release(c, s.h32); release(c, s.fw32);
     for (int b = 0; b < 2; ++b) { release(c, s.ghostW32[b]); release(c, s.ghostE32[b]); s.ghostW32[b] = s.ghostE32[b] = nullptr; }
     s.h32 = s.fw32 = nullptr;
+    for (int side = 0; side < 2; ++side) {
+      for (int b = 0; b < 2; ++b) { release(c, s.hsend32[side][b]); s.hsend32[side][b] = nullptr; }
+      release(c, s.hrecv32[side]);
+      s.hrecv32[side] = nullptr;
+    }
   }
 }
 
@@ -192,7 +213,11 @@ void enqueue_boundaries_timed(piks_ctx *c, cudaStream_t st, int n) {
   const int cap = n & 1, prev = (n - 1) & 1;
   const bool f32 = c->prec == PIKS_PREC_FP32;
   { Timed t(c, KT_COMMIT); f32 ? launch_commit32(s, st) : launch_commit(s, st); }
-  { Timed t(c, KT_CAPTURE); f32 ? launch_capture32(s, cap, st) : launch_capture(s, cap, st); }
+  {
+    Timed t(c, KT_CAPTURE);
+    f32 ? launch_capture32(s, cap, st) : launch_capture(s, cap, st);
+    if (c->setup.nranks > 1) launch_halo(s, f32, cap, st);  // solver.F90:535-560 on a slab
+  }
   {
     Timed t(c, KT_WALLS);
     const auto &ls = c->geo.level_start;
@@ -494,7 +519,9 @@ piks_status piks_setup_physical_grid(piks_ctx *c, const uint8_t *raw, int64_t nb
     st = preprocess_box(c->setup, raw, nbytes, box, err);
     if (st) return fail(st, err);
     const auto t1 = clk::now();
-    if (c->device >= 0 && c->prep == PIKS_PREP_DEVICE) {
+    // (a slab of an x-decomposed box is classified on the host: its node set includes the
+    // read voxels of the neighbour ranks' planes)
+    if (c->device >= 0 && c->prep == PIKS_PREP_DEVICE && c->setup.nranks == 1) {
       st = classify_device(c->setup, box, c->geo, c->stream, err);
       if (st) return fail(st, err);
     } else {
@@ -542,6 +569,12 @@ piks_status piks_setup_physical_grid(piks_ctx *c, const uint8_t *raw, int64_t nb
   UP(g.plane_x1, plane_x1, pi); UP(g.plane_xN, plane_xN, pi);
   UP(g.sym_node, sym_node, pi); UP(g.sym_flag, sym_flag, pu8);
   UP(g.flux_list, flux_list, pi);
+  for (int side = 0; side < 2; ++side) {
+    s.nhalo_send[side] = (int)g.halo_send[side].size();
+    s.nhalo_recv[side] = (int)g.halo_recv[side].size();
+    if (s.nhalo_send[side]) UP(g.halo_send[side], halo_send[side], pi);
+    if (s.nhalo_recv[side]) UP(g.halo_recv[side], halo_recv[side], pi);
+  }
   {
     // per-velocity sweep constants: cx cy cz w; the products c*C of the upwind terms
     // (C1 = 2/ds second order, 1/ds first order; C2 = -0.5/ds) for x, y, z; the
@@ -622,6 +655,8 @@ piks_status piks_iterate(piks_ctx *c, int32_t nsteps) {
   if (c->device < 0) return fail(PIKS_ERR_NOT_FOUND, "host-only context (device -1) cannot iterate");
   if (!c->have_geometry) return fail(PIKS_ERR_STATE, "piks_setup_physical_grid has not been called");
   if (nsteps < 0) return fail(PIKS_ERR_ARG, "nsteps < 0");
+  if (c->setup.nranks > 1 && nsteps > 1)
+    return fail(PIKS_ERR_ARG, "a slab context iterates one step per call (its halos are exchanged between calls)");
   cudaSetDevice(c->device);
   // The dataflow sweep takes the iteration number as its epoch and per-kernel timing records
   // events, so both launch plainly; otherwise one graph launch per iteration replaces about
@@ -670,6 +705,15 @@ piks_status piks_chk_converge(piks_ctx *c, double *mass, double *perm, double *e
   if (!c) return fail(PIKS_ERR_ARG, "null context");
   if (!c->have_geometry) return fail(PIKS_ERR_STATE, "piks_setup_physical_grid has not been called");
   cudaSetDevice(c->device);
+  if (!c->geo.wglob) {
+    // output.F90:89: only the west-most slab computes the check; the others keep their values
+    piks_status st = check_sweep_error(c);
+    if (st) return st;
+    if (mass) *mass = c->mass;
+    if (perm) *perm = c->permeability;
+    if (err) *err = c->error;
+    return PIKS_OK;
+  }
   {
     Timed t(c, KT_FLUX);
     launch_check(c, c->stream);
@@ -844,6 +888,8 @@ piks_status check_and_report(piks_ctx *c, int step, const char *results_path, in
 // iteration run in *last.
 piks_status run_loop(piks_ctx *c, int first_step, double eps, bool stop_on_stall, const char *results_path,
                      const char *out_dir, int verbose, int *last) {
+  if (c->setup.nranks > 1)
+    return fail(PIKS_ERR_STATE, "a slab context is driven by its host (one iteration and one halo exchange at a time)");
   const piks_params &p = c->setup.p;
   piks_status st;
   double best = HUGE_VAL;
@@ -939,6 +985,7 @@ piks_status piks_set_precision(piks_ctx *c, int32_t precision) {
     for (int b = 0; b < 2; ++b) {
       launch_widen(s.ghostW32[b], s.ghostW[b], z.plane, c->stream);
       launch_widen(s.ghostE32[b], s.ghostE[b], z.plane, c->stream);
+      for (int side = 0; side < 2; ++side) launch_widen(s.hsend32[side][b], s.hsend[side][b], z.hsend[side], c->stream);
     }
   } else {
     launch_narrow(s.h, s.h32, z.h, c->stream);
@@ -946,6 +993,7 @@ piks_status piks_set_precision(piks_ctx *c, int32_t precision) {
     for (int b = 0; b < 2; ++b) {
       launch_narrow(s.ghostW[b], s.ghostW32[b], z.plane, c->stream);
       launch_narrow(s.ghostE[b], s.ghostE32[b], z.plane, c->stream);
+      for (int side = 0; side < 2; ++side) launch_narrow(s.hsend[side][b], s.hsend32[side][b], z.hsend[side], c->stream);
     }
   }
   st = cuda_check(cudaGetLastError(), "precision convert");
@@ -1126,6 +1174,8 @@ piks_status piks_geometry_array(piks_ctx *c, const char *name, void *out, int64_
   ARR("bcorner", g.bcorner) ARR("roles", g.roles) ARR("commit", g.commit) ARR("plane_x1", g.plane_x1)
   ARR("plane_xN", g.plane_xN) ARR("sym_node", g.sym_node) ARR("sym_flag", g.sym_flag)
   ARR("flux_list", g.flux_list) ARR("tasks", g.tasks) ARR("hyper_start", g.hyper_start) ARR("cx", c->vel.cx) ARR("cy", c->vel.cy) ARR("cz", c->vel.cz) ARR("w", c->vel.w)
+  ARR("halo_send_w", g.halo_send[0]) ARR("halo_send_e", g.halo_send[1])
+  ARR("halo_recv_w", g.halo_recv[0]) ARR("halo_recv_e", g.halo_recv[1])
   const TileJobs &tj = c->tiles;
   ARR("tile_rows", tj.rows) ARR("tile_row_begin", tj.row_begin) ARR("tile_row_count", tj.row_count)
   ARR("tile_tasks", tj.tasks)
@@ -1187,6 +1237,54 @@ piks_status piks_set_preprocessing(piks_ctx *c, int32_t where) {
 piks_status piks_setup_seconds(piks_ctx *c, double *out) {
   if (!c || !out) return fail(PIKS_ERR_ARG, "null argument");
   for (int i = 0; i < 4; ++i) out[i] = c->setup_seconds[i];
+  return PIKS_OK;
+}
+
+piks_status piks_set_decomposition(piks_ctx *c, int32_t nranks, int32_t rank) {
+  if (!c) return fail(PIKS_ERR_ARG, "null context");
+  if (c->have_host_geometry) return fail(PIKS_ERR_STATE, "piks_set_decomposition must come before piks_setup_physical_grid");
+  std::string err;
+  piks_status st = set_slab(c->setup, nranks, rank, err);
+  if (st) return fail(st, err);
+  return PIKS_OK;
+}
+
+piks_status piks_get_slab(piks_ctx *c, int32_t *out) {
+  if (!c || !out) return fail(PIKS_ERR_ARG, "null argument");
+  out[0] = c->setup.xl; out[1] = c->setup.xu; out[2] = c->setup.nranks; out[3] = c->setup.rank;
+  return PIKS_OK;
+}
+
+piks_status piks_halo_buffers(piks_ctx *c, int32_t side, void **send, void **recv, int64_t *bytes) {
+  if (!c || !send || !recv || !bytes) return fail(PIKS_ERR_ARG, "null argument");
+  if (side != 0 && side != 1) return fail(PIKS_ERR_ARG, "side must be 0 (west) or 1 (east)");
+  if (!c->have_geometry) return fail(PIKS_ERR_STATE, "piks_setup_physical_grid has not been called");
+  *send = *recv = nullptr;
+  bytes[0] = bytes[1] = 0;
+  if (c->setup.nranks == 1) return PIKS_OK;  // one rank exchanges with itself inside the iteration
+  const DevState &s = c->ds;
+  const bool f32 = c->prec == PIKS_PREC_FP32;
+  const size_t e = f32 ? sizeof(float) : sizeof(double);
+  const int par = c->iStep & 1;  // the buffers the last iteration packed / the next one reads
+  const StateSizes z = state_sizes(c);
+  const bool edge = side == 0 ? c->geo.wglob : c->geo.eglob;
+  if (edge) {
+    // the periodic pair of the first and last slab: the plane x = 1 (sent west, read by
+    // the outlet) and the plane x = Nx (sent east, read by the inlet), one iteration behind
+    if (side == 0) {
+      *send = f32 ? (void *)s.ghostE32[par] : (void *)s.ghostE[par];
+      *recv = f32 ? (void *)s.ghostW32[par] : (void *)s.ghostW[par];
+    } else {
+      *send = f32 ? (void *)s.ghostW32[par] : (void *)s.ghostW[par];
+      *recv = f32 ? (void *)s.ghostE32[par] : (void *)s.ghostE[par];
+    }
+    bytes[0] = bytes[1] = (int64_t)(z.plane * e);
+    return PIKS_OK;
+  }
+  *send = f32 ? (void *)s.hsend32[side][par] : (void *)s.hsend[side][par];
+  *recv = f32 ? (void *)s.hrecv32[side] : (void *)s.hrecv[side];
+  bytes[0] = (int64_t)(z.hsend[side] * e);
+  bytes[1] = (int64_t)(z.hrecv[side] * e);
   return PIKS_OK;
 }
 

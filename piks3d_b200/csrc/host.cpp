@@ -117,6 +117,29 @@ piks_status make_setup(const piks_params &p, Setup &s, std::string &err) {
   s.Nx = p.block_repx * Nx; s.Ny = p.block_repy * p.Ny; s.Nz = p.block_repz * p.Nz;
   s.ds = 1.0 / (s.Nx - 1 - 2 * p.fluidlayer);   // physicalGrid.F90:228
   s.mu = std::sqrt(kPi / 2.0) / p.Kn;          // flow.F90:90
+  s.nranks = 1; s.rank = 0; s.xl = 1; s.xu = s.Nx;
+  return PIKS_OK;
+}
+
+// mpiParams.F90:165-175: the xmax - xmin plane gaps are dealt out in equal parts, the first
+// `partial` ranks one more, and the last rank also takes the plane xmax.
+piks_status set_slab(Setup &s, int nranks, int rank, std::string &err) {
+  if (nranks < 1 || rank < 0 || rank >= nranks) { err = "rank must be in [0, nranks)"; return PIKS_ERR_ARG; }
+  const int xmin = 1, xmax = s.Nx;
+  const int complete = (xmax - xmin) / nranks, partial = (xmax - xmin) - complete * nranks;
+  auto bounds = [&](int c, int &xl, int &xu) {
+    if (c + 1 <= partial) { xl = xmin + (complete + 1) * c; xu = xmin + (complete + 1) * (c + 1) - 1; }
+    else { xl = xmin + complete * c + partial; xu = xmin + complete * (c + 1) + partial - 1; }
+    if ((c + 1) % nranks == 0) xu = xu + 1;
+  };
+  for (int c = 0; c < nranks; ++c) {
+    int l, u;
+    bounds(c, l, u);
+    if (u - l + 1 < 2) { err = "every rank needs at least two x planes (Nx too small for nranks)"; return PIKS_ERR_ARG; }
+  }
+  s.nranks = nranks;
+  s.rank = rank;
+  bounds(rank, s.xl, s.xu);
   return PIKS_OK;
 }
 
@@ -405,6 +428,7 @@ void classify_host(const Setup &s, const std::vector<uint8_t> &box, Geometry &g)
     return box[(size_t)(i + 1) + (size_t)(j + 1) * BGX + (size_t)(k + 1) * BGX * BGY];
   };
   g.Nx = Nx; g.Ny = Ny; g.Nz = Nz; g.GX = Nx + 4; g.GY = Ny + 4; g.GZ = Nz + 4;
+  g.xl = s.xl; g.xu = s.xu; g.wglob = s.xl == 1; g.eglob = s.xu == Nx;
   const size_t NG = (size_t)g.GX * g.GY * g.GZ;
   g.label.assign(NG, L_GHOST);
   // labels (physicalGrid.F90:546-671); ghosts are not fluid here
@@ -441,25 +465,28 @@ void classify_host(const Setup &s, const std::vector<uint8_t> &box, Geometry &g)
           if (real(i, j, k + d)) keep[g.ghost_index(i, j, k + d)] = 1;
         }
       }
+  // Nodes: the owned fluid voxels, then the other voxels of the slab's window that are read
+  // (owned solids as above; on a side shared with a neighbour rank, the read voxels of its
+  // two ghost planes, fluid or solid). For one rank the window is the box.
   g.nodemap.assign(NG, -2);
   g.node_g.clear();
   g.NF = 0;
-  for (int pass = 0; pass < 2; ++pass)
+  for (int pass = 0; pass < 2; ++pass) {
     for (int k = 1; k <= Nz; ++k)
       for (int j = 1; j <= Ny; ++j)
         for (int i = 1; i <= Nx; ++i) {
           int64_t gi = g.ghost_index(i, j, k);
-          bool fluid = LAB(i, j, k) == L_FLUID;
+          const bool fluid = LAB(i, j, k) == L_FLUID, own = i >= g.xl && i <= g.xu;
           if (pass == 0) {
             g.nodemap[gi] = -1;
-            if (fluid) { g.nodemap[gi] = (int32_t)g.node_g.size(); g.node_g.push_back((int32_t)gi); }
-          } else if (!fluid && keep[gi]) {
+            if (fluid && own) { g.nodemap[gi] = (int32_t)g.node_g.size(); g.node_g.push_back((int32_t)gi); }
+          } else if (!(fluid && own) && g.in_window(i) && (fluid || keep[gi])) {
             g.nodemap[gi] = (int32_t)g.node_g.size();
             g.node_g.push_back((int32_t)gi);
           }
         }
-  g.NF = 0;
-  for (int32_t gi : g.node_g) if (g.label[gi] == L_FLUID) g.NF++;
+    if (pass == 0) g.NF = (int32_t)g.node_g.size();
+  }
   g.NB = (int32_t)g.node_g.size() - g.NF;
 
   // walls in raster (vecWall) order, 3-fold corners numbered in the same order
@@ -468,7 +495,7 @@ void classify_host(const Setup &s, const std::vector<uint8_t> &box, Geometry &g)
   g.nCorner = 0;
   for (int k = 1; k <= Nz; ++k)
     for (int j = 1; j <= Ny; ++j)
-      for (int i = 1; i <= Nx; ++i) {
+      for (int i = g.xl; i <= g.xu; ++i) {
         int lab = LAB(i, j, k);
         if (!is_wall_label(lab)) continue;
         int node = g.nodemap[g.ghost_index(i, j, k)];
@@ -505,8 +532,9 @@ void wall_extrapolation(const Setup &s, const Geometry &g, int i, int j, int k, 
     int v = LAB(id, jd, kd);
     uint8_t fm = face_mask(v);
     bool first = false;
-    if ((fm & FACE_W) && id == 2 && LAB(1, jd, kd) == L_FLUID) first = true;
-    if ((fm & FACE_E) && id == Nx - 1 && LAB(Nx, jd, kd) == L_FLUID) first = true;
+    // the rank's own first / last plane (physicalGrid.F90:903-906 use xl, xu)
+    if ((fm & FACE_W) && id == g.xl + 1 && LAB(g.xl, jd, kd) == L_FLUID) first = true;
+    if ((fm & FACE_E) && id == g.xu - 1 && LAB(g.xu, jd, kd) == L_FLUID) first = true;
     if ((fm & FACE_S) && jd == 2 && LAB(id, 1, kd) == L_FLUID) first = true;
     if ((fm & FACE_N) && jd == Ny - 1 && LAB(id, Ny, kd) == L_FLUID) first = true;
     if ((fm & FACE_B) && kd == 2 && LAB(id, jd, 1) == L_FLUID) first = true;
@@ -519,7 +547,7 @@ void wall_extrapolation(const Setup &s, const Geometry &g, int i, int j, int k, 
 // (see Geometry::wall_nb).
 void wall_neighbours(const Geometry &g, const WProg *P, int i, int j, int k, int32_t *nb) {
   const int Nx = g.Nx, Ny = g.Ny, Nz = g.Nz;
-  auto real = [&](int ii, int jj, int kk) { return ii >= 1 && ii <= Nx && jj >= 1 && jj <= Ny && kk >= 1 && kk <= Nz; };
+  auto real = [&](int ii, int jj, int kk) { return g.in_window(ii) && jj >= 1 && jj <= Ny && kk >= 1 && kk <= Nz; };
   for (int t = 0; t < 6; ++t) nb[t] = -1;
   for (int fi = 0; fi < P->nface; ++fi) {
     int dir = P->face[fi].dir;
@@ -542,7 +570,12 @@ piks_status finish_geometry(const Setup &s, Geometry &g, std::string &err) {
   // node*8 + slot codes of the sweep must stay below 2^30
   if ((int64_t)g.node_g.size() * 8 >= (int64_t)1 << 30) { err = "image too large (more than 2^27 nodes read by the solver)"; return PIKS_ERR_ARG; }
   auto LAB = [&](int i, int j, int k) -> int { return g.label[g.ghost_index(i, j, k)]; };
-  auto real = [&](int i, int j, int k) { return i >= 1 && i <= Nx && j >= 1 && j <= Ny && k >= 1 && k <= Nz; };
+  // voxels of the slab's window (the box for one rank) and the rank's own voxels
+  auto real = [&](int i, int j, int k) { return g.in_window(i) && j >= 1 && j <= Ny && k >= 1 && k <= Nz; };
+  auto owned = [&](int i, int j, int k) { return i >= g.xl && i <= g.xu && j >= 1 && j <= Ny && k >= 1 && k <= Nz; };
+  // first / last swept x plane of an octant: the box's inflow plane is not swept
+  // (physicalGrid.F90:976-985); a plane next to a neighbour rank's ghost planes is
+  const int xs_lo = g.wglob ? 2 : g.xl, xs_hi = g.eglob ? Nx - 1 : g.xu;
   const int GX = g.GX, GXY = g.GX * g.GY;
 
   // Dependency levels: a wall whose extrapolation reads another wall's slots must see
@@ -581,9 +614,9 @@ piks_status finish_geometry(const Setup &s, Geometry &g, std::string &err) {
     std::memset(zrule, -1, sizeof zrule);
     for (const SwitchRow &r : kSwitch) (r.axis == 0 ? yrule : zrule)[r.o][r.label] = (int8_t)r.src;
     auto swept = [&](int i, int j, int k, int o) {
-      if (!real(i, j, k) || LAB(i, j, k) != L_FLUID) return false;
+      if (!owned(i, j, k) || LAB(i, j, k) != L_FLUID) return false;
       int sx = oct_sx(o), sy = oct_sy(o), sz = oct_sz(o);
-      bool ix = sx > 0 ? (i >= 2) : (i <= Nx - 1);
+      bool ix = sx > 0 ? (i >= xs_lo) : (i <= xs_hi);
       bool iy = sy > 0 ? (j >= 2) : (j <= Ny - 1);
       bool iz = sz > 0 ? (k >= 2) : (k <= Nz - 1);
       return ix && iy && iz;
@@ -613,9 +646,13 @@ piks_status finish_geometry(const Setup &s, Geometry &g, std::string &err) {
 
   // Sweep tasks ordered by hyperplane (see Geometry::tasks).
   {
-    const int nhyper = (Nx - 1) + (Ny - 1) + (Nz - 1) - 2;  // u+v+w from 3 to Nx+Ny+Nz-3
+    // u counts x planes from the plane before the first swept one (v, w likewise in y, z)
+    const int ux_pos = g.wglob ? 1 : g.xl - 1, ux_neg = g.eglob ? Nx : g.xu + 1;
+    const int umax = std::max(g.xu - ux_pos, ux_neg - g.xl);
+    const int nhyper = umax + (Ny - 1) + (Nz - 1) - 2;  // u+v+w from 3 to umax+Ny+Nz-3
     std::vector<int64_t> count(nhyper + 1, 0);
     auto local = [&](int i, int n, int sgn) { return sgn > 0 ? i - 1 : n - i; };
+    auto local_x = [&](int i, int sgn) { return sgn > 0 ? i - ux_pos : ux_neg - i; };
     auto upwind_code = [&](int i, int j, int k, int o, int role, bool first_order_zero) -> int32_t {
       // role: 0/1 x1/x2 (slot o as is), 2..5 y1, y2, z1, z2 (resolved switch roles)
       if (first_order_zero) return -2;
@@ -635,14 +672,16 @@ piks_status finish_geometry(const Setup &s, Geometry &g, std::string &err) {
       const int sx = oct_sx(o), sy = oct_sy(o), sz = oct_sz(o);
       for (int k = 1; k <= Nz; ++k)
         for (int j = 1; j <= Ny; ++j)
-          for (int i = 1; i <= Nx; ++i) {
+          for (int i = g.xl; i <= g.xu; ++i) {
             if (LAB(i, j, k) != L_FLUID) continue;
-            const int u = local(i, Nx, sx), v = local(j, Ny, sy), w = local(k, Nz, sz);
+            const int u = local_x(i, sx), v = local(j, Ny, sy), w = local(k, Nz, sz);
             if (u < 1 || v < 1 || w < 1) continue;  // inflow planes are not swept
             const int h = u + v + w - 3;
             if (pass == 0) { ocount[(size_t)o][(size_t)h]++; continue; }
             // first-order flags (physicalGrid.F90:1269-1298 and the seven sibling blocks)
-            const bool fx = (u == 1) || (face_mask(LAB(i - sx, j, k)) & (sx > 0 ? FACE_E : FACE_W));
+            // the x rule in its label form: a ghost two planes upwind (the box's edge), not
+            // the first swept plane of the slab, which reads its neighbour's planes
+            const bool fx = LAB(i - 2 * sx, j, k) == L_GHOST || (face_mask(LAB(i - sx, j, k)) & (sx > 0 ? FACE_E : FACE_W));
             const bool fy = (v == 1) || (face_mask(LAB(i, j - sy, k)) & (sy > 0 ? FACE_N : FACE_S));
             const bool fz = (w == 1) || (face_mask(LAB(i, j, k - sz)) & (sz > 0 ? FACE_F : FACE_B));
             int32_t *t = &g.tasks[(size_t)(*fillpos)[(size_t)h]++ * 8];
@@ -683,22 +722,41 @@ piks_status finish_geometry(const Setup &s, Geometry &g, std::string &err) {
   }
 
   // x = 1 / x = Nx planes (inlet/outlet targets and halo sources), symmetry planes
+  // (only the slabs at the box's sides hold them)
   g.plane_x1.assign((size_t)Ny * Nz, -1);
   g.plane_xN.assign((size_t)Ny * Nz, -1);
   for (int k = 1; k <= Nz; ++k)
     for (int j = 1; j <= Ny; ++j) {
-      g.plane_x1[(size_t)(k - 1) * Ny + (j - 1)] = std::max(-1, g.nodemap[g.ghost_index(1, j, k)]);
-      g.plane_xN[(size_t)(k - 1) * Ny + (j - 1)] = std::max(-1, g.nodemap[g.ghost_index(Nx, j, k)]);
+      if (g.wglob) g.plane_x1[(size_t)(k - 1) * Ny + (j - 1)] = std::max(-1, g.nodemap[g.ghost_index(1, j, k)]);
+      if (g.eglob) g.plane_xN[(size_t)(k - 1) * Ny + (j - 1)] = std::max(-1, g.nodemap[g.ghost_index(Nx, j, k)]);
     }
   g.sym_node.clear(); g.sym_flag.clear();
   for (int32_t n = 0; n < (int32_t)g.node_g.size(); ++n) {
     int64_t gi = g.node_g[n];
-    int j = (int)((gi / GX) % g.GY) - 1, k = (int)(gi / GXY) - 1;
+    int i = (int)(gi % GX) - 1, j = (int)((gi / GX) % g.GY) - 1, k = (int)(gi / GXY) - 1;
+    if (i < g.xl || i > g.xu) continue;  // solver.F90:1870-1917 run over the rank's own planes
     uint8_t fl8 = (j == 1 ? 1 : 0) | (j == Ny ? 2 : 0) | (k == 1 ? 4 : 0) | (k == Nz ? 8 : 0);
     if (fl8) { g.sym_node.push_back(n); g.sym_flag.push_back(fl8); }
   }
-  // chkConverge's plane x = 2 in its summation order (output.F90:90-136)
+  // x halos of a slab (solver.F90:535-560 move the two planes at each side)
+  for (int side = 0; side < 2; ++side) {
+    g.halo_send[side].clear();
+    g.halo_recv[side].clear();
+    if (side == 0 ? g.wglob : g.eglob) continue;
+    const int s0 = side == 0 ? g.xl : g.xu - 1, r0 = side == 0 ? g.xl - 2 : g.xu + 1;
+    for (int k = 1; k <= Nz; ++k)
+      for (int j = 1; j <= Ny; ++j)
+        for (int q = 0; q < 2; ++q) {
+          const int32_t ns = g.nodemap[g.ghost_index(s0 + q, j, k)], nr = g.nodemap[g.ghost_index(r0 + q, j, k)];
+          if (ns >= 0) g.halo_send[side].push_back(ns);
+          if (nr >= 0) g.halo_recv[side].push_back(nr);
+        }
+  }
+  // chkConverge's plane x = 2 in its summation order (output.F90:90-136); only the west-most
+  // slab holds it (output.F90:89)
   g.flux_list.clear();
+  for (int q = 0; q < 10; ++q) g.flux_groups[q] = 0;
+  if (!g.wglob) return PIKS_OK;
   auto fnode = [&](int j, int k) -> int32_t {
     int32_t n = g.nodemap[g.ghost_index(2, j, k)];
     return (n >= 0 && n < g.NF) ? n : -1;

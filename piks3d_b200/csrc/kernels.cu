@@ -921,6 +921,44 @@ void launch_capture(const DevState &s, int buf, cudaStream_t st) {
   k_capture<<<blocks_for(n, 256), 256, 0, st>>>(s, buf);
 }
 
+// Halo rows (solver.F90:535-560 for the planes of a slab boundary): element idx of a
+// [count][4][Nc8] buffer is row (nodes[q], octant set[k]) at velocity l; `pack` copies rows
+// into the buffer, otherwise the buffer into the rows. cx > 0 octants are 0, 3, 4, 7.
+template <typename T>
+__global__ void k_halo_rows(T *h, T *buf, const int32_t *nodes, int count, int cx_pos, int Nc8, bool pack) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (size_t)count * 4 * Nc8) return;
+  const int l = (int)(idx % Nc8);
+  const int k = (int)((idx / Nc8) % 4);
+  const int q = (int)(idx / ((size_t)Nc8 * 4));
+  const int o = cx_pos ? ((k == 0) ? 0 : (k == 1) ? 3 : (k == 2) ? 4 : 7) : ((k == 0) ? 1 : (k == 1) ? 2 : (k == 2) ? 5 : 6);
+  T *row = h + hidx(nodes[q], o, Nc8, l);
+  if (pack) buf[idx] = *row;
+  else *row = buf[idx];
+}
+
+template <typename T>
+void halo_rows(T *h, T *buf, const int32_t *nodes, int count, int cx_pos, int Nc8, bool pack, cudaStream_t st) {
+  if (count <= 0) return;
+  const size_t n = (size_t)count * 4 * Nc8;
+  k_halo_rows<T><<<blocks_for(n, 256), 256, 0, st>>>(h, buf, nodes, count, cx_pos, Nc8, pack);
+}
+
+void launch_halo(const DevState &s, bool fp32, int cap, cudaStream_t st) {
+  for (int side = 0; side < 2; ++side) {
+    // the west neighbour reads this slab's cx < 0 rows, the east one its cx > 0 rows; the
+    // west ghost planes receive cx > 0 rows, the east ones cx < 0 rows
+    const int send_pos = side == 1, recv_pos = side == 0;
+    if (fp32) {
+      halo_rows(s.h32, s.hsend32[side][cap], s.halo_send[side], s.nhalo_send[side], send_pos, s.Nc8, true, st);
+      halo_rows(s.h32, s.hrecv32[side], s.halo_recv[side], s.nhalo_recv[side], recv_pos, s.Nc8, false, st);
+    } else {
+      halo_rows(s.h, s.hsend[side][cap], s.halo_send[side], s.nhalo_send[side], send_pos, s.Nc8, true, st);
+      halo_rows(s.h, s.hrecv[side], s.halo_recv[side], s.nhalo_recv[side], recv_pos, s.Nc8, false, st);
+    }
+  }
+}
+
 void launch_inlet_outlet(const DevState &s, int buf, cudaStream_t st) {
   const size_t n = (size_t)s.Ny * s.Nz * 4 * s.Nc8;
   k_inlet_outlet<<<blocks_for(n, 256), 256, 0, st>>>(s, buf);

@@ -70,6 +70,14 @@ struct DevState {
   float *ghostW32[2], *ghostE32[2];
   const float *vtab32;          // [Nc8][kVtab] sweep constants rounded to FP32
   TileView tv;                  // tile-wavefront sweep schedule (when built)
+  // x halos of a slab (side 0 west, 1 east; solver.F90:535-560): the nodes whose rows are
+  // sent and the ghost-plane nodes received into, and per precision the send buffers (by
+  // iteration parity) and the receive buffer, [count][4][Nc8] of the four octants the
+  // receiver reads (west ghosts: cx > 0, east ghosts: cx < 0)
+  int nhalo_send[2], nhalo_recv[2];
+  const int32_t *halo_send[2], *halo_recv[2];
+  double *hsend[2][2], *hrecv[2];
+  float *hsend32[2][2], *hrecv32[2];
 };
 
 // Runs configure() once per (key, current device) for the whole process, under a mutex:
@@ -127,6 +135,9 @@ void launch_tile_sweep_columns(const DevState &s, bool fp32, int epoch, cudaStre
 void launch_tile_sweep_pipelined(const DevState &s, bool fp32, int epoch, cudaStream_t st);
 // Whether the column-march kernel's shared memory holds the schedule's largest job.
 bool column_sweep_fits(const TileView &tv, int Nc8, bool fp32);
+// Halo rows of iteration parity `cap`: pack the rows this slab sends into its send buffers,
+// unpack the received buffers into its ghost-plane nodes (FP32 or FP64 state).
+void launch_halo(const DevState &s, bool fp32, int cap, cudaStream_t st);
 void launch_widen(const float *src, double *dst, size_t n, cudaStream_t st);
 void launch_narrow(const double *src, float *dst, size_t n, cudaStream_t st);
 void launch_division_selftest(int64_t samples, uint64_t seed, unsigned long long *mismatches);

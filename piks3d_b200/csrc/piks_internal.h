@@ -88,7 +88,13 @@ struct Setup {
   int Nx = 0, Ny = 0, Nz = 0;              // box after fluidlayer and block_rep
   int Nx_base = 0, Ny_base = 0, Nz_base = 0;
   double ds = 0.0, mu = 0.0;
+  // x-only decomposition of the box into slabs, one per rank (mpiParams.F90:150-191 with
+  // dims = (nranks, 1, 1)); this rank owns the x planes [xl, xu] (the whole box for one rank)
+  int nranks = 1, rank = 0, xl = 1, xu = 0;
 };
+// Sets the slab of `rank` among `nranks` (the reference's partition of xmax - xmin planes);
+// fails when a rank would own fewer than two planes (its neighbours read two of them).
+piks_status set_slab(Setup &s, int nranks, int rank, std::string &err);
 
 // Compact device-side geometry produced by preprocess().
 struct Geometry {
@@ -111,7 +117,17 @@ struct Geometry {
   std::vector<int32_t> plane_x1, plane_xN;  // [Nz*Ny] node at x=1 / x=Nx or -1
   std::vector<int32_t> sym_node;   // nodes on the y/z boundary planes
   std::vector<uint8_t> sym_flag;   // bit0 y=1, bit1 y=Ny, bit2 z=1, bit3 z=Nz
-  std::vector<int32_t> flux_list;  // x=2 plane entries in chkConverge's summation order
+  std::vector<int32_t> flux_list;  // x=2 plane entries in chkConverge's summation order (west-most slab only)
+  // Slab of an x-decomposed box: owned planes [xl, xu]; a side that is not the box's side
+  // (wglob / eglob false) has two ghost planes owned by the neighbour rank, whose read
+  // voxels are nodes here too (after the fluid nodes, in [NF, NF + NB)).
+  int xl = 1, xu = 0;
+  bool wglob = true, eglob = true;
+  // x halos (side 0 west, 1 east): the nodes whose rows this rank sends (its two planes at
+  // that side) and the ghost-plane nodes it receives into; both ranks of a pair list the
+  // same voxels in the same order (z, then y, then x)
+  std::vector<int32_t> halo_send[2], halo_recv[2];
+  bool in_window(int i) const { return i >= (wglob ? 1 : xl - 2) && i <= (eglob ? Nx : xu + 2); }
   // Sweep tasks: one per (swept fluid node, octant), ordered by the hyperplane index
   // u+v+w of the octant's frame; tasks of one hyperplane are independent.
   // Record (8 x int32): node, flags (octant | fx<<3 | fy<<4 | fz<<5), then the value

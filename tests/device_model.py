@@ -88,6 +88,15 @@ class DeviceModel:
         self.iStep = 0
         self.progs = wall_programs()
         self.mass = 1.0
+        # x halos of a slab (side 0 west, 1 east): node lists, send buffers by parity, receive
+        sl = solver.slab()
+        self.slab = sl
+        self.nranks = sl["nranks"]
+        self.hsend_nodes = [g("halo_send_w"), g("halo_send_e")]
+        self.hrecv_nodes = [g("halo_recv_w"), g("halo_recv_e")]
+        self.hs = [[np.zeros((len(self.hsend_nodes[sd]), 4, self.Nc8)) for _ in range(2)] for sd in range(2)]
+        self.hr = [np.zeros((len(self.hrecv_nodes[sd]), 4, self.Nc8)) for sd in range(2)]
+        self.wglob, self.eglob = sl["xl"] == 1, sl["xu"] == self.Nx
 
     def _diffflux(self):
         d = 0.0
@@ -448,6 +457,16 @@ class DeviceModel:
                 for q, (oW, oE) in enumerate(((0, 1), (3, 2), (4, 5), (7, 6))):
                     self.gW[cap, r, q] = self.h[nW, oW] if nW >= 0 else 0.0
                     self.gE[cap, r, q] = self.h[nE, oE] if nE >= 0 else 0.0
+            if self.nranks > 1:
+                pos, neg = [0, 3, 4, 7], [1, 2, 5, 6]
+                for sd in range(2):
+                    # the west neighbour reads cx < 0 rows, the east one cx > 0 rows
+                    self.hs[sd][cap] = self.h[self.hsend_nodes[sd]][:, pos if sd == 1 else neg]
+                    nodes = self.hrecv_nodes[sd]
+                    if len(nodes):
+                        rows = self.h[nodes]
+                        rows[:, pos if sd == 0 else neg] = self.hr[sd]
+                        self.h[nodes] = rows
             self.walls(prev)
             wdp = self.w * self.p.pressDrop
             for r in range(self.Ny * self.Nz):
@@ -506,3 +525,32 @@ class DeviceModel:
         for n in range(self.nn):
             f[:, :, self.node_g[n]] = self.h[n]
         return f.reshape(-1)
+
+
+    def halo(self, side):
+        """(send, recv) arrays of the exchange before the next iteration on `side`, as
+        piks_halo_buffers names them: the inlet / outlet planes at the box's edge, the slab
+        halos elsewhere."""
+        par = self.iStep & 1
+        if (self.wglob if side == 0 else self.eglob):
+            return (self.gE[par], self.gW[par]) if side == 0 else (self.gW[par], self.gE[par])
+        return self.hs[side][par], self.hr[side]
+
+
+def exchange(models):
+    """Moves every rank's send arrays into its neighbours' receive arrays (periodic in x):
+    rank r's west receive gets rank r-1's east send, its east receive rank r+1's west send."""
+    n = len(models)
+    if n == 1:
+        return
+    sends = [(m.halo(0)[0].copy(), m.halo(1)[0].copy()) for m in models]
+    for r, m in enumerate(models):
+        m.halo(0)[1][...] = sends[(r - 1) % n][1]
+        m.halo(1)[1][...] = sends[(r + 1) % n][0]
+
+
+def iterate_slabs(models, n=1):
+    for _ in range(n):
+        exchange(models)
+        for m in models:
+            m.iterate(1)
