@@ -337,6 +337,7 @@ piks_status classify_device(const Setup &s, const std::vector<uint8_t> &box, Geo
   k_walls<<<blocks_of(d.NG, 256), 256, 0, st>>>(d, s.p.wallExtOrder, NF, dlabel, dnodemap, dwall_of, dcorner_of, w_node,
                                                   w_label, w_corner, w_e, w_nb, dbcorner);
   g.Nx = s.Nx; g.Ny = s.Ny; g.Nz = s.Nz; g.GX = d.GX; g.GY = d.GY; g.GZ = s.Nz + 4;
+  g.xl = 1; g.xu = s.Nx; g.wglob = g.eglob = true;  // one rank: the whole box
   g.NF = NF; g.NB = NB; g.nWall = nWall; g.nCorner = nCorner;
   g.label.resize((size_t)d.NG);
   g.nodemap.resize((size_t)d.NG);
