@@ -540,6 +540,73 @@ def run_batch_workload(args, world, rank, local):
     return 0
 
 
+def run_slab_workload(args, world, rank, local):
+    """One image over `world` GPUs as x slabs (strong scaling; the reference's MPI
+    decomposition with mpi_xdim = world): the 128^3 workload's FP64 and FP32 iterations,
+    each rank a SlabSolver, the halos moved by NCCL point-to-point calls on the context's
+    stream between iterations; value = the whole box's voxel-velocity updates/s (time =
+    max over ranks, CUDA events on the launching stream). On one GPU it also times the same
+    box cut into 2 and 4 slab contexts sharing the device (block-Jacobi in x: the slabs'
+    sweeps run concurrently, the halos one iteration behind)."""
+    import torch
+    import torch.distributed as dist
+    import piks3d_b200 as pk
+    from piks3d_b200.slab import LocalSlabs, SlabSolver
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    img = workload_image()
+    p = workload_params(pk)
+    out = {}
+    for prec in ("fp64", "fp32"):
+        ss = SlabSolver(p, img, device=local, precision=prec)
+        nf = ss.solver.info()["Nfluid"]
+        if world > 1:
+            t = torch.tensor([nf], dtype=torch.int64, device=device)
+            dist.all_reduce(t)
+            nf = int(t.item())
+        nv = 8 * ss.solver.info()["Nc8"]
+        ss.iterate(args.warmup)
+        torch.cuda.synchronize()
+        barrier(world, device)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(ss.stream)
+        ss.iterate(args.steps)
+        ev1.record(ss.stream)
+        torch.cuda.synchronize()
+        ms = reduce_max(ev0.elapsed_time(ev1), world, device)
+        m, k, e = ss.chk_converge()
+        sl = ss.solver.slab()
+        ss.close()
+        out[prec] = {"value": nf * nv * args.steps / (ms * 1e-3) / 1e9, "unit": UNIT,
+                     "ms_per_step": ms / args.steps, "mass_after": m, "slab_of_rank0": [sl["xl"], sl["xu"]]}
+    emulated = None
+    if world == 1:
+        emulated = {}
+        for n in (1, 2, 4):
+            row = {}
+            for prec in ("fp64", "fp32"):
+                ls = LocalSlabs(p, img, n, devices=(local,), precision=prec)
+                ls.iterate(args.warmup)
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                ls.iterate(args.steps)
+                for s_ in ls.solvers:
+                    s_.synchronize()
+                row[prec + "_ms_per_step"] = (time.perf_counter() - t0) * 1e3 / args.steps
+                ls.close()
+            emulated["%d_slabs" % n] = row
+    if rank != 0:
+        return 0
+    line = {"metric": METRIC, "workload": "slab", "value": out["fp64"]["value"], "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": out["fp64"]["ms_per_step"],
+            "higher_is_better": True, "scaling": "strong", "dtype": "f64", "data": "synthetic",
+            "config": {**config_dict(), "parallelism": "x slabs, one per GPU (halo exchange by NCCL send / recv)"},
+            "fp32": out["fp32"], "fp64": out["fp64"],
+            "emulated_ranks_one_gpu": emulated}
+    print(json.dumps(line))
+    return 0
+
+
 def run_serve_workload(args, world, rank, local):
     """The serving workload: a seeded Poisson request stream through the server."""
     import torch
@@ -581,9 +648,10 @@ def main():
     ap.add_argument("--no-solve", action="store_true", help="skip the full solves (solve / e2e blocks)")
     ap.add_argument("--batch-images", type=int, default=12,
                     help="images of the reduced batching workload in the default line (0: skip)")
-    ap.add_argument("--workload", default="precision", choices=["precision", "batch", "serve", "large"],
+    ap.add_argument("--workload", default="precision", choices=["precision", "batch", "serve", "large", "slab"],
                     help="precision: the 128^3 pack (default); batch: many images; serve: request stream; "
-                         "large: the 256^3 Gaussian random field (add --solve-large for the full solves)")
+                         "large: the 256^3 Gaussian random field (add --solve-large for the full solves); "
+                         "slab: the 128^3 pack decomposed over the GPUs as x slabs (strong scaling)")
     ap.add_argument("--solve-large", action="store_true")
     ap.add_argument("--images", type=int, default=64)
     ap.add_argument("--seed", type=int, default=2024)
@@ -613,6 +681,8 @@ def main():
             rc = run_batch_workload(args, world, rank, local)
         elif args.workload == "serve":
             rc = run_serve_workload(args, world, rank, local)
+        elif args.workload == "slab":
+            rc = run_slab_workload(args, world, rank, local)
         else:
             rc = run_ours(args, world, rank, local)
     finally:
