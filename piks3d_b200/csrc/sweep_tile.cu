@@ -44,9 +44,11 @@ __host__ __device__ inline size_t tile_smem_bytes(int slots, int ntask, int step
          (size_t)steps_stride * 2;
 }
 
-// One job (tile, octant) for the velocity chunk `chunk`, by the whole CTA.
+// One job (tile, octant) for the velocity chunks chunk0 .. chunk0 + nch - 1, by the whole
+// CTA: the job's row codes, task records, steps and moments are staged once, then each
+// chunk's rows are staged, swept and written back in turn.
 template <typename T, int V>
-__device__ __forceinline__ void tile_job(const DevState &a, int job, int chunk, int slots_cap, int tasks_cap,
+__device__ __forceinline__ void tile_job(const DevState &a, int job, int chunk0, int nch, int slots_cap, int tasks_cap,
                                          unsigned char *smem_raw) {
   constexpr int LPT = V / 2;                        // lanes per task
   constexpr int THREADS = LPT * groups_of<T>();
@@ -58,7 +60,6 @@ __device__ __forceinline__ void tile_job(const DevState &a, int job, int chunk, 
 
   const TileView &tv = a.tv;
   const int Nc8 = a.Nc8;
-  const int l0 = chunk * V;
   const int64_t rb = tv.row_begin[job];
   const int nrows = tv.row_count[job];
   const int64_t tb = tv.task_begin[job];
@@ -88,55 +89,72 @@ __device__ __forceinline__ void tile_job(const DevState &a, int job, int chunk, 
     cp_async16(Mom + i, reinterpret_cast<const double2 *>(a.mom) + 2 * (size_t)m + (i & 1));
   }
   asm volatile("griddepcontrol.wait;" ::: "memory");
-  for (int i = threadIdx.x; i < nrows * PIECES; i += THREADS) {
-    const int r = i / PIECES, pc = i - r * PIECES;
-    const int code = Codes[r];
-    const T *src = ((code & kFwBit) ? fw : h) + (size_t)(code & ~kFwBit) * (size_t)Nc8 + l0 + pc * EPP;
-    cp_async16(S + (size_t)(1 + r) * V + pc * EPP, src);
-  }
   if (threadIdx.x < PIECES) *reinterpret_cast<int4 *>(S + threadIdx.x * EPP) = make_int4(0, 0, 0, 0);
-
-  // per-lane constants of its two velocities
   const int grp = threadIdx.x / LPT, sub = threadIdx.x % LPT;
-  const int lp = l0 + 2 * sub;
   const int o = Codes[0] & 7;                       // own row code = node * 8 + octant
   const bool nx_ = neg_x(o), ny_ = neg_y(o), nz_ = neg_z(o);
-  T K[13][2];
-  load_lane_consts<T>(a, lp, K);
-
-  cp_async_wait_all();
-  __syncthreads();
-
-  // 2. the part of every update that does not depend on this sweep's values,
-  //    mu * (fEq - f_old / 2) (solver.F90:205-214), replaces f_old in the task's own slot
-  base_pass<T, V, GROUPS>(a, Mom, S, 1, ntask, grp, sub, K, nx_, ny_, nz_);
-  __syncthreads();
-
-  // 3. local hyperplanes: the upwind terms in the reference's order, then the division
-  for (int s = 0; s < nsteps; ++s) {
-    const int t0 = Steps[s], t1 = Steps[s + 1];
-    if (t0 == t1) continue;
-    for (int t = t0 + grp; t < t1; t += GROUPS) update_task<T, V>(a, S, Trec[t], 1 + t, sub, lp, K);
-    __syncthreads();
-  }
-
-  // 4. own rows -> global
   T *hw = const_cast<T *>(h);
-  for (int i = threadIdx.x; i < ntask * PIECES; i += THREADS) {
-    const int r = i / PIECES, pc = i - r * PIECES;
-    const int code = Codes[r];
-    *reinterpret_cast<int4 *>(hw + (size_t)code * Nc8 + l0 + pc * EPP) =
-        *reinterpret_cast<const int4 *>(S + (size_t)(1 + r) * V + pc * EPP);
+
+  for (int c = 0; c < nch; ++c) {
+    const int l0 = (chunk0 + c) * V;
+    if (c > 0) __syncthreads();                     // the previous chunk's write-back read S
+    for (int i = threadIdx.x; i < nrows * PIECES; i += THREADS) {
+      const int r = i / PIECES, pc = i - r * PIECES;
+      const int code = Codes[r];
+      const T *src = ((code & kFwBit) ? fw : h) + (size_t)(code & ~kFwBit) * (size_t)Nc8 + l0 + pc * EPP;
+      cp_async16(S + (size_t)(1 + r) * V + pc * EPP, src);
+    }
+
+    // per-lane constants of its two velocities
+    const int lp = l0 + 2 * sub;
+    T K[13][2];
+    load_lane_consts<T>(a, lp, K);
+
+    cp_async_wait_all();
+    __syncthreads();
+
+    // 2. the part of every update that does not depend on this sweep's values,
+    //    mu * (fEq - f_old / 2) (solver.F90:205-214), replaces f_old in the task's own slot
+    base_pass<T, V, GROUPS>(a, Mom, S, 1, ntask, grp, sub, K, nx_, ny_, nz_);
+    __syncthreads();
+
+    // 3. local hyperplanes: the upwind terms in the reference's order, then the division
+    for (int s = 0; s < nsteps; ++s) {
+      const int t0 = Steps[s], t1 = Steps[s + 1];
+      if (t0 == t1) continue;
+      for (int t = t0 + grp; t < t1; t += GROUPS) update_task<T, V>(a, S, Trec[t], 1 + t, sub, lp, K);
+      __syncthreads();
+    }
+
+    // 4. own rows -> global
+    for (int i = threadIdx.x; i < ntask * PIECES; i += THREADS) {
+      const int r = i / PIECES, pc = i - r * PIECES;
+      const int code = Codes[r];
+      *reinterpret_cast<int4 *>(hw + (size_t)code * Nc8 + l0 + pc * EPP) =
+          *reinterpret_cast<const int4 *>(S + (size_t)(1 + r) * V + pc * EPP);
+    }
   }
+}
+
+// Velocity chunks one CTA of a diagonal launch sweeps: the largest power of two that divides
+// the chunk count and is at most kChunksPerCta<T>. Measured on B200 (128^3 pack, 512
+// velocities, sweep per iteration): FP64 one / two / four chunks of 16 per CTA 6.03 / 5.73 /
+// 5.90 ms; FP32 one / two chunks of 32: 2.79 / 2.94 ms.
+template <typename T> constexpr int kChunksPerCta = sizeof(T) == 8 ? 2 : 1;
+template <typename T>
+inline int chunks_per_cta(int nchunk) {
+  int c = kChunksPerCta<T>;
+  while (c > 1 && nchunk % c) c >>= 1;
+  return c;
 }
 
 template <typename T, int V>
 __global__ void __launch_bounds__(threads_of<T, V>())
-k_tile_sweep(const DevState a, int job0, int slots_cap, int tasks_cap) {
+k_tile_sweep(const DevState a, int job0, int slots_cap, int tasks_cap, int cpb) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int nchunk = a.Nc8 / V;
-  tile_job<T, V>(a, a.tv.job_list[job0 + (int)(blockIdx.x / nchunk)], (int)(blockIdx.x % nchunk), slots_cap,
-                 tasks_cap, smem_raw);
+  const int per_job = a.Nc8 / V / cpb;              // CTAs per job
+  tile_job<T, V>(a, a.tv.job_list[job0 + (int)(blockIdx.x / per_job)], (int)(blockIdx.x % per_job) * cpb, cpb,
+                 slots_cap, tasks_cap, smem_raw);
 }
 
 // Lets `fn` use all the shared memory a block may opt into, less its static shared memory.
@@ -198,7 +216,7 @@ k_tile_sweep_dataflow(const DevState a, int epoch, int slots_cap, int tasks_cap)
       if (u >= 0 && !wait_flag(tv.flags + (size_t)u * nchunk + chunk, epoch, tv.err)) skip_s = 1;
     }
     __syncthreads();
-    if (!skip_s) tile_job<T, V>(a, job, chunk, slots_cap, tasks_cap, smem_raw);
+    if (!skip_s) tile_job<T, V>(a, job, chunk, 1, slots_cap, tasks_cap, smem_raw);
     __syncthreads();
     if (threadIdx.x == 0) {
       __threadfence();
@@ -231,7 +249,7 @@ k_tile_sweep_batch(const DevState *states, const int2 *items, int nitems, int sl
       if (u >= 0 && !wait_flag(a.tv.flags + (size_t)u * nchunk + chunk, 1, err)) skip_s = 1;
     }
     __syncthreads();
-    if (!skip_s) tile_job<T, V>(a, job, chunk, slots_cap, tasks_cap, smem_raw);
+    if (!skip_s) tile_job<T, V>(a, job, chunk, 1, slots_cap, tasks_cap, smem_raw);
     __syncthreads();
     if (threadIdx.x == 0) {
       __threadfence();
@@ -271,8 +289,9 @@ template <typename T, int V>
 void launch_one(const DevState &s, int job0, int njobs, int slots, int tasks, bool pdl, cudaStream_t st) {
   once_per_device(reinterpret_cast<const void *>(k_tile_sweep<T, V>),
                   [](int dev) { allow_dynamic_smem(reinterpret_cast<const void *>(k_tile_sweep<T, V>), dev); });
+  const int cpb = chunks_per_cta<T>(s.Nc8 / V);
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)((size_t)njobs * (s.Nc8 / V)));
+  cfg.gridDim = dim3((unsigned)((size_t)njobs * (s.Nc8 / V / cpb)));
   cfg.blockDim = dim3(threads_of<T, V>());
   cfg.dynamicSmemBytes = tile_smem_bytes(slots, tasks, s.tv.steps_stride, V * (int)sizeof(T));
   cfg.stream = st;
@@ -281,7 +300,7 @@ void launch_one(const DevState &s, int job0, int njobs, int slots, int tasks, bo
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
   cfg.numAttrs = pdl ? 1 : 0;
-  cudaLaunchKernelEx(&cfg, k_tile_sweep<T, V>, s, job0, slots, tasks);
+  cudaLaunchKernelEx(&cfg, k_tile_sweep<T, V>, s, job0, slots, tasks, cpb);
 }
 
 }  // namespace
