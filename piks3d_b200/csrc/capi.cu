@@ -194,10 +194,10 @@ void drain_timing(piks_ctx *c) {
   c->ev_next = 0;
 }
 
-// The dataflow sweep's error flag: set when a dependency wait gave up (the values of that
-// sweep are then not the solver's).
+// The tile sweeps' error flag: set when a dependency wait or a staging wait gave up (the
+// values of that sweep are then not the solver's).
 piks_status check_sweep_error(piks_ctx *c) {
-  if (!c->use_tiles || !c->ds.tv.err || !c->dataflow_used) return PIKS_OK;
+  if (!c->use_tiles || !c->ds.tv.err) return PIKS_OK;
   int e = 0;
   piks_status st = cuda_check(cudaMemcpyAsync(&e, c->ds.tv.err, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "err D2H");
   if (!st) st = cuda_check(cudaStreamSynchronize(c->stream), "err sync");
@@ -238,11 +238,9 @@ void enqueue_sweep(piks_ctx *c, cudaStream_t st, int n) {
   {
     Timed t(c, KT_SWEEP);
     if (c->use_tiles && c->tiles.split) {
-      c->dataflow_used = true;
       if (c->tiles.columns) launch_tile_sweep_columns(s, f32, 1, st);
       else launch_tile_sweep_pipelined(s, f32, 1, st);
     } else if (c->use_tiles && c->schedule == PIKS_SCHED_TILE_DATAFLOW) {
-      c->dataflow_used = true;
       launch_tile_sweep_dataflow(s, f32, n, c->tiles.max_rows, c->tiles.max_tasks, st);
     } else if (c->use_tiles) {
       const auto &L = c->tiles.launches;

@@ -53,7 +53,6 @@ struct piks_ctx {
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   int graph_key = -1, graph_warm = 0;
   bool graph_failed = false;
-  bool dataflow_used = false;       // a dataflow sweep ran (its error flag needs reading)
   cudaStream_t cap_stream = nullptr;
   std::vector<cudaEvent_t> ev_pool;
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pending;

@@ -38,7 +38,6 @@ namespace {
 
 using namespace sweep;
 
-constexpr unsigned long long kWaitNs = 2000000000ull;
 
 // 256 zero bytes: the source of every region's zero row (slot 0).
 __device__ __align__(128) unsigned char g_zero_row[256] = {0};
@@ -59,30 +58,6 @@ struct Desc {
   int job, chunk, base, ntask, ncin, ncout, fresh, pad;
 };
 
-__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ unsigned long long gtimer() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_arrive(unsigned bar, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(unsigned bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
-__device__ __forceinline__ bool mbar_try(unsigned bar, unsigned parity) {
-  unsigned ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(ok)
-      : "r"(bar), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
 // Waits for the phase of `parity` to complete; gives up (false, *abort and *err set) after
 // kWaitNs or as soon as another warp of the CTA has aborted.
 __device__ bool mbar_wait(unsigned bar, unsigned parity, volatile int *abort, int *err) {
@@ -99,11 +74,6 @@ __device__ bool mbar_wait(unsigned bar, unsigned parity, volatile int *abort, in
       }
     }
   }
-}
-__device__ __forceinline__ void bulk_g2s(unsigned dst, const void *src, unsigned bytes, unsigned bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-               "l"(src), "r"(bytes), "r"(bar)
-               : "memory");
 }
 // 16 bytes global -> shared through L2 (LSU path); completion is tracked per thread.
 __device__ __forceinline__ void cp16(unsigned dst, const void *src) {

@@ -47,9 +47,12 @@ __host__ __device__ inline size_t tile_smem_bytes(int slots, int ntask, int step
 // One job (tile, octant) for the velocity chunks chunk0 .. chunk0 + nch - 1, by the whole
 // CTA: the job's row codes, task records, steps and moments are staged once, then each
 // chunk's rows are staged, swept and written back in turn.
-template <typename T, int V>
-__device__ __forceinline__ void tile_job(const DevState &a, int job, int chunk0, int nch, int slots_cap, int tasks_cap,
-                                         unsigned char *smem_raw) {
+// With `meta_bar` (an mbarrier in shared memory, initialised, phase 0) the three contiguous
+// metadata arrays arrive by bulk asynchronous copies issued by one thread; without it (the
+// persistent kernels, which run many jobs per CTA) every thread copies 16-byte pieces.
+template <typename T, int V, int NCH = 1>
+__device__ __forceinline__ void tile_job(const DevState &a, int job, int chunk0, int slots_cap, int tasks_cap,
+                                         unsigned char *smem_raw, unsigned long long *meta_bar = nullptr) {
   constexpr int LPT = V / 2;                        // lanes per task
   constexpr int THREADS = LPT * groups_of<T>();
   constexpr int GROUPS = groups_of<T>();            // tasks in flight per pass
@@ -74,14 +77,38 @@ __device__ __forceinline__ void tile_job(const DevState &a, int job, int chunk0,
   // the next tile diagonal (launched as a programmatic dependent) may start its first round
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 
-  // 1a. row codes, task records and step offsets -> shared memory
-  for (int i = threadIdx.x; i < (nrows + 3) / 4; i += THREADS)
-    cp_async16(Codes + 4 * i, tv.rows + rb + 4 * i);
-  for (int i = threadIdx.x; i < ntask; i += THREADS) cp_async16(Trec + i, tv.tasks + tb + i);
-  for (int i = threadIdx.x; i < tv.steps_stride / 8; i += THREADS)
-    cp_async16(Steps + 8 * i, tv.steps + (size_t)job * tv.steps_stride + 8 * i);
-  cp_async_wait_all();
-  __syncthreads();
+  // 1a. row codes, task records and step offsets -> shared memory (row lists start at a
+  //     multiple of four entries, records are 16 bytes, the step stride a multiple of eight)
+  if (meta_bar) {
+    const unsigned bar = smem_u32(meta_bar);
+    if (threadIdx.x == 0) {
+      const unsigned b_codes = (unsigned)((nrows + 3) / 4) * 16u, b_trec = (unsigned)ntask * 16u,
+                     b_steps = (unsigned)tv.steps_stride * 2u;
+      mbar_expect_arrive(bar, b_codes + b_trec + b_steps);
+      bulk_g2s(smem_u32(Codes), tv.rows + rb, b_codes, bar);
+      bulk_g2s(smem_u32(Trec), tv.tasks + tb, b_trec, bar);
+      bulk_g2s(smem_u32(Steps), tv.steps + (size_t)job * tv.steps_stride, b_steps, bar);
+    }
+    // bounded wait: a phase that never completes marks the sweep failed and skips the job
+    bool ok = mbar_try(bar, 0);
+    if (!ok) {
+      const unsigned long long t0 = gtimer();
+      while (!(ok = mbar_try(bar, 0)) && gtimer() - t0 < kWaitNs) {
+      }
+    }
+    if (__syncthreads_or(!ok)) {
+      if (threadIdx.x == 0) atomicExch(tv.err, 1);
+      return;
+    }
+  } else {
+    for (int i = threadIdx.x; i < (nrows + 3) / 4; i += THREADS)
+      cp_async16(Codes + 4 * i, tv.rows + rb + 4 * i);
+    for (int i = threadIdx.x; i < ntask; i += THREADS) cp_async16(Trec + i, tv.tasks + tb + i);
+    for (int i = threadIdx.x; i < tv.steps_stride / 8; i += THREADS)
+      cp_async16(Steps + 8 * i, tv.steps + (size_t)job * tv.steps_stride + 8 * i);
+    cp_async_wait_all();
+    __syncthreads();
+  }
   // 1b. the moments of the tasks' nodes (FP64 Rho, Ux | Uy, Uz; written by the previous
   //     iteration), then, once the previous diagonal's rows are visible, the rows
   for (int i = threadIdx.x; i < 2 * ntask; i += THREADS) {
@@ -95,7 +122,8 @@ __device__ __forceinline__ void tile_job(const DevState &a, int job, int chunk0,
   const bool nx_ = neg_x(o), ny_ = neg_y(o), nz_ = neg_z(o);
   T *hw = const_cast<T *>(h);
 
-  for (int c = 0; c < nch; ++c) {
+#pragma unroll 1
+  for (int c = 0; c < NCH; ++c) {
     const int l0 = (chunk0 + c) * V;
     if (c > 0) __syncthreads();                     // the previous chunk's write-back read S
     for (int i = threadIdx.x; i < nrows * PIECES; i += THREADS) {
@@ -136,25 +164,30 @@ __device__ __forceinline__ void tile_job(const DevState &a, int job, int chunk0,
   }
 }
 
-// Velocity chunks one CTA of a diagonal launch sweeps: the largest power of two that divides
-// the chunk count and is at most kChunksPerCta<T>. Measured on B200 (128^3 pack, 512
-// velocities, sweep per iteration): FP64 one / two / four chunks of 16 per CTA 6.03 / 5.73 /
-// 5.90 ms; FP32 one / two chunks of 32: 2.79 / 2.94 ms.
+// Velocity chunks one CTA of a diagonal launch sweeps (when they divide the chunk count;
+// otherwise one). Measured on B200 (128^3 pack, 512 velocities, sweep per iteration): FP64
+// one / two / four chunks of 16 per CTA 6.03 / 5.73 / 5.90 ms; FP32 one / two chunks of 32:
+// 2.79 / 2.94 ms.
 template <typename T> constexpr int kChunksPerCta = sizeof(T) == 8 ? 2 : 1;
-template <typename T>
-inline int chunks_per_cta(int nchunk) {
-  int c = kChunksPerCta<T>;
-  while (c > 1 && nchunk % c) c >>= 1;
-  return c;
-}
+// Whether a diagonal launch's CTAs take their job metadata by bulk copies: measured on the
+// same workload, FP64 5.96 ms with them against 6.03 without, FP32 2.85 against 2.79.
+template <typename T> constexpr bool kBulkMeta = sizeof(T) == 8;
 
-template <typename T, int V>
+template <typename T, int V, int CPB>
 __global__ void __launch_bounds__(threads_of<T, V>())
-k_tile_sweep(const DevState a, int job0, int slots_cap, int tasks_cap, int cpb) {
+k_tile_sweep(const DevState a, int job0, int slots_cap, int tasks_cap) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int per_job = a.Nc8 / V / cpb;              // CTAs per job
-  tile_job<T, V>(a, a.tv.job_list[job0 + (int)(blockIdx.x / per_job)], (int)(blockIdx.x % per_job) * cpb, cpb,
-                 slots_cap, tasks_cap, smem_raw);
+  __shared__ __align__(8) unsigned long long meta_bar;
+  if (kBulkMeta<T>) {
+    if (threadIdx.x == 0) {
+      mbar_init(smem_u32(&meta_bar), 1);
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+  }
+  const int per_job = a.Nc8 / V / CPB;              // CTAs per job
+  tile_job<T, V, CPB>(a, a.tv.job_list[job0 + (int)(blockIdx.x / per_job)], (int)(blockIdx.x % per_job) * CPB,
+                      slots_cap, tasks_cap, smem_raw, kBulkMeta<T> ? &meta_bar : nullptr);
 }
 
 // Lets `fn` use all the shared memory a block may opt into, less its static shared memory.
@@ -216,7 +249,7 @@ k_tile_sweep_dataflow(const DevState a, int epoch, int slots_cap, int tasks_cap)
       if (u >= 0 && !wait_flag(tv.flags + (size_t)u * nchunk + chunk, epoch, tv.err)) skip_s = 1;
     }
     __syncthreads();
-    if (!skip_s) tile_job<T, V>(a, job, chunk, 1, slots_cap, tasks_cap, smem_raw);
+    if (!skip_s) tile_job<T, V>(a, job, chunk, slots_cap, tasks_cap, smem_raw);
     __syncthreads();
     if (threadIdx.x == 0) {
       __threadfence();
@@ -249,7 +282,7 @@ k_tile_sweep_batch(const DevState *states, const int2 *items, int nitems, int sl
       if (u >= 0 && !wait_flag(a.tv.flags + (size_t)u * nchunk + chunk, 1, err)) skip_s = 1;
     }
     __syncthreads();
-    if (!skip_s) tile_job<T, V>(a, job, chunk, 1, slots_cap, tasks_cap, smem_raw);
+    if (!skip_s) tile_job<T, V>(a, job, chunk, slots_cap, tasks_cap, smem_raw);
     __syncthreads();
     if (threadIdx.x == 0) {
       __threadfence();
@@ -285,13 +318,12 @@ void launch_dataflow(const DevState &s, int epoch, int slots, int tasks, cudaStr
   k_tile_sweep_dataflow<T, V><<<(unsigned)grid, threads_of<T, V>(), smem, st>>>(s, epoch, slots, tasks);
 }
 
-template <typename T, int V>
-void launch_one(const DevState &s, int job0, int njobs, int slots, int tasks, bool pdl, cudaStream_t st) {
-  once_per_device(reinterpret_cast<const void *>(k_tile_sweep<T, V>),
-                  [](int dev) { allow_dynamic_smem(reinterpret_cast<const void *>(k_tile_sweep<T, V>), dev); });
-  const int cpb = chunks_per_cta<T>(s.Nc8 / V);
+template <typename T, int V, int CPB>
+void launch_cpb(const DevState &s, int job0, int njobs, int slots, int tasks, bool pdl, cudaStream_t st) {
+  once_per_device(reinterpret_cast<const void *>(k_tile_sweep<T, V, CPB>),
+                  [](int dev) { allow_dynamic_smem(reinterpret_cast<const void *>(k_tile_sweep<T, V, CPB>), dev); });
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)((size_t)njobs * (s.Nc8 / V / cpb)));
+  cfg.gridDim = dim3((unsigned)((size_t)njobs * (s.Nc8 / V / CPB)));
   cfg.blockDim = dim3(threads_of<T, V>());
   cfg.dynamicSmemBytes = tile_smem_bytes(slots, tasks, s.tv.steps_stride, V * (int)sizeof(T));
   cfg.stream = st;
@@ -300,7 +332,14 @@ void launch_one(const DevState &s, int job0, int njobs, int slots, int tasks, bo
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
   cfg.numAttrs = pdl ? 1 : 0;
-  cudaLaunchKernelEx(&cfg, k_tile_sweep<T, V>, s, job0, slots, tasks, cpb);
+  cudaLaunchKernelEx(&cfg, k_tile_sweep<T, V, CPB>, s, job0, slots, tasks);
+}
+
+template <typename T, int V>
+void launch_one(const DevState &s, int job0, int njobs, int slots, int tasks, bool pdl, cudaStream_t st) {
+  constexpr int C = kChunksPerCta<T>;
+  if (C > 1 && (s.Nc8 / V) % C == 0) launch_cpb<T, V, C>(s, job0, njobs, slots, tasks, pdl, st);
+  else launch_cpb<T, V, 1>(s, job0, njobs, slots, tasks, pdl, st);
 }
 
 }  // namespace
