@@ -25,11 +25,14 @@ namespace {
 
 using namespace sweep;
 
-// Task groups per CTA (tasks of one local hyperplane in flight): 16 for FP64, 6 for FP32,
-// whose groups have twice the lanes (V = 32 velocities); both measured fastest on B200
-// (FP32 sweep of a 128^3 pack per iteration: 4 groups 2.76 ms, 6: 2.69, 8: 2.74, 12: 3.39).
-template <typename T> constexpr int groups_of() { return sizeof(T) == 8 ? 16 : 6; }
-template <typename T, int V> constexpr int threads_of() { return V / 2 * groups_of<T>(); }
+// Task groups per CTA (tasks of one local hyperplane in flight): FP64 CTAs of 64 threads
+// (8 groups of 8 lanes for 16 velocities), FP32 6 groups of 16 lanes (32 velocities).
+// Measured on B200 (128^3 pack, 512 velocities, sweep per iteration): FP64 with 8x4x4 tiles
+// and two chunks per CTA 4 / 6 / 8 / 12 / 16 groups 6.15 / 5.84 / 5.42 / 5.41 / 5.77 ms
+// (4x4x4 tiles: 5.32 / 5.63 / 5.46 / 6.19 / 7.01); FP32 4 groups 2.76 ms, 6: 2.69, 8: 2.74,
+// 12: 3.39.
+template <typename T, int V> constexpr int groups_of() { return sizeof(T) == 8 ? 64 / (V / 2) : 6; }
+template <typename T, int V> constexpr int threads_of() { return V / 2 * groups_of<T, V>(); }
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
@@ -54,8 +57,8 @@ template <typename T, int V, int NCH = 1>
 __device__ __forceinline__ void tile_job(const DevState &a, int job, int chunk0, int slots_cap, int tasks_cap,
                                          unsigned char *smem_raw, unsigned long long *meta_bar = nullptr) {
   constexpr int LPT = V / 2;                        // lanes per task
-  constexpr int THREADS = LPT * groups_of<T>();
-  constexpr int GROUPS = groups_of<T>();            // tasks in flight per pass
+  constexpr int THREADS = LPT * groups_of<T, V>();
+  constexpr int GROUPS = groups_of<T, V>();            // tasks in flight per pass
   constexpr int EPP = 16 / (int)sizeof(T);          // elements per 16-byte piece
   constexpr int PIECES = V / EPP;                   // pieces per row
   using T2 = typename Pair<T>::type;
