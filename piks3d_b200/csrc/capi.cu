@@ -319,7 +319,7 @@ int tile_form(int schedule) {
 
 // Tile jobs for a tile shape in the given form (the split forms fall back to the slot form
 // when the producer / consumer kernel cannot hold the largest job in shared memory).
-bool build_tiles_for(const piks_ctx *c, const int *dims, int form, TileJobs &tj) {
+bool build_tiles_for(const piks_ctx *c, const int *dims, int form, TileJobs &tj, int prec) {
   tj = TileJobs{};
   if (dims[0] <= 0) return false;
   if (form != TILE_FORM_SLOTS) {
@@ -330,11 +330,12 @@ bool build_tiles_for(const piks_ctx *c, const int *dims, int form, TileJobs &tj)
   }
   const bool ok = build_tile_jobs(c->geo, dims[0], dims[1], dims[2], tile_slots(c, dims), tj);
   if (!ok) tj = TileJobs{};
+  else plan_for_precision(tj, prec);
   return ok;
 }
 
 bool build_tiles(piks_ctx *c) {
-  c->use_tiles = build_tiles_for(c, c->tile_dims, tile_form(c->schedule), c->tiles);
+  c->use_tiles = build_tiles_for(c, c->tile_dims, tile_form(c->schedule), c->tiles, c->prec);
   return c->use_tiles;
 }
 
@@ -384,6 +385,7 @@ piks_status upload_tiles(piks_ctx *c) {
   tv.err = pw + 1;
   tv.nsteps = tj.nsteps;
   tv.steps_stride = tj.steps_stride;
+  tv.paired = tj.paired ? 1 : 0;
   if (tj.split) {
     const TileView sz = column_sizes(tj);
     tv.max_tasks = sz.max_tasks; tv.max_nrows = sz.max_nrows; tv.max_carry = sz.max_carry;
@@ -638,7 +640,7 @@ piks_status piks_setup_physical_grid(piks_ctx *c, const uint8_t *raw, int64_t nb
     (void)slots;
     const int form = tile_form(c->schedule);
     c->tiles_next_ready = std::async(std::launch::async, [c, form] {
-      return build_tiles_for(c, c->tiles_next_dims, form, c->tiles_next);
+      return build_tiles_for(c, c->tiles_next_dims, form, c->tiles_next, PIKS_PREC_FP64);
     });
   }
   c->mass = 1.0;  // flow.F90:97
@@ -956,7 +958,7 @@ static piks_status retile_for_precision(piks_ctx *c) {
     ok = c->tiles_next_ready.get();
     if (ok) tj = std::move(c->tiles_next);
   } else {
-    ok = build_tiles_for(c, d, tile_form(c->schedule), tj);
+    ok = build_tiles_for(c, d, tile_form(c->schedule), tj, c->prec);
   }
   drop_tiles_next(c);
   if (!ok) return PIKS_OK;  // keep the current schedule
@@ -1000,6 +1002,12 @@ piks_status piks_set_precision(piks_ctx *c, int32_t precision) {
   free_state(c, c->prec);
   c->prec = precision;
   if (c->use_tiles && !c->tiles_explicit && !c->tiles_tuned && (st = retile_for_precision(c))) return st;
+  if (c->use_tiles && !c->tiles.split && c->tiles.plan_prec != precision) {
+    // the schedule stayed: its launch plan becomes the new precision's
+    plan_for_precision(c->tiles, precision);
+    if ((st = upload_tiles(c))) return st;
+    if ((st = cuda_check(cudaStreamSynchronize(c->stream), "replan"))) return st;
+  }
   c->version += 1;
   return PIKS_OK;
 }

@@ -20,6 +20,7 @@ struct TileView {
   int *err;                     // set when a dependency wait gave up
   int njobs;
   int nsteps, steps_stride;
+  int paired;                   // diagonal launches sweep job pairs (TileJobs::paired)
   // column form (TileJobs::columns): per-job headers, carry lists, columns in dependency order
   const int32_t *hdr;           // [njobs][8]
   const int32_t *carry;

@@ -172,6 +172,9 @@ struct TileJobs {
   std::vector<int32_t> launches;     // per launch: first job_list entry, job count, slots, tasks
   std::vector<int32_t> launch_diag_end;  // launch offset after each diagonal
   std::vector<int32_t> up;           // [njobs][4]: jobs of the upwind x, y, z neighbour tiles (same octant) or -1
+  bool paired = false;               // launches sweep job pairs (job_list holds the pairs adjacently)
+  int slot_cap = 0;                  // the shared-memory slots one job may use (build_tile_jobs' max_slots)
+  int plan_prec = -1;                // precision the launch plan was made for (plan_for_precision)
   int32_t max_rows = 0;              // largest slot count of a job
   int32_t max_tasks = 0;             // largest task count of a job
   // Column form (built with columns = true; only the column-march sweep reads it). A column
@@ -211,7 +214,14 @@ bool build_tile_jobs(const Geometry &g, int TX, int TY, int TZ, int max_slots, T
                      int form = TILE_FORM_SLOTS);
 // (Re)builds the launch plan with at most max_classes size classes per diagonal; a class
 // holds the jobs whose slot count is above `ratio` times its largest.
-void plan_tile_launches(TileJobs &tj, int max_classes, double ratio);
+// Launch plan of the diagonals: the jobs of a diagonal by slot count, in up to max_classes
+// size classes (one launch each); with `pairs` (one class) the jobs are interleaved largest
+// with smallest and each launch record holds the largest slot and task sums of a pair (one
+// CTA sweeps a pair, each job in its own part of the CTA's shared memory).
+void plan_tile_launches(TileJobs &tj, int max_classes, double ratio, bool pairs);
+// The launch plan of a precision: job pairs for the FP64 sweep (when a pair fits the shared
+// memory one job may use), single jobs for FP32 (prec: PIKS_PREC_FP64 or PIKS_PREC_FP32).
+void plan_for_precision(TileJobs &tj, int prec);
 
 piks_status make_setup(const piks_params &p, Setup &s, std::string &err);
 piks_status make_velocity(const piks_params &p, Velocity &v, std::string &err);

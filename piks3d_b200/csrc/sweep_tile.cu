@@ -47,15 +47,41 @@ __host__ __device__ inline size_t tile_smem_bytes(int slots, int ntask, int step
          (size_t)steps_stride * 2;
 }
 
-// One job (tile, octant) for the velocity chunks chunk0 .. chunk0 + nch - 1, by the whole
-// CTA: the job's row codes, task records, steps and moments are staged once, then each
-// chunk's rows are staged, swept and written back in turn.
+// Synchronisation of the threads sweeping one job: the whole CTA (bar 0) or the half of a
+// pair CTA (named barrier `bar` of N threads).
+// The barrier number is a compile-time constant (a register operand would make the kernel
+// reserve every hardware barrier and cut its residency); pairs exist only for teams of
+// whole warps.
+template <int N, int BAR>
+__device__ __forceinline__ void team_sync() {
+  if constexpr (BAR == 0 || N % 32 != 0) __syncthreads();
+  else asm volatile("bar.sync %0, %1;" ::"n"(BAR), "n"(N) : "memory");
+}
+template <int N, int BAR>
+__device__ __forceinline__ bool team_or(bool v) {
+  if constexpr (BAR == 0 || N % 32 != 0) {
+    return __syncthreads_or(v) != 0;
+  } else {
+    unsigned r;
+    asm volatile("{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.or.pred q, %2, %3, p;\n selp.u32 %0, 1, 0, q;\n}\n"
+                 : "=r"(r)
+                 : "r"((unsigned)v), "n"(BAR), "n"(N)
+                 : "memory");
+    return r != 0;
+  }
+}
+
+// One job (tile, octant) for the velocity chunks chunk0 .. chunk0 + nch - 1, by one team
+// (thread `tid` of THREADS, synchronised through `bar`): the job's row codes, task records,
+// steps and moments are staged once, then each chunk's rows are staged, swept and written
+// back in turn.
 // With `meta_bar` (an mbarrier in shared memory, initialised, phase 0) the three contiguous
 // metadata arrays arrive by bulk asynchronous copies issued by one thread; without it (the
 // persistent kernels, which run many jobs per CTA) every thread copies 16-byte pieces.
-template <typename T, int V, int NCH = 1>
+template <typename T, int V, int NCH = 1, int BAR = 0>
 __device__ __forceinline__ void tile_job(const DevState &a, int job, int chunk0, int slots_cap, int tasks_cap,
-                                         unsigned char *smem_raw, unsigned long long *meta_bar = nullptr) {
+                                         unsigned char *smem_raw, unsigned long long *meta_bar = nullptr,
+                                         int tid = (int)threadIdx.x) {
   constexpr int LPT = V / 2;                        // lanes per task
   constexpr int THREADS = LPT * groups_of<T, V>();
   constexpr int GROUPS = groups_of<T, V>();            // tasks in flight per pass
@@ -84,7 +110,7 @@ __device__ __forceinline__ void tile_job(const DevState &a, int job, int chunk0,
   //     multiple of four entries, records are 16 bytes, the step stride a multiple of eight)
   if (meta_bar) {
     const unsigned bar = smem_u32(meta_bar);
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
       const unsigned b_codes = (unsigned)((nrows + 3) / 4) * 16u, b_trec = (unsigned)ntask * 16u,
                      b_steps = (unsigned)tv.steps_stride * 2u;
       mbar_expect_arrive(bar, b_codes + b_trec + b_steps);
@@ -99,28 +125,28 @@ __device__ __forceinline__ void tile_job(const DevState &a, int job, int chunk0,
       while (!(ok = mbar_try(bar, 0)) && gtimer() - t0 < kWaitNs) {
       }
     }
-    if (__syncthreads_or(!ok)) {
-      if (threadIdx.x == 0) atomicExch(tv.err, 1);
+    if (team_or<THREADS, BAR>(!ok)) {
+      if (tid == 0) atomicExch(tv.err, 1);
       return;
     }
   } else {
-    for (int i = threadIdx.x; i < (nrows + 3) / 4; i += THREADS)
+    for (int i = tid; i < (nrows + 3) / 4; i += THREADS)
       cp_async16(Codes + 4 * i, tv.rows + rb + 4 * i);
-    for (int i = threadIdx.x; i < ntask; i += THREADS) cp_async16(Trec + i, tv.tasks + tb + i);
-    for (int i = threadIdx.x; i < tv.steps_stride / 8; i += THREADS)
+    for (int i = tid; i < ntask; i += THREADS) cp_async16(Trec + i, tv.tasks + tb + i);
+    for (int i = tid; i < tv.steps_stride / 8; i += THREADS)
       cp_async16(Steps + 8 * i, tv.steps + (size_t)job * tv.steps_stride + 8 * i);
     cp_async_wait_all();
-    __syncthreads();
+    team_sync<THREADS, BAR>();
   }
   // 1b. the moments of the tasks' nodes (FP64 Rho, Ux | Uy, Uz; written by the previous
   //     iteration), then, once the previous diagonal's rows are visible, the rows
-  for (int i = threadIdx.x; i < 2 * ntask; i += THREADS) {
+  for (int i = tid; i < 2 * ntask; i += THREADS) {
     const int m = Trec[i >> 1].x & ((1 << 27) - 1);
     cp_async16(Mom + i, reinterpret_cast<const double2 *>(a.mom) + 2 * (size_t)m + (i & 1));
   }
   asm volatile("griddepcontrol.wait;" ::: "memory");
-  if (threadIdx.x < PIECES) *reinterpret_cast<int4 *>(S + threadIdx.x * EPP) = make_int4(0, 0, 0, 0);
-  const int grp = threadIdx.x / LPT, sub = threadIdx.x % LPT;
+  if (tid < PIECES) *reinterpret_cast<int4 *>(S + tid * EPP) = make_int4(0, 0, 0, 0);
+  const int grp = tid / LPT, sub = tid % LPT;
   const int o = Codes[0] & 7;                       // own row code = node * 8 + octant
   const bool nx_ = neg_x(o), ny_ = neg_y(o), nz_ = neg_z(o);
   T *hw = const_cast<T *>(h);
@@ -128,8 +154,8 @@ __device__ __forceinline__ void tile_job(const DevState &a, int job, int chunk0,
 #pragma unroll 1
   for (int c = 0; c < NCH; ++c) {
     const int l0 = (chunk0 + c) * V;
-    if (c > 0) __syncthreads();                     // the previous chunk's write-back read S
-    for (int i = threadIdx.x; i < nrows * PIECES; i += THREADS) {
+    if (c > 0) team_sync<THREADS, BAR>();                     // the previous chunk's write-back read S
+    for (int i = tid; i < nrows * PIECES; i += THREADS) {
       const int r = i / PIECES, pc = i - r * PIECES;
       const int code = Codes[r];
       const T *src = ((code & kFwBit) ? fw : h) + (size_t)(code & ~kFwBit) * (size_t)Nc8 + l0 + pc * EPP;
@@ -142,23 +168,23 @@ __device__ __forceinline__ void tile_job(const DevState &a, int job, int chunk0,
     load_lane_consts<T>(a, lp, K);
 
     cp_async_wait_all();
-    __syncthreads();
+    team_sync<THREADS, BAR>();
 
     // 2. the part of every update that does not depend on this sweep's values,
     //    mu * (fEq - f_old / 2) (solver.F90:205-214), replaces f_old in the task's own slot
     base_pass<T, V, GROUPS>(a, Mom, S, 1, ntask, grp, sub, K, nx_, ny_, nz_);
-    __syncthreads();
+    team_sync<THREADS, BAR>();
 
     // 3. local hyperplanes: the upwind terms in the reference's order, then the division
     for (int s = 0; s < nsteps; ++s) {
       const int t0 = Steps[s], t1 = Steps[s + 1];
       if (t0 == t1) continue;
       for (int t = t0 + grp; t < t1; t += GROUPS) update_task<T, V>(a, S, Trec[t], 1 + t, sub, lp, K);
-      __syncthreads();
+      team_sync<THREADS, BAR>();
     }
 
     // 4. own rows -> global
-    for (int i = threadIdx.x; i < ntask * PIECES; i += THREADS) {
+    for (int i = tid; i < ntask * PIECES; i += THREADS) {
       const int r = i / PIECES, pc = i - r * PIECES;
       const int code = Codes[r];
       *reinterpret_cast<int4 *>(hw + (size_t)code * Nc8 + l0 + pc * EPP) =
@@ -191,6 +217,50 @@ k_tile_sweep(const DevState a, int job0, int slots_cap, int tasks_cap) {
   const int per_job = a.Nc8 / V / CPB;              // CTAs per job
   tile_job<T, V, CPB>(a, a.tv.job_list[job0 + (int)(blockIdx.x / per_job)], (int)(blockIdx.x % per_job) * CPB,
                       slots_cap, tasks_cap, smem_raw, kBulkMeta<T> ? &meta_bar : nullptr);
+}
+
+// A pair of jobs per CTA: two teams of threads_of<T, V>() threads, each sweeping one job in
+// its own part of the shared memory (the first job's part, sized for it, then the second's),
+// so that a large job and a small one share one CTA's allocation instead of each CTA
+// reserving room for the diagonal's largest job. Pairs are job_list[job0 + 2p, +1].
+__host__ __device__ inline size_t job_smem_bytes(int nrows, int ntask, int steps_stride, int row_bytes) {
+  return tile_smem_bytes(nrows + 1, ntask, steps_stride, row_bytes);
+}
+template <typename T, int V, int CPB>
+__global__ void __launch_bounds__(2 * threads_of<T, V>())
+k_tile_sweep_pairs(const DevState a, int job0, int njobs, unsigned smem_bytes) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ __align__(8) unsigned long long meta_bar[2];
+  constexpr int TH = threads_of<T, V>();
+  if (kBulkMeta<T>) {
+    if (threadIdx.x == 0) {
+      mbar_init(smem_u32(&meta_bar[0]), 1);
+      mbar_init(smem_u32(&meta_bar[1]), 1);
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+  }
+  const TileView &tv = a.tv;
+  const int per_pair = a.Nc8 / V / CPB;             // CTAs per pair
+  const int pr = (int)(blockIdx.x / per_pair), chunk0 = (int)(blockIdx.x % per_pair) * CPB;
+  const int half = (int)threadIdx.x / TH, tid = (int)threadIdx.x % TH;
+  const int q = 2 * pr + half;
+  if (q >= njobs) return;                           // the lone job of an odd count: one team
+  const int ja = tv.job_list[job0 + 2 * pr], job = tv.job_list[job0 + q];
+  const int rb = V * (int)sizeof(T);
+  const size_t off = half ? job_smem_bytes(tv.row_count[ja], (int)(tv.task_begin[ja + 1] - tv.task_begin[ja]),
+                                           tv.steps_stride, rb)
+                          : 0;
+  const int nrows = tv.row_count[job], ntask = (int)(tv.task_begin[job + 1] - tv.task_begin[job]);
+  if (off + job_smem_bytes(nrows, ntask, tv.steps_stride, rb) > smem_bytes) {
+    if (tid == 0) atomicExch(tv.err, 1);            // the plan's bound was exceeded: report, skip
+    return;
+  }
+  if (half == 0)
+    tile_job<T, V, CPB, 1>(a, job, chunk0, nrows + 1, ntask, smem_raw, kBulkMeta<T> ? &meta_bar[0] : nullptr, tid);
+  else
+    tile_job<T, V, CPB, 2>(a, job, chunk0, nrows + 1, ntask, smem_raw + off, kBulkMeta<T> ? &meta_bar[1] : nullptr,
+                           tid);
 }
 
 // Lets `fn` use all the shared memory a block may opt into, less its static shared memory.
@@ -338,11 +408,44 @@ void launch_cpb(const DevState &s, int job0, int njobs, int slots, int tasks, bo
   cudaLaunchKernelEx(&cfg, k_tile_sweep<T, V, CPB>, s, job0, slots, tasks);
 }
 
+// A launch of job pairs; slots / tasks are the largest sums of a pair (TileJobs::paired).
+template <typename T, int V, int CPB>
+void launch_pairs(const DevState &s, int job0, int njobs, int slots, int tasks, bool pdl, cudaStream_t st) {
+  once_per_device(reinterpret_cast<const void *>(k_tile_sweep_pairs<T, V, CPB>), [](int dev) {
+    allow_dynamic_smem(reinterpret_cast<const void *>(k_tile_sweep_pairs<T, V, CPB>), dev);
+  });
+  // both parts' layouts: the pair's slot and task sums, a second step array and the
+  // rounding of two code arrays
+  const size_t bytes = tile_smem_bytes(slots, tasks, s.tv.steps_stride, V * (int)sizeof(T)) +
+                       (size_t)s.tv.steps_stride * 2 + 32;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)((size_t)(njobs + 1) / 2 * (s.Nc8 / V / CPB)));
+  cfg.blockDim = dim3(2 * threads_of<T, V>());
+  cfg.dynamicSmemBytes = bytes;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, k_tile_sweep_pairs<T, V, CPB>, s, job0, njobs, (unsigned)bytes);
+}
+
 template <typename T, int V>
 void launch_one(const DevState &s, int job0, int njobs, int slots, int tasks, bool pdl, cudaStream_t st) {
   constexpr int C = kChunksPerCta<T>;
-  if (C > 1 && (s.Nc8 / V) % C == 0) launch_cpb<T, V, C>(s, job0, njobs, slots, tasks, pdl, st);
-  else launch_cpb<T, V, 1>(s, job0, njobs, slots, tasks, pdl, st);
+  const bool cpb = C > 1 && (s.Nc8 / V) % C == 0;
+  if constexpr (threads_of<T, V>() % 32 == 0) {
+    if (s.tv.paired) {
+      if (cpb) launch_pairs<T, V, C>(s, job0, njobs, slots, tasks, pdl, st);
+      else launch_pairs<T, V, 1>(s, job0, njobs, slots, tasks, pdl, st);
+      return;
+    }
+  }
+  {
+    if (cpb) launch_cpb<T, V, C>(s, job0, njobs, slots, tasks, pdl, st);
+    else launch_cpb<T, V, 1>(s, job0, njobs, slots, tasks, pdl, st);
+  }
 }
 
 }  // namespace
