@@ -141,6 +141,7 @@ __global__ void __launch_bounds__(256) k_walls32(const DevState a, int begin, in
   const int nface = P.nface;
   const int chunkw = LANES * VPL;
   auto far_ptr = [&](int code, int oo, int lf) -> const float * {
+    if (e2 == 0.f) return nullptr;  // as in k_walls32_onchip
     if (code >= 0) return a.h32 + hidx(code, oo, Nc8, lf);
     if (code == -1) return nullptr;
     const int cc = -code - 2;
@@ -257,7 +258,10 @@ __global__ void __launch_bounds__(256, 4) k_walls32_onchip(const DevState a, int
   const int nface = P.nface;
   const int lf = lane * VPL;
   const bool lv = lf < Nc8;
+  // the second extrapolation point only matters when its coefficient does (wallExtOrder 1
+  // makes it 0: the FP32 path, exact to its tolerance and not to the bit, skips the load)
   auto far_ptr = [&](int code, int oo) -> const float * {
+    if (e2 == 0.f) return nullptr;
     if (code >= 0) return a.h32 + hidx(code, oo, Nc8, lf);
     if (code == -1) return nullptr;
     const int cc = -code - 2;
