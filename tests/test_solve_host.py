@@ -156,6 +156,26 @@ def test_tolerance_rule_waits_past_a_turning_point():
     assert stop * 10 > 1000
 
 
+def test_prior_contraction_does_not_stop_at_a_turning_point():
+    """The FP64 phase of a refined solve starts with the contraction fitted in its FP32 phase
+    (prior_r). Fed the turning-point trace from anywhere before the turn, with that fit or a
+    too-fast or too-slow one, the rule still waits for the gate on the size of the changes
+    and stops within tolerance of the limit."""
+    import json
+    import os
+    ms = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "mass_trace_turning.json")))["masses"]
+    fp32 = Convergence(tol=1e-4)
+    for m in ms[:50]:
+        fp32.update(m, 1.0)
+    assert fp32.last_r is not None
+    for start in (30, 45, 55, 60, 65):
+        for r in (fp32.last_r, 0.5, 0.95):
+            c = Convergence(tol=1e-4, prior_r=r)
+            stop = next(start + k for k, m in enumerate(ms[start:]) if c.update(m, 1.0))
+            assert stop * 10 > 1000
+            assert abs(ms[stop] - ms[-1]) / abs(ms[-1]) <= 1e-4
+
+
 def test_watchdog_flags_non_finite_and_blowup():
     c = Convergence(tol=1e-4)
     for m in (1.0, 0.9, 0.85):
