@@ -4,8 +4,9 @@
  *
  * PIKS3D (Fortran 90 + MPI + OpenMP) has no library API: main.F90 drives zero-argument
  * module routines over module globals. Each entry point below replaces one of those
- * routines for a single-process, single-GPU run (the reference's mpi 1x1x1 layout) and
- * keeps its argument meaning, file formats and error behaviour. Every function takes
+ * routines for one GPU holding the box (the reference's mpi 1x1x1 layout; x slabs of a box
+ * over several GPUs: piks_set_decomposition) and keeps its argument meaning, file formats
+ * and error behaviour. Every function takes
  * plain pointers and sizes, is callable from C, C++, Fortran ISO_C_BINDING or ctypes,
  * and returns a piks_status (0 = success). piks_last_error() gives the message.
  *
@@ -41,7 +42,7 @@ typedef struct piks_params {
   double Ref_L;                  /* 1 (default) or 2                                     */
   int32_t Nc_fundamental;        /* velocityNml: half the points per velocity axis       */
   int32_t halfRange;             /* 1 = half-range Gauss-Hermite                          */
-  int32_t mpi_xdim, mpi_ydim, mpi_zdim;   /* mpiNml: read and ignored (one process)      */
+  int32_t mpi_xdim, mpi_ydim, mpi_zdim;   /* mpiNml: read; slabs via piks_set_decomposition */
   int32_t block_repx, block_repy, block_repz;
   int32_t maxStep, chkConvergeStep, saveStep;   /* solverNml */
   double eps;
@@ -126,6 +127,29 @@ piks_status piks_set_preprocessing(piks_ctx *ctx, int32_t where);
  * and drill / thin; voxel classification; the rest of the geometry and the sweep tasks; the
  * whole call (tile schedule, uploads and allocation included). */
 piks_status piks_setup_seconds(piks_ctx *ctx, double *out);
+
+/* ---- Extrapolation of the iteration (refined solves) ----
+ * The source iteration is affine, f_{n+1} = M f_n + b: its error e_n = M^n e_0 is soon
+ * dominated by a few slow modes of M. From states x_0 .. x_{k+1} taken every m iterations
+ * (m even), minimal polynomial extrapolation (MPE) finds the combination s = sum_j g_j x_j
+ * (j <= k) that cancels k modes: with u_j = x_{j+1} - x_j, c minimises |U c + u_k| over the
+ * first k differences, c_k = 1 and g = c / sum(c). k = 1 is Aitken's extrapolation of the
+ * whole state.
+ *   piks_snapshot_slot  copies the state the next iteration reads (f, fw, the moments, the
+ *                       lagged ghost planes) into slot `slot` of `nslots` (at most 8, one
+ *                       device buffer of nslots state sizes);
+ *   piks_snapshot_gram  the (n-1) x (n-1) Gram matrix of the differences of slots 0 .. n-1,
+ *                       summed in FP64 in a fixed order (the same states give the same matrix);
+ *   piks_snapshot_combine  the state becomes sum_j coef[j] * slot_j over slots 0 .. n-1
+ *                       (FP64 evaluation); slots must lie an even number of iterations from
+ *                       the current state.
+ * This takes the iteration off the reference's path: the refined solver (piks3d_b200.solve,
+ * FP32 + FP64 refinement) uses it and is judged by its permeability against the plain FP64
+ * solve; the plain FP64 solve never calls it. Single-box contexts only. No counterpart in
+ * the reference. */
+piks_status piks_snapshot_slot(piks_ctx *ctx, int32_t slot, int32_t nslots);
+piks_status piks_snapshot_gram(piks_ctx *ctx, int32_t n, double *gram);
+piks_status piks_snapshot_combine(piks_ctx *ctx, int32_t n, const double *coef);
 
 /* ---- One box over several GPUs: x slabs (setupVirtualProcessGrid, mpiParams.F90:120-240,
  * with mpi_xdim = nranks, mpi_ydim = mpi_zdim = 1; the halo exchange of solver.F90:146-170

@@ -69,6 +69,9 @@ def load():
         lib.oracle_halo_size.argtypes = [ctypes.c_void_p]
         lib.oracle_halo_send.argtypes = [ctypes.c_void_p, P(d), P(d)]
         lib.oracle_halo_recv.argtypes = [ctypes.c_void_p, P(d), P(d)]
+        lib.oracle_set_fw.argtypes = [ctypes.c_void_p, P(d)]
+        lib.oracle_set_macro.argtypes = [ctypes.c_void_p, P(d), P(d), P(d), P(d)]
+        lib.oracle_set_halo_send.argtypes = [ctypes.c_void_p, P(d), P(d)]
         _lib = lib
     return _lib
 
@@ -212,6 +215,23 @@ class Oracle:
         w, e = np.zeros(n), np.zeros(n)
         self.lib.oracle_halo_send(self.h, _d(w), _d(e))
         return w, e
+
+    def state(self):
+        """(f, fw, macro list, (west_snd, east_snd)): everything the next iteration reads."""
+        return self.f(), self.fw().copy(), [m.copy() for m in self.macro()], self.halo_send()
+
+    def set_state(self, st):
+        f, fw, mac, (w, e) = st
+        self.set_f(f)
+        d = self.dims()
+        fwb = np.zeros(max(1, d["nCorner"]) * d["Nc8"] * 8)
+        fwb[:fw.size] = fw
+        self.lib.oracle_set_fw(self.h, _d(fwb))
+        m = [np.ascontiguousarray(a, dtype=np.float64).reshape(-1) for a in mac]
+        self.lib.oracle_set_macro(self.h, *[_d(a) for a in m])
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        e = np.ascontiguousarray(e, dtype=np.float64)
+        self.lib.oracle_set_halo_send(self.h, _d(w), _d(e))
 
     def halo_recv(self, west, east):
         """Sets the messages received from the west / east neighbour for the next iteration."""

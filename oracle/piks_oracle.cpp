@@ -1009,6 +1009,17 @@ void oracle_halo_send(void *h, double *west, double *east) {
   std::copy(s->west_snd.begin(), s->west_snd.end(), west);
   std::copy(s->east_snd.begin(), s->east_snd.end(), east);
 }
+void oracle_set_fw(void *h, const double *in) { auto *s = static_cast<Oracle *>(h); std::copy(in, in + s->fw.size(), s->fw.begin()); }
+void oracle_set_macro(void *h, const double *rho, const double *ux, const double *uy, const double *uz) {
+  auto *s = static_cast<Oracle *>(h);
+  std::copy(rho, rho + s->Rho.size(), s->Rho.begin()); std::copy(ux, ux + s->Ux.size(), s->Ux.begin());
+  std::copy(uy, uy + s->Uy.size(), s->Uy.begin()); std::copy(uz, uz + s->Uz.size(), s->Uz.begin());
+}
+void oracle_set_halo_send(void *h, const double *west, const double *east) {
+  auto *s = static_cast<Oracle *>(h);
+  std::copy(west, west + s->west_snd.size(), s->west_snd.begin());
+  std::copy(east, east + s->east_snd.size(), s->east_snd.begin());
+}
 void oracle_halo_recv(void *h, const double *west, const double *east) {
   auto *s = static_cast<Oracle *>(h);
   std::copy(west, west + s->west_rcv.size(), s->west_rcv.begin());

@@ -97,6 +97,11 @@ void oracle_slab(void *h, int32_t *out);
 int64_t oracle_halo_size(void *h);
 void oracle_halo_send(void *h, double *west, double *east);
 void oracle_halo_recv(void *h, const double *west, const double *east);
+/* Setters of the rest of the iteration state (for tests that move the state: fw as
+ * oracle_get_fw, the macro fields as oracle_get_macro, the packed x messages). */
+void oracle_set_fw(void *h, const double *in);
+void oracle_set_macro(void *h, const double *rho, const double *ux, const double *uy, const double *uz);
+void oracle_set_halo_send(void *h, const double *west, const double *east);
 
 #ifdef __cplusplus
 }

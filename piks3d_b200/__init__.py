@@ -83,6 +83,9 @@ def load_library(path=LIB_PATH):
         "piks_set_preprocessing": (i32, [c_void_p, i32]),
         "piks_setup_seconds": (i32, [c_void_p, P(dbl)]),
         "piks_set_decomposition": (i32, [c_void_p, i32, i32]),
+        "piks_snapshot_slot": (i32, [c_void_p, i32, i32]),
+        "piks_snapshot_gram": (i32, [c_void_p, i32, P(dbl)]),
+        "piks_snapshot_combine": (i32, [c_void_p, i32, P(dbl)]),
         "piks_get_slab": (i32, [c_void_p, P(i32)]),
         "piks_halo_buffers": (i32, [c_void_p, i32, P(c_void_p), P(c_void_p), P(i64)]),
         "piks_kernel_times": (i32, [c_void_p, P(dbl), i32, i32]),
@@ -230,6 +233,21 @@ class Solver:
         a = (ctypes.c_double * 4)()
         _check(self.lib.piks_setup_seconds(self._ctx, a))
         return tuple(a)
+
+    def snapshot_slot(self, slot, nslots):
+        """Copies the iteration state into snapshot slot `slot` of `nslots` (device memory)."""
+        _check(self.lib.piks_snapshot_slot(self._ctx, int(slot), int(nslots)))
+
+    def snapshot_gram(self, n):
+        """(n-1) x (n-1) Gram matrix of the differences of slots 0 .. n-1 (FP64)."""
+        g = np.zeros((n - 1) * (n - 1))
+        _check(self.lib.piks_snapshot_gram(self._ctx, int(n), _dptr(g)))
+        return g.reshape(n - 1, n - 1)
+
+    def snapshot_combine(self, coef):
+        """The state becomes sum_j coef[j] * slot_j."""
+        c = np.ascontiguousarray(coef, dtype=np.float64)
+        _check(self.lib.piks_snapshot_combine(self._ctx, len(c), _dptr(c)))
 
     def set_decomposition(self, nranks, rank):
         """Makes this context rank `rank` of `nranks` x slabs of the box (before

@@ -82,6 +82,8 @@ void free_device(piks_ctx *c) {
   c->allocations.clear();
   c->dev_bytes = 0;
   c->have_geometry = false;
+  c->snap = nullptr;
+  c->snap_bytes = 0;
 }
 
 void release(piks_ctx *c, void *p) {
@@ -976,6 +978,11 @@ piks_status piks_set_precision(piks_ctx *c, int32_t precision) {
   cudaSetDevice(c->device);
   piks_status st = cuda_check(cudaStreamSynchronize(c->stream), "precision sync");
   if (st) return st;
+  if (c->snap) {  // snapshots of the other precision are of no further use: free them first
+    release(c, c->snap);
+    c->snap = nullptr;
+    c->snap_bytes = 0;
+  }
   if ((st = alloc_state(c, precision))) { free_state(c, precision); return st; }
   DevState &s = c->ds;
   const StateSizes z = state_sizes(c);
@@ -1244,6 +1251,150 @@ piks_status piks_setup_seconds(piks_ctx *c, double *out) {
   if (!c || !out) return fail(PIKS_ERR_ARG, "null argument");
   for (int i = 0; i < 4; ++i) out[i] = c->setup_seconds[i];
   return PIKS_OK;
+}
+
+// Regions of the iteration state, in snapshot order: f, fw (state precision), moments (FP64),
+// the west and east ghost planes the next iteration reads (state precision).
+struct StateRegion { void *p; size_t bytes; };
+static int state_regions(piks_ctx *c, StateRegion *r) {
+  const StateSizes z = state_sizes(c);
+  DevState &s = c->ds;
+  const bool f32 = c->prec == PIKS_PREC_FP32;
+  const size_t e = f32 ? sizeof(float) : sizeof(double);
+  const int par = c->iStep & 1;
+  r[0] = {f32 ? (void *)s.h32 : (void *)s.h, z.h * e};
+  r[1] = {f32 ? (void *)s.fw32 : (void *)s.fw, z.fw * e};
+  r[2] = {(void *)s.mom, (size_t)c->geo.NF * 4 * sizeof(double)};
+  r[3] = {f32 ? (void *)s.ghostW32[par] : (void *)s.ghostW[par], z.plane * e};
+  r[4] = {f32 ? (void *)s.ghostE32[par] : (void *)s.ghostE[par], z.plane * e};
+  return 5;
+}
+
+// Bytes of one snapshot slot (each region rounded up to 256 bytes).
+static size_t slot_bytes(piks_ctx *c) {
+  StateRegion r[5];
+  const int n = state_regions(c, r);
+  size_t b = 0;
+  for (int i = 0; i < n; ++i) b += (r[i].bytes + 255) / 256 * 256;
+  return b;
+}
+
+piks_status piks_snapshot_slot(piks_ctx *c, int32_t slot, int32_t nslots) {
+  if (!c) return fail(PIKS_ERR_ARG, "null context");
+  if (c->device < 0 || !c->have_geometry) return fail(PIKS_ERR_STATE, "snapshots need a device state");
+  if (c->setup.nranks > 1) return fail(PIKS_ERR_STATE, "snapshots cover single-box contexts");
+  if (nslots < 1 || nslots > kMaxSnapSlots || slot < 0 || slot >= nslots) return fail(PIKS_ERR_ARG, "bad snapshot slot");
+  cudaSetDevice(c->device);
+  const size_t sb = slot_bytes(c);
+  piks_status st;
+  if (c->snap && (c->snap_bytes < sb * (size_t)nslots || c->snap_prec != c->prec || c->snap_version != c->version)) {
+    release(c, c->snap);
+    c->snap = nullptr;
+    c->snap_bytes = 0;
+  }
+  if (!c->snap) {
+    void *p = nullptr;
+    const size_t need = sb * (size_t)nslots;
+    if ((st = cuda_check(cudaMalloc(&p, need), "snapshot slots"))) return st;
+    c->allocations.push_back({p, need});
+    c->dev_bytes += need;
+    c->snap = p;
+    c->snap_bytes = need;
+    c->snap_prec = c->prec;
+    c->snap_version = c->version;
+    for (auto &v : c->snap_steps) v = -1;
+  }
+  StateRegion r[5];
+  const int n = state_regions(c, r);
+  size_t off = sb * (size_t)slot;
+  for (int i = 0; i < n; ++i) {
+    if (r[i].bytes && (st = cuda_check(cudaMemcpyAsync(static_cast<char *>(c->snap) + off, r[i].p, r[i].bytes,
+                                                      cudaMemcpyDeviceToDevice, c->stream), "snapshot copy")))
+      return st;
+    off += (r[i].bytes + 255) / 256 * 256;
+  }
+  c->snap_steps[slot] = c->iStep;
+  return cuda_check(cudaStreamSynchronize(c->stream), "snapshot");
+}
+
+// Slots 0 .. n-1 hold states of this context's current allocation, all an even number of
+// iterations apart from each other and from the current state (their ghost planes are the
+// ones the next iteration reads).
+static piks_status check_slots(piks_ctx *c, int n) {
+  if (!c->have_geometry || !c->snap || c->snap_prec != c->prec || c->snap_version != c->version)
+    return fail(PIKS_ERR_STATE, "no snapshots of this state");
+  if (n < 1 || n > kMaxSnapSlots || slot_bytes(c) * (size_t)n > c->snap_bytes) return fail(PIKS_ERR_ARG, "bad slot count");
+  for (int j = 0; j < n; ++j)
+    if (c->snap_steps[j] < 0 || ((c->iStep - c->snap_steps[j]) & 1))
+      return fail(PIKS_ERR_STATE, "snapshot slot empty or an odd number of iterations away");
+  return PIKS_OK;
+}
+
+piks_status piks_snapshot_gram(piks_ctx *c, int32_t n, double *gram) {
+  if (!c || !gram) return fail(PIKS_ERR_ARG, "null argument");
+  if (n < 2) return fail(PIKS_ERR_ARG, "the Gram matrix of differences needs two slots or more");
+  piks_status st = check_slots(c, n);
+  if (st) return st;
+  cudaSetDevice(c->device);
+  StateRegion r[5];
+  const int nr = state_regions(c, r);
+  const bool f32 = c->prec == PIKS_PREC_FP32;
+  const size_t sb = slot_bytes(c);
+  const int nd = n - 1, npair = nd * (nd + 1) / 2;
+  const int nblk = kGramBlocks;
+  double *part = nullptr;
+  if ((st = cuda_check(cudaMalloc(&part, (size_t)nr * nblk * npair * sizeof(double)), "gram partials"))) return st;
+  size_t off = 0;
+  for (int i = 0; i < nr; ++i) {
+    const char *base = static_cast<const char *>(c->snap) + off;
+    double *pi = part + (size_t)i * nblk * npair;
+    if (i == 2 || !f32) launch_gram(reinterpret_cast<const double *>(base), sb, n, r[i].bytes / sizeof(double), pi, c->stream);
+    else launch_gram(reinterpret_cast<const float *>(base), sb, n, r[i].bytes / sizeof(float), pi, c->stream);
+    off += (r[i].bytes + 255) / 256 * 256;
+  }
+  std::vector<double> h((size_t)nr * nblk * npair);
+  st = cuda_check(cudaMemcpyAsync(h.data(), part, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "gram D2H");
+  if (!st) st = cuda_check(cudaStreamSynchronize(c->stream), "gram");
+  cudaFree(part);
+  if (st) return st;
+  // fixed summation order: regions, then blocks
+  int q = 0;
+  for (int a = 0; a < nd; ++a)
+    for (int b = a; b < nd; ++b, ++q) {
+      double sum = 0.0;
+      for (int i = 0; i < nr; ++i)
+        for (int k = 0; k < nblk; ++k) sum += h[((size_t)i * nblk + k) * npair + q];
+      gram[a * nd + b] = gram[b * nd + a] = sum;
+    }
+  return PIKS_OK;
+}
+
+piks_status piks_snapshot_combine(piks_ctx *c, int32_t n, const double *coef) {
+  if (!c || !coef) return fail(PIKS_ERR_ARG, "null argument");
+  piks_status st = check_slots(c, n);
+  if (st) return st;
+  for (int j = 0; j < n; ++j)
+    if (!std::isfinite(coef[j])) return fail(PIKS_ERR_ARG, "combination coefficient is not finite");
+  cudaSetDevice(c->device);
+  StateRegion r[5];
+  const int nr = state_regions(c, r);
+  const bool f32 = c->prec == PIKS_PREC_FP32;
+  const size_t sb = slot_bytes(c);
+  size_t off = 0;
+  for (int i = 0; i < nr; ++i) {
+    const char *base = static_cast<const char *>(c->snap) + off;
+    if (i == 2 || !f32)
+      launch_combine(static_cast<double *>(r[i].p), reinterpret_cast<const double *>(base), sb, n, coef,
+                     r[i].bytes / sizeof(double), c->stream);
+    else
+      launch_combine(static_cast<float *>(r[i].p), reinterpret_cast<const float *>(base), sb, n, coef,
+                     r[i].bytes / sizeof(float), c->stream);
+    off += (r[i].bytes + 255) / 256 * 256;
+  }
+  for (auto &v : c->snap_steps) v = -1;  // used up: the state moved off the iteration's path
+  st = cuda_check(cudaGetLastError(), "combine");
+  if (!st) st = cuda_check(cudaStreamSynchronize(c->stream), "combine");
+  return st;
 }
 
 piks_status piks_set_decomposition(piks_ctx *c, int32_t nranks, int32_t rank) {

@@ -44,6 +44,12 @@ struct piks_ctx {
   double setup_seconds[4] = {0, 0, 0, 0};  // last setup: box, classification, rest of the geometry, all
   int iStep = 0;
   int version = 0;                  // bumped whenever the device state is reallocated
+  // copies of the iteration state (piks_snapshot_slot): per slot f, fw, moments and the
+  // ghost planes the next iteration reads, slots back to back in one buffer
+  void *snap = nullptr;
+  size_t snap_bytes = 0;
+  int snap_prec = -1, snap_version = -1;
+  int snap_steps[8] = {-1, -1, -1, -1, -1, -1, -1, -1};  // iteration of each slot's copy
   double mass = 1.0, error = 1.0, permeability = 0.0;
   bool timing = false;
   double kt_ms[piks::KT_N] = {0};

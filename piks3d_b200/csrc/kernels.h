@@ -139,6 +139,19 @@ bool column_sweep_fits(const TileView &tv, int Nc8, bool fp32);
 // Halo rows of iteration parity `cap`: pack the rows this slab sends into its send buffers,
 // unpack the received buffers into its ghost-plane nodes (FP32 or FP64 state).
 void launch_halo(const DevState &s, bool fp32, int cap, cudaStream_t st);
+// State snapshots (piks_snapshot_slot): at most kMaxSnapSlots copies, `stride` bytes apart.
+constexpr int kMaxSnapSlots = 8;
+constexpr int kGramBlocks = 148 * 4;
+// Per-block FP64 sums of u_a[i] u_b[i] (a <= b < n - 1, u_a = slot_{a+1} - slot_a) over the
+// `count` elements of one region at `base` in every slot: partial[block][pair], pairs in
+// row order of the upper triangle; a fixed-size grid and fixed summation order.
+void launch_gram(const double *base, size_t stride, int n, size_t count, double *partial, cudaStream_t st);
+void launch_gram(const float *base, size_t stride, int n, size_t count, double *partial, cudaStream_t st);
+// dst[i] = sum_j coef[j] slot_j[i] over n slots, evaluated in FP64.
+void launch_combine(double *dst, const double *base, size_t stride, int n, const double *coef, size_t count,
+                    cudaStream_t st);
+void launch_combine(float *dst, const float *base, size_t stride, int n, const double *coef, size_t count,
+                    cudaStream_t st);
 void launch_widen(const float *src, double *dst, size_t n, cudaStream_t st);
 void launch_narrow(const double *src, float *dst, size_t n, cudaStream_t st);
 void launch_division_selftest(int64_t samples, uint64_t seed, unsigned long long *mismatches);

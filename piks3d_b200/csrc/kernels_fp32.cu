@@ -520,6 +520,86 @@ void launch_moments32(const DevState &s, cudaStream_t st) {
   else if (s.Nc8 % 2 == 0) k_moments32<2, 32><<<nblocks((size_t)s.NF * 32, 256), 256, 0, st>>>(s);
   else k_moments32<1, 32><<<nblocks((size_t)s.NF * 32, 256), 256, 0, st>>>(s);
 }
+template <typename T>
+__global__ void __launch_bounds__(256) k_gram(const char *base, size_t stride, int n, size_t count, double *partial) {
+  constexpr int kMaxD = kMaxSnapSlots - 1, kMaxPairs = kMaxD * (kMaxD + 1) / 2;
+  __shared__ double red[256];
+  const int nd = n - 1, npair = nd * (nd + 1) / 2;
+  double acc[kMaxPairs];
+#pragma unroll
+  for (int q = 0; q < kMaxPairs; ++q) acc[q] = 0.0;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (size_t)gridDim.x * blockDim.x) {
+    double x[kMaxSnapSlots], u[kMaxD];
+#pragma unroll
+    for (int j = 0; j < kMaxSnapSlots; ++j)
+      x[j] = j < n ? (double)reinterpret_cast<const T *>(base + (size_t)j * stride)[i] : 0.0;
+#pragma unroll
+    for (int a = 0; a < kMaxD; ++a) u[a] = x[a + 1] - x[a];
+    int q = 0;
+#pragma unroll
+    for (int a = 0; a < kMaxD; ++a)
+#pragma unroll
+      for (int b = a; b < kMaxD; ++b, ++q)
+        if (b < nd) acc[q] += u[a] * u[b];
+  }
+  // block sums in a fixed tree order, pair by pair
+  int q = 0;
+  for (int a = 0; a < nd; ++a)
+    for (int b = a; b < nd; ++b, ++q) {
+      double v = 0.0;
+#pragma unroll
+      for (int k = 0; k < kMaxPairs; ++k)
+        if (k == q) v = acc[k];
+      red[threadIdx.x] = v;
+      __syncthreads();
+      for (int w = 128; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+      }
+      if (threadIdx.x == 0) partial[(size_t)blockIdx.x * npair + q] = red[0];
+      __syncthreads();
+    }
+}
+template <typename T>
+void gram_any(const T *base, size_t stride, int n, size_t count, double *partial, cudaStream_t st) {
+  const int npair = (n - 1) * n / 2;
+  if (!count) {
+    cudaMemsetAsync(partial, 0, (size_t)kGramBlocks * npair * sizeof(double), st);
+    return;
+  }
+  k_gram<T><<<kGramBlocks, 256, 0, st>>>(reinterpret_cast<const char *>(base), stride, n, count, partial);
+}
+void launch_gram(const double *base, size_t stride, int n, size_t count, double *partial, cudaStream_t st) {
+  gram_any(base, stride, n, count, partial, st);
+}
+void launch_gram(const float *base, size_t stride, int n, size_t count, double *partial, cudaStream_t st) {
+  gram_any(base, stride, n, count, partial, st);
+}
+
+struct Coefs { double c[kMaxSnapSlots]; };
+template <typename T>
+__global__ void k_combine(T *dst, const char *base, size_t stride, int n, Coefs cf, size_t count) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (size_t)gridDim.x * blockDim.x) {
+    double v = 0.0;
+    for (int j = 0; j < n; ++j) v += cf.c[j] * (double)reinterpret_cast<const T *>(base + (size_t)j * stride)[i];
+    dst[i] = (T)v;
+  }
+}
+template <typename T>
+void combine_any(T *dst, const T *base, size_t stride, int n, const double *coef, size_t count, cudaStream_t st) {
+  if (!count) return;
+  Coefs cf{};
+  for (int j = 0; j < n && j < kMaxSnapSlots; ++j) cf.c[j] = coef[j];
+  k_combine<T><<<148 * 16, 256, 0, st>>>(dst, reinterpret_cast<const char *>(base), stride, n, cf, count);
+}
+void launch_combine(double *dst, const double *base, size_t stride, int n, const double *coef, size_t count,
+                    cudaStream_t st) {
+  combine_any(dst, base, stride, n, coef, count, st);
+}
+void launch_combine(float *dst, const float *base, size_t stride, int n, const double *coef, size_t count,
+                    cudaStream_t st) {
+  combine_any(dst, base, stride, n, coef, count, st);
+}
 void launch_widen(const float *src, double *dst, size_t n, cudaStream_t st) {
   if (n) k_widen<<<148 * 16, 256, 0, st>>>(src, dst, n);
 }

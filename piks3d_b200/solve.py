@@ -47,6 +47,7 @@ class Convergence:
         # refined solve): until enough checks exist for a fit of its own, the estimate uses it
         self.prior_r = prior_r
         self.last_r = None            # contraction of the last fit that met the residual bound
+        self.r_now = None             # contraction of this check's fit (None: no fit, or a poor one)
         # watchdog: a non-finite mass flux or error, or a mass flux `blowup` times the largest
         # of the first checks, marks the iteration as diverged (the reference would run on to
         # maxStep)
@@ -82,6 +83,7 @@ class Convergence:
         if self.tol is None:
             return error <= self.eps
         w = self.window
+        self.r_now = None
         if len(self.masses) < max(w + 1, self.min_checks):
             if self.prior_r is None or len(self.masses) < 2:
                 return False
@@ -105,6 +107,7 @@ class Convergence:
             good = r < 1.0 and res <= self.maxres
             if good:
                 self.last_r = r
+                self.r_now = r
             self.estimate = math.exp(a + b * (w - 1)) * r / (1.0 - r) if good else math.inf
         self._ok_run = self._ok_run + 1 if self.estimate <= self.safety * self.tol else 0
         self._gate_ok = self._gate_ok + 1 if self.last_change() <= self.gate * self.tol else 0
@@ -119,6 +122,59 @@ class Convergence:
         return self.since_best >= self.stall_checks
 
 
+class Extrapolator:
+    """Moves a refined solve's state toward the iteration's limit by minimal polynomial
+    extrapolation (MPE) of its checks.
+
+    The source iteration is affine (f_{n+1} = M f_n + b), so its error is soon a few slow
+    modes of M. After `burn` checks from the start or from the last jump, the states of
+    k + 2 consecutive checks x_0 .. x_{k+1} go to snapshot slots on the device; with the
+    differences u_j = x_{j+1} - x_j, c minimises |U c + u_k| over the first k differences
+    (from their Gram matrix), c_k = 1, and the state becomes sum_j g_j x_j (j <= k) with
+    g = c / sum(c): the combination that cancels k modes (k = 1: Aitken's extrapolation of
+    the whole state). The caller then starts a fresh stopping rule (the trace restarts from
+    the new state). Once the rule's estimate is below `quiet` times its tolerance the solve
+    is left to finish. Used in the FP32 phase of refined solves only; the plain FP64 solve
+    stays the reference's iteration."""
+
+    def __init__(self, k=3, burn=6, quiet=1.0):
+        self.k, self.burn, self.quiet = k, burn, quiet
+        self.since = 0
+        self.n = 0                    # slots filled in this round
+        self.jumps = 0
+
+    def slots(self):
+        return self.k + 2
+
+    def after_check(self, solver, conv):
+        """Call after each check with the solve's stopping rule; True when the state jumped."""
+        self.since += 1
+        if math.isfinite(conv.estimate) and conv.tol is not None and conv.estimate < self.quiet * conv.tol:
+            self.n = 0
+            return False
+        if self.since <= self.burn:
+            return False
+        k = self.k
+        solver.snapshot_slot(self.n, k + 2)
+        self.n += 1
+        if self.n < k + 2:
+            return False
+        self.n = 0
+        G = solver.snapshot_gram(k + 2)
+        c = np.linalg.lstsq(G[:k, :k], -G[:k, k], rcond=None)[0]
+        c = np.append(c, 1.0)
+        total = float(c.sum())
+        if not np.all(np.isfinite(c)) or abs(total) < 1e-12:
+            return False
+        g = c / total
+        if np.max(np.abs(g)) > 1e4:   # ill-conditioned: the differences are noise
+            return False
+        solver.snapshot_combine(g)
+        self.jumps += 1
+        self.since = 0
+        return True
+
+
 class Job:
     """One solve request: an image (uint8, z-y-x) and its piks_params."""
 
@@ -130,6 +186,7 @@ class Job:
         self.solver = None
         self.tuned = None             # (TX, TY, TZ, schedule) chosen by the batch runner's autotuner
         self.conv = None
+        self.ex = None                # Extrapolator of a refined job's FP32 phase
         self.phase = None             # "fp32" / "fp64"
         self.steps32 = 0
         self.steps = 0
@@ -139,11 +196,13 @@ class Job:
         self.footprint = None
 
 
-def footprint_bytes(image, params, precision="refined"):
+def footprint_bytes(image, params, precision="refined", slots=None):
     """HBM needed by a solve, estimated from the image before preprocessing: per fluid voxel
     the distribution function (8 octants x Nc8 velocities, FP32 or FP64) and its FP64 moments,
     plus the solid voxels next to fluid (walls) and a fixed overhead for tables. A refined
-    solve holds FP32 and FP64 copies of f for the instant of the switch."""
+    solve holds the extrapolator's snapshot slots of its FP32 state (`slots`, default the
+    Extrapolator's) during its FP32 phase, and FP32 and FP64 copies of f for the instant of
+    the switch (the slots are freed first)."""
     nc8 = params.Nc_fundamental ** 3
     if isinstance(image, tuple):      # (n voxels, porosity) before the image exists
         fluid = int(image[0] * image[1])
@@ -160,7 +219,9 @@ def footprint_bytes(image, params, precision="refined"):
         return f64 + moments + tables
     if precision == "fp32":
         return f32 + moments + tables
-    return f32 + f64 + moments + tables
+    if slots is None:
+        slots = Extrapolator().slots()
+    return max((f32 + moments) * (1 + slots), f32 + f64 + moments) + tables
 
 
 # Tile shapes the batch runner's autotuner times on each job (the batch sweeps every member
@@ -195,12 +256,13 @@ class BatchRunner:
     retired (state freed) as soon as they converge."""
 
     def __init__(self, device=0, precision="refined", tol=1e-4, eps=None, switch_eps=1e-6, switch_change=1e-6,
-                 max_members=64, hbm_budget=None, prep_threads=4, keep_fields=False, autotune=True):
+                 max_members=64, hbm_budget=None, prep_threads=4, keep_fields=False, autotune=True, extrapolate=True):
         import torch  # noqa: F401  (device memory query only)
         self.device, self.precision, self.tol, self.eps = device, precision, tol, eps
         self.switch_eps, self.max_members, self.keep_fields = switch_eps, max_members, keep_fields
         self.switch_change = switch_change
         self.autotune = autotune
+        self.extrapolate = extrapolate
         if hbm_budget is None:
             import torch
             free, _total = torch.cuda.mem_get_info(device)
@@ -236,7 +298,7 @@ class BatchRunner:
             img = (p.Nx * p.Ny * p.Nz, job.porosity if job.porosity is not None else 1.0)
         else:
             img = job.image
-        fp = footprint_bytes(img, job.params, self.precision)
+        fp = footprint_bytes(img, job.params, self.precision, slots=None if self.extrapolate else 0)
         if fp > self.hbm_budget:
             # can never fit, not even alone: refused rather than left to fail on allocation
             job.footprint = 0
@@ -267,6 +329,8 @@ class BatchRunner:
                     continue
                 job.phase = "fp64" if self.precision == "fp64" else "fp32"
                 job.conv = self._new_conv(job)
+                job.ex = Extrapolator() if (self.extrapolate and self.precision == "refined" and self.tol is not None) \
+                    else None
                 self.batch.add(job.solver)
                 self.active.append(job)
             else:
@@ -312,10 +376,14 @@ class BatchRunner:
                 job.result = {"steps": job.steps, "steps32": job.steps32, "mass": float(mass[i]),
                               "permeability": float(perm[i]), "error": float(err[i]),
                               "converged": bool(conv), "diverged": job.conv.diverged,
-                              "estimate": job.conv.estimate, "tiles": job.tuned}
+                              "estimate": job.conv.estimate, "tiles": job.tuned,
+                              "jumps": job.ex.jumps if job.ex else 0}
                 if self.keep_fields:
                     job.result["macro"] = job.solver.get_macro()
                 done.append(job)
+                continue
+            if job.ex is not None and job.phase == "fp32" and job.ex.after_check(job.solver, job.conv):
+                job.conv = self._new_conv(job)
         done_solved = list(done)
         done = ended + done
         for job in done_solved:
@@ -341,9 +409,11 @@ class BatchRunner:
 
 
 def solve_one(image, params, device=0, precision="fp64", tol=None, eps=None, switch_eps=1e-6, switch_change=1e-6,
-              tiles=None, keep_fields=False):
+              tiles=None, keep_fields=False, extrapolate=True):
     """One solve through a context of its own (no batch): the reference's loop with the same
-    stopping rule as the batch runner. Returns a result dict."""
+    stopping rule as the batch runner. With a tolerance, the FP32 phase of a refined solve
+    also extrapolates its state along its slowest mode (Extrapolator; `extrapolate`).
+    Returns a result dict."""
     s = Solver(params, device=device)
     if tiles is not None:
         s.set_tiles(*tiles)
@@ -355,6 +425,7 @@ def solve_one(image, params, device=0, precision="fp64", tol=None, eps=None, swi
     phase = "fp64" if precision == "fp64" else "fp32"
     base_eps = eps if eps is not None else params.eps
     conv = Convergence(eps=max(base_eps, switch_eps) if precision == "refined" else base_eps, tol=tol)
+    ex = Extrapolator() if (extrapolate and precision == "refined" and tol is not None) else None
     steps = steps32 = 0
     while True:
         s.iterate(chk)
@@ -373,8 +444,10 @@ def solve_one(image, params, device=0, precision="fp64", tol=None, eps=None, swi
         if ok or conv.diverged or steps >= params.maxStep:
             res = {"steps": steps, "steps32": steps32, "mass": m, "permeability": k, "error": e,
                    "converged": bool(ok), "diverged": conv.diverged, "estimate": conv.estimate,
-                   "setup_seconds": setup_seconds}
+                   "setup_seconds": setup_seconds, "jumps": ex.jumps if ex else 0}
             if keep_fields:
                 res["macro"] = s.get_macro()
             s.close()
             return res
+        if ex is not None and phase == "fp32" and ex.after_check(s, conv):
+            conv = Convergence(eps=max(base_eps, switch_eps), tol=tol)
