@@ -542,14 +542,16 @@ __global__ void __launch_bounds__(256) k_gram(const char *base, size_t stride, i
       for (int b = a; b < kMaxD; ++b, ++q)
         if (b < nd) acc[q] += u[a] * u[b];
   }
-  // block sums in a fixed tree order, pair by pair
+  // block sums in a fixed tree order, pair by pair (acc is indexed over the kMaxD triangle,
+  // the output over the nd triangle)
   int q = 0;
   for (int a = 0; a < nd; ++a)
     for (int b = a; b < nd; ++b, ++q) {
+      const int qa = a * kMaxD - a * (a - 1) / 2 + (b - a);
       double v = 0.0;
 #pragma unroll
       for (int k = 0; k < kMaxPairs; ++k)
-        if (k == q) v = acc[k];
+        if (k == qa) v = acc[k];
       red[threadIdx.x] = v;
       __syncthreads();
       for (int w = 128; w > 0; w >>= 1) {
