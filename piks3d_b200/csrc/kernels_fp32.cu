@@ -296,11 +296,14 @@ __global__ void __launch_bounds__(256, 4) k_walls32_onchip(const DevState a, int
           else st32<VPL>(a.fw32 + hidx(corner, oo, Nc8, lf), ext[mm]);
         }
       }
+      // the four octants of a velocity summed in FP32 (one conversion per velocity rather
+      // than four; FP64 ops and conversions are the kernel's short-scoreboard stalls), the
+      // velocities and lanes in FP64
 #pragma unroll
       for (int v = 0; v < VPL; ++v) {
         const int l = lf + v;
         const double ca = dir < 2 ? __ldg(a.cx + l) : dir < 4 ? __ldg(a.cy + l) : __ldg(a.cz + l);
-        racc += ca * (((double)ext[0][v] + (double)ext[1][v]) + (double)ext[2][v] + (double)ext[3][v]);
+        racc += ca * (double)__fadd_rn(__fadd_rn(__fadd_rn(ext[0][v], ext[1][v]), ext[2][v]), ext[3][v]);
       }
     }
     // segment sum in FP64 (the FP32 path does not keep the reference's summation order)
@@ -308,14 +311,20 @@ __global__ void __launch_bounds__(256, 4) k_walls32_onchip(const DevState a, int
     if (fi == 0) rho0 = racc; else if (fi == 1) rho1 = racc; else rho2 = racc;
   }
   if (!lv) return;
-  const double r0 = rho0 / a.DiffFlux, r1 = rho1 / a.DiffFlux, r2 = rho2 / a.DiffFlux;
-  const double one_m = 1.0 - a.accom;
+  // re-emission in FP32: accom * rho_face rounded once per face, then w * that + (1 - accom)
+  // * the extrapolated value, with the weights rounded to FP32 (vtab32 column 3)
+  const float af[3] = {(float)(a.accom * (rho0 / a.DiffFlux)), (float)(a.accom * (rho1 / a.DiffFlux)),
+                       (float)(a.accom * (rho2 / a.DiffFlux))};
+  const float one_m = (float)(1.0 - a.accom);
+  float wl[VPL];
+#pragma unroll
+  for (int v = 0; v < VPL; ++v) wl[v] = __ldg(a.vtab32 + (size_t)(lf + v) * kVtab + 3);
   for (int k = 0; k < P.nwr; ++k) {
     const float *sp = E + (size_t)P.src[k] * Nc8 + lf;
-    const double rf = P.face[k] == 0 ? r0 : P.face[k] == 1 ? r1 : r2;
+    const float rf = P.face[k] == 0 ? af[0] : P.face[k] == 1 ? af[1] : af[2];
     float val[VPL];
 #pragma unroll
-    for (int v = 0; v < VPL; ++v) val[v] = (float)(a.accom * __ldg(a.w + lf + v) * rf + one_m * (double)sp[v]);
+    for (int v = 0; v < VPL; ++v) val[v] = __fmaf_rn(rf, wl[v], __fmul_rn(one_m, sp[v]));
     if (P.dst_store[k] == ST_F) st32<VPL>(a.h32 + hidx(node, P.dst_o[k], Nc8, lf), val);
     else st32<VPL>(a.fw32 + hidx(corner, P.dst_o[k], Nc8, lf), val);
   }
