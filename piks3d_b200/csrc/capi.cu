@@ -567,6 +567,18 @@ piks_status piks_setup_physical_grid(piks_ctx *c, const uint8_t *raw, int64_t nb
   UP(v.cx, cx, pd); UP(v.cy, cy, pd); UP(v.cz, cz, pd); UP(v.w, w, pd);
   UP(g.wall_node, wall_node, pi); UP(g.wall_label, wall_label, pi); UP(g.wall_corner, wall_corner, pi);
   UP(g.wall_nb, wall_nb, pi); UP(g.wall_order, wall_order, pi); UP(g.wall_e, wall_e, pd);
+  {
+    std::vector<int32_t> rec(g.wall_order.size() * 16, 0);
+    for (size_t w = 0; w < g.wall_order.size(); ++w) {
+      const size_t q = (size_t)g.wall_order[w];
+      int32_t *r = &rec[w * 16];
+      r[0] = g.wall_node[q]; r[1] = g.wall_corner[q]; r[2] = g.wall_label[q];
+      std::memcpy(r + 4, &g.wall_e[2 * q], 2 * sizeof(double));
+      for (int k = 0; k < 6; ++k) r[8 + k] = g.wall_nb[6 * q + k];
+    }
+    if ((st = upload(c, rec, &pi))) return st;
+    s.wall_rec = reinterpret_cast<const int4 *>(pi);
+  }
   UP(g.commit, commit, pi);
   UP(g.plane_x1, plane_x1, pi); UP(g.plane_xN, plane_xN, pi);
   UP(g.sym_node, sym_node, pi); UP(g.sym_flag, sym_flag, pu8);

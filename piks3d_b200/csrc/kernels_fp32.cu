@@ -249,12 +249,13 @@ __global__ void __launch_bounds__(256, 4) k_walls32_onchip(const DevState a, int
   const unsigned seg = LANES == 32 ? 0xffffffffu : (((1u << LANES) - 1u) << (threadIdx.x & 31 & ~(LANES - 1)));
   const int Nc8 = a.Nc8;
   float *E = wall32_sm + (size_t)wib * 12 * Nc8;
-  const int q = a.wall_order[widx];
-  const int node = a.wall_node[q];
-  const int corner = a.wall_corner[q];
-  const WPlan &P = c32_plan[c32_prog_of[a.wall_label[q]]];
-  const float e1 = (float)a.wall_e[2 * q], e2 = (float)a.wall_e[2 * q + 1];
-  const int *nb = a.wall_nb + 6 * q;
+  const int4 *rp = a.wall_rec + (size_t)widx * 4;
+  const int4 r0 = __ldg(rp);
+  const double2 ee = __ldg(reinterpret_cast<const double2 *>(rp + 1));
+  const int node = r0.x;
+  const int corner = r0.y;
+  const WPlan &P = c32_plan[c32_prog_of[r0.z]];
+  const float e1 = (float)ee.x, e2 = (float)ee.y;
   const int nface = P.nface;
   const int lf = lane * VPL;
   const bool lv = lf < Nc8;
@@ -271,7 +272,10 @@ __global__ void __launch_bounds__(256, 4) k_walls32_onchip(const DevState a, int
   double rho0 = 0.0, rho1 = 0.0, rho2 = 0.0;
   for (int fi = 0; fi < nface; ++fi) {
     const int dir = P.dir[fi], st = P.store[fi], keep = P.keep[fi];
-    const int n1 = nb[2 * fi], code = nb[2 * fi + 1];
+    // the face's (neighbour, far point) pair from the record's second half (the same
+    // 128-byte line as its first, so an L1 hit after the loads above)
+    const int2 nbp = __ldg(reinterpret_cast<const int2 *>(rp + 2) + fi);
+    const int n1 = nbp.x, code = nbp.y;
     double racc = 0.0;
     if (lv) {
       float nv[4][VPL], fv[4][VPL];
