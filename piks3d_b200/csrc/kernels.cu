@@ -353,7 +353,7 @@ __global__ void __launch_bounds__(256, 5) k_walls(const DevState a, int begin, i
 // order; per warp, 12 * Nc8 face values and Nc8 density terms.
 constexpr int kWallWarps = 8;
 template <int VPL>
-__global__ void __launch_bounds__(kWallWarps * 32, 4) k_walls_onchip(const DevState a, int begin, int end, int gbuf) {
+__global__ void __launch_bounds__(kWallWarps * 32, 3) k_walls_onchip(const DevState a, int begin, int end, int gbuf) {
   extern __shared__ __align__(16) double wall_sm[];
   const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int widx = begin + (int)blockIdx.x * kWallWarps + wib;
@@ -361,19 +361,23 @@ __global__ void __launch_bounds__(kWallWarps * 32, 4) k_walls_onchip(const DevSt
   const int Nc8 = a.Nc8;
   double *E = wall_sm + (size_t)wib * 13 * Nc8;
   double *Tm = E + 12 * Nc8;
-  const int q = a.wall_order[widx];
-  const int node = a.wall_node[q];
-  const int corner = a.wall_corner[q];
-  const WPlan &P = c_plan[c_prog_of[a.wall_label[q]]];
-  const double e1 = a.wall_e[2 * q], e2 = a.wall_e[2 * q + 1];
-  const int *nb = a.wall_nb + 6 * q;
+  // the wall's fields from its level-order record (one round trip; see DevState::wall_rec)
+  const int4 *rp = a.wall_rec + (size_t)widx * 4;
+  const int4 r0 = __ldg(rp);
+  const double2 ee = __ldg(reinterpret_cast<const double2 *>(rp + 1));
+  const int node = r0.x;
+  const int corner = r0.y;
+  const WPlan &P = c_plan[c_prog_of[r0.z]];
+  const double e1 = ee.x, e2 = ee.y;
   const int nface = P.nface;
   const int lf = lane * VPL;
   const bool lv = lf < Nc8;
   double rho0 = 0.0, rho1 = 0.0, rho2 = 0.0;
   for (int fi = 0; fi < nface; ++fi) {
     const int dir = P.dir[fi], st = P.store[fi], keep = P.keep[fi];
-    const int n1 = nb[2 * fi], code = nb[2 * fi + 1];
+    // the face's (neighbour, far point) pair: the record's second half, an L1 hit
+    const int2 nbp = __ldg(reinterpret_cast<const int2 *>(rp + 2) + fi);
+    const int n1 = nbp.x, code = nbp.y;
     if (lv) {
       const double *plane = nullptr;
       size_t prow = 0;

@@ -52,10 +52,11 @@ struct DevState {
   const int32_t *wall_node, *wall_label, *wall_corner, *wall_nb, *wall_order;
   const double *wall_e;
   // the same fields in level order, one 64-byte record (four int4) per wall position:
-  // node, corner, label, 0 | e1, e2 (FP64) | nb[0..3] | nb[4], nb[5], 0, 0; the FP32 on-chip
-  // wall kernel reads a wall's fields in one round trip instead of two (wall_order, then the
-  // rest): 0.476 -> 0.446 ms per iteration on a 128^3 pack. The FP64 kernel keeps the separate
-  // arrays (0.834 ms against 0.870 with the records: one more register spill there)
+  // node, corner, label, 0 | e1, e2 (FP64) | nb[0..3] | nb[4], nb[5], 0, 0; the on-chip wall
+  // kernels read a wall's fields in one round trip instead of two (wall_order, then the
+  // rest). Per iteration on a 128^3 pack: FP32 0.476 -> 0.446 ms; FP64 0.845 -> 0.758 ms
+  // together with three blocks per SM instead of four (no register spills; the records alone
+  // at four blocks spilled and took 0.870 against 0.834)
   const int4 *wall_rec;
   // post-sweep switch commits
   int ncommit;

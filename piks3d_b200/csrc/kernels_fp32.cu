@@ -240,7 +240,7 @@ __global__ void __launch_bounds__(256) k_walls32(const DevState a, int begin, in
 // per wall): the re-emission reads them there (WPlan) instead of re-loading the slots,
 // and a face value is stored only where it is the slot's final content.
 template <int VPL, int LANES>
-__global__ void __launch_bounds__(256, 4) k_walls32_onchip(const DevState a, int begin, int end, int gbuf) {
+__global__ void __launch_bounds__(256, 3) k_walls32_onchip(const DevState a, int begin, int end, int gbuf) {
   extern __shared__ __align__(16) float wall32_sm[];
   const int wib = threadIdx.x / LANES;
   const int widx = begin + (int)blockIdx.x * (256 / LANES) + wib;
