@@ -350,10 +350,13 @@ __global__ void __launch_bounds__(256, 5) k_walls(const DevState a, int begin, i
 // the extrapolated face values kept in shared memory: the re-emission reads them there
 // (WPlan) instead of re-loading the slots, and a face value is stored only where it is
 // the slot's final content. Same operations on the same operands as k_walls, in the same
-// order; per warp, 12 * Nc8 face values and Nc8 density terms.
-constexpr int kWallWarps = 8;
+// order; per warp, 12 * Nc8 face values and Nc8 density terms. One wall (warp) per block,
+// 24 blocks per SM (74 registers, no spills): a block's shared memory is free as soon as its
+// wall is done (per iteration on a 128^3 pack: 8 walls per block 0.758 ms, 4 0.698, 2 0.648,
+// 1 0.615).
+constexpr int kWallWarps = 1;
 template <int VPL>
-__global__ void __launch_bounds__(kWallWarps * 32, 3) k_walls_onchip(const DevState a, int begin, int end, int gbuf) {
+__global__ void __launch_bounds__(kWallWarps * 32, 24 / kWallWarps) k_walls_onchip(const DevState a, int begin, int end, int gbuf) {
   extern __shared__ __align__(16) double wall_sm[];
   const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int widx = begin + (int)blockIdx.x * kWallWarps + wib;

@@ -55,8 +55,8 @@ struct DevState {
   // node, corner, label, 0 | e1, e2 (FP64) | nb[0..3] | nb[4], nb[5], 0, 0; the on-chip wall
   // kernels read a wall's fields in one round trip instead of two (wall_order, then the
   // rest). Per iteration on a 128^3 pack: FP32 0.476 -> 0.446 ms; FP64 0.845 -> 0.758 ms
-  // together with three blocks per SM instead of four (no register spills; the records alone
-  // at four blocks spilled and took 0.870 against 0.834)
+  // together with up to 85 registers per thread instead of 64 (no spills; the records alone at 64
+  // registers spilled and took 0.870 against 0.834)
   const int4 *wall_rec;
   // post-sweep switch commits
   int ncommit;
