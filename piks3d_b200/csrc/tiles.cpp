@@ -1,5 +1,6 @@
 // Tile-wavefront schedule of the sweep tasks (TileJobs, declared in piks_internal.h).
 #include <algorithm>
+#include <atomic>
 #include <numeric>
 #include <thread>
 
@@ -9,20 +10,32 @@ namespace piks {
 
 namespace {
 
-// Runs fn(begin, end) over [0, n) split into contiguous chunks on up to 16 threads.
-template <typename F>
-void parallel_chunks(int64_t n, F fn) {
+// Number of contiguous chunks parallel_chunks splits [0, n) into (one per thread, up to 16).
+int chunk_count(int64_t n) {
   unsigned hw = std::thread::hardware_concurrency();
   int nt = (int)std::min<unsigned>(hw ? hw : 1, 16u);
-  if (n < 4096) nt = 1;
-  if (nt <= 1) { fn((int64_t)0, n); return; }
+  return n < 4096 ? 1 : std::max(nt, 1);
+}
+
+// Runs fn(chunk, begin, end) over [0, n) split into chunk_count(n) contiguous chunks, one
+// thread each.
+template <typename F>
+void parallel_chunks_indexed(int64_t n, F fn) {
+  const int nt = chunk_count(n);
+  if (nt <= 1) { fn(0, (int64_t)0, n); return; }
   std::vector<std::thread> th;
   th.reserve((size_t)nt);
   for (int i = 0; i < nt; ++i) {
     const int64_t b = n * i / nt, e = n * (i + 1) / nt;
-    th.emplace_back([=, &fn] { fn(b, e); });
+    th.emplace_back([=, &fn] { fn(i, b, e); });
   }
   for (auto &t : th) t.join();
+}
+
+// Runs fn(begin, end) over [0, n) split into contiguous chunks on up to 16 threads.
+template <typename F>
+void parallel_chunks(int64_t n, F fn) {
+  parallel_chunks_indexed(n, [&fn](int, int64_t b, int64_t e) { fn(b, e); });
 }
 
 // Row de-duplication inside one job: open addressing on the row index, cleared by a
@@ -265,42 +278,104 @@ bool build_tile_jobs(const Geometry &g, int TX, int TY, int TZ, int max_slots, T
   const int64_t GX = g.GX, GXY = (int64_t)g.GX * g.GY;
   const int64_t ntask = (int64_t)(g.tasks.size() / 8);
   const int nsteps = tj.nsteps;
-  // (octant, tile) pair and local step of every task
+  // (octant, tile) pair and local step of every task. A node's ghosted coordinates are
+  // found once (its octants are up to eight tasks); the tile of a coordinate and its local
+  // position from either side come from per-axis tables over the ghosted extent.
+  struct AxisTable { std::vector<int32_t> tile, pos, neg; };
+  auto axis_table = [](int G, int N, int T) {
+    AxisTable t{std::vector<int32_t>((size_t)G), std::vector<int32_t>((size_t)G), std::vector<int32_t>((size_t)G)};
+    for (int X = 0; X < G; ++X) {
+      const int x = X - 2, a = x / T, hi = std::min((a + 1) * T, N) - 1;
+      t.tile[(size_t)X] = a;
+      t.pos[(size_t)X] = x - a * T;
+      t.neg[(size_t)X] = hi - x;
+    }
+    return t;
+  };
+  const AxisTable ax = axis_table(g.GX, Nx, TX), ay = axis_table(g.GY, Ny, TY), az = axis_table(g.GZ, Nz, TZ);
+  const int64_t nnode = (int64_t)g.node_g.size();
+  BigVec<uint64_t> xyz((size_t)nnode);  // X | Y << 21 | Z << 42 (ghosted coordinates)
+  parallel_chunks(nnode, [&](int64_t b, int64_t e) {
+    for (int64_t n = b; n < e; ++n) {
+      const int64_t gi = g.node_g[(size_t)n];
+      xyz[(size_t)n] = (uint64_t)(gi % GX) | ((uint64_t)((gi / GX) % g.GY) << 21) | ((uint64_t)(gi / GXY) << 42);
+    }
+  });
   BigVec<int32_t> pair_of((size_t)ntask);
   BigVec<uint16_t> step((size_t)ntask);
   parallel_chunks(ntask, [&](int64_t b, int64_t e) {
     for (int64_t t = b; t < e; ++t) {
       const int32_t *r = &g.tasks[(size_t)t * 8];
       const int node = r[0], o = r[1] & 7;
-      const int64_t gi = g.node_g[(size_t)node];
-      const int x = (int)(gi % GX) - 2, y = (int)((gi / GX) % g.GY) - 2, z = (int)(gi / GXY) - 2;
-      const int a = x / TX, bb = y / TY, c = z / TZ;
-      const int xhi = std::min((a + 1) * TX, Nx) - 1, yhi = std::min((bb + 1) * TY, Ny) - 1,
-                zhi = std::min((c + 1) * TZ, Nz) - 1;
-      const int u = oct_sx(o) > 0 ? x - a * TX : xhi - x;
-      const int v = oct_sy(o) > 0 ? y - bb * TY : yhi - y;
-      const int w = oct_sz(o) > 0 ? z - c * TZ : zhi - z;
+      const uint64_t q = xyz[(size_t)node];
+      const size_t X = (size_t)(q & 0x1FFFFF), Y = (size_t)((q >> 21) & 0x1FFFFF), Z = (size_t)(q >> 42);
+      const int a = ax.tile[X], bb = ay.tile[Y], c = az.tile[Z];
+      const int u = oct_sx(o) > 0 ? ax.pos[X] : ax.neg[X];
+      const int v = oct_sy(o) > 0 ? ay.pos[Y] : ay.neg[Y];
+      const int w = oct_sz(o) > 0 ? az.pos[Z] : az.neg[Z];
       step[(size_t)t] = (uint16_t)(u + v + w);
       pair_of[(size_t)t] = (int32_t)((int64_t)o * ntiles + a + (int64_t)nTx * (bb + (int64_t)nTy * c));
     }
   });
   // The passes over all tasks below run one thread per octant: the pairs, jobs and output
   // positions of different octants are disjoint, and each thread visits its tasks in order.
+  // The tasks lie in hyperplane order with a hyperplane's octants one after another, so an
+  // octant's tasks form one segment per hyperplane (found by binary search) and a thread
+  // visits only its octant's segments; should the tasks not be grouped that way, the count
+  // pass misses tasks and every pass falls back to scanning all tasks.
+  std::vector<std::vector<std::pair<int64_t, int64_t>>> oct_seg(8);
+  {
+    const auto &hs = g.hyper_start;
+    auto oct = [&](int64_t t) { return g.tasks[(size_t)t * 8 + 1] & 7; };
+    for (size_t h = 0; h + 1 < hs.size(); ++h) {
+      int64_t b = hs[h];
+      const int64_t e = hs[h + 1];
+      for (int o = 0; o < 8; ++o) {
+        int64_t lo = b, hi = e;  // first task in [b, e) whose octant is above o
+        while (lo < hi) {
+          const int64_t m = lo + (hi - lo) / 2;
+          if (oct(m) <= o) lo = m + 1; else hi = m;
+        }
+        if (lo > b) oct_seg[(size_t)o].push_back({b, lo});
+        b = lo;
+      }
+    }
+  }
+  bool segmented = true;
+  // fn(lo, hi, begin, end): the octant's pairs are [lo, hi), its tasks lie among [begin, end)
   auto by_octant = [&](auto fn) {
-    if (ntask < 4096) { for (int o = 0; o < 8; ++o) fn((int64_t)o * ntiles, (int64_t)(o + 1) * ntiles); return; }
+    auto run = [&](int o) {
+      const int64_t lo = (int64_t)o * ntiles, hi = lo + ntiles;
+      if (segmented) {
+        for (const auto &sg : oct_seg[(size_t)o]) fn(lo, hi, sg.first, sg.second);
+      } else {
+        fn(lo, hi, (int64_t)0, ntask);
+      }
+    };
+    if (ntask < 4096) { for (int o = 0; o < 8; ++o) run(o); return; }
     std::vector<std::thread> th;
-    for (int o = 0; o < 8; ++o) th.emplace_back([&fn, o, ntiles] { fn((int64_t)o * ntiles, (int64_t)(o + 1) * ntiles); });
+    for (int o = 0; o < 8; ++o) th.emplace_back([&run, o] { run(o); });
     for (auto &x : th) x.join();
   };
   // jobs = non-empty pairs, ordered by (diagonal * 8 + octant), then tile (counting sort)
   const int64_t npairs = ntiles * 8;
   std::vector<int32_t> pair_tasks((size_t)npairs, 0);
-  by_octant([&](int64_t lo, int64_t hi) {
-    for (int64_t t = 0; t < ntask; ++t) {
+  std::atomic<int64_t> counted{0};
+  auto count_pairs = [&](int64_t lo, int64_t hi, int64_t tb, int64_t te) {
+    int64_t k = 0;
+    for (int64_t t = tb; t < te; ++t) {
       const int64_t pr = pair_of[(size_t)t];
-      if (pr >= lo && pr < hi) pair_tasks[(size_t)pr]++;
+      if (pr >= lo && pr < hi) { pair_tasks[(size_t)pr]++; ++k; }
     }
-  });
+    counted += k;
+  };
+  by_octant(count_pairs);
+  if (counted.load() != ntask) {
+    segmented = false;
+    counted = 0;
+    std::fill(pair_tasks.begin(), pair_tasks.end(), 0);
+    by_octant(count_pairs);
+  }
   auto dio_of = [&](int64_t pr) {
     const int o = (int)(pr / ntiles);
     const int64_t tl = pr % ntiles;
@@ -333,8 +408,8 @@ bool build_tile_jobs(const Geometry &g, int TX, int TY, int TZ, int max_slots, T
   for (int32_t j = 0; j < njobs; ++j)
     tj.task_begin[(size_t)j + 1] = tj.task_begin[(size_t)j] + pair_tasks[(size_t)job_pair[(size_t)j]];
   std::vector<int32_t> jstep((size_t)njobs * nsteps + 1, 0);  // tasks per (job, step), then positions
-  by_octant([&](int64_t lo, int64_t hi) {
-    for (int64_t t = 0; t < ntask; ++t) {
+  by_octant([&](int64_t lo, int64_t hi, int64_t tb, int64_t te) {
+    for (int64_t t = tb; t < te; ++t) {
       const int64_t pr = pair_of[(size_t)t];
       if (pr >= lo && pr < hi) jstep[(size_t)job_of_pair[(size_t)pr] * nsteps + step[(size_t)t]]++;
     }
@@ -344,8 +419,8 @@ bool build_tile_jobs(const Geometry &g, int TX, int TY, int TZ, int max_slots, T
     for (size_t k = 0; k + 1 < jstep.size(); ++k) { const int32_t c = jstep[k]; jstep[k] = (int32_t)acc; acc += c; }
   }
   BigVec<int64_t> order((size_t)ntask);
-  by_octant([&](int64_t lo, int64_t hi) {
-    for (int64_t t = 0; t < ntask; ++t) {
+  by_octant([&](int64_t lo, int64_t hi, int64_t tb, int64_t te) {
+    for (int64_t t = tb; t < te; ++t) {
       const int64_t pr = pair_of[(size_t)t];
       if (pr >= lo && pr < hi) order[(size_t)jstep[(size_t)job_of_pair[(size_t)pr] * nsteps + step[(size_t)t]]++] = t;
     }
@@ -386,7 +461,9 @@ bool build_tile_jobs(const Geometry &g, int TX, int TY, int TZ, int max_slots, T
       const int64_t q = tj.task_begin[(size_t)j], e = tj.task_begin[(size_t)j + 1];
       int32_t n = 0;
       bool added;
-      for (int64_t p = q; p < e; ++p) {
+      // both loops stop at max_slots rows (the job is then too large for the tile shape), so
+      // the set never holds more than max_slots + 6 rows, within its capacity
+      for (int64_t p = q; p < e && n < max_slots; ++p) {
         const int32_t *r = &g.tasks[(size_t)order[(size_t)p] * 8];
         set.find_or_add(r[0] * 8 + (r[1] & 7), n + 1, &added);
         n += added;

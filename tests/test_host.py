@@ -415,3 +415,16 @@ def test_sweep_tasks_follow_their_order(n, kw):
     assert np.array_equal(hs[:-1], np.searchsorted(h, np.arange(len(hs) - 1)))
     assert hs[-1] == len(t)
     assert len(np.unique(t[:, 0] * 8 + o)) == len(t)
+
+
+@pytest.mark.timeout(120)
+def test_oversized_tiles_fall_back_to_the_node_schedule():
+    """A tile shape whose jobs need more shared-memory rows than a block holds (here 16^3
+    tiles, whose own rows alone exceed the row set's capacity) is rejected while the jobs are
+    built, and the context falls back to the per-node hyperplane schedule."""
+    img = images.sphere_pack(20, 0.45, 1.5, 3.0, seed=8)
+    s = pk.Solver(base_params(20, wallExtOrder=1), device=-1)
+    s.set_tiles(16, 16, 16)
+    s.setup_physical_grid(img)
+    assert s.schedule()["tiles"] is False
+    s.close()
