@@ -144,7 +144,7 @@ piks_status piks_setup_seconds(piks_ctx *ctx, double *out);
  *                       (FP64 evaluation); slots must lie an even number of iterations from
  *                       the current state.
  * This takes the iteration off the reference's path: the refined solver (piks3d_b200.solve,
- * FP32 + FP64 refinement) uses it and is judged by its permeability against the plain FP64
+ * FP32 + FP64 refinement) uses it and is assessed by its permeability against the plain FP64
  * solve; the plain FP64 solve never calls it. Single-box contexts only. No counterpart in
  * the reference. */
 piks_status piks_snapshot_slot(piks_ctx *ctx, int32_t slot, int32_t nslots);
